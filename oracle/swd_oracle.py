@@ -1,0 +1,629 @@
+"""TEST INFRASTRUCTURE ONLY -- the CPU oracle for the SWD gradient hot path.
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
+leg may import this module; the product package ``swd_b200`` never does.
+
+Parity status: UNPINNED.  The reference (zhangchang271/SWD) has no tests,
+golden vectors or stored outputs, and it cannot run here (MATLAB, Octave,
+Eigen and the MATLAB MEX headers are all absent).  Every function below is a
+restatement of a reference function, cited by file:line, in double precision
+like MATLAB, so that the GPU path can be compared with it on identical
+seeded inputs.  Third-party semantics that the reference relies on but does
+not contain are restated from their published definitions:
+
+* MATLAB ``fft``/``ifft``: the plain DFT definition (numpy's pocketfft).
+* MATLAB ``softmax`` (Deep Learning Toolbox): column-wise, max-shifted.
+* MATLAB ``findpeaks`` (Signal Processing Toolbox), no options: a sample
+  strictly larger than both neighbours; a flat peak is reported at its first
+  index; signal endpoints are never peaks.
+* MATLAB ``max``: first index of the maximum.
+* MATLAB ``interp1`` 'linear' (NaN outside the sample range) and
+  'nearest','extrap'.
+* MATLAB ``round``: half away from zero.
+
+The FD time loops live in ``oracle/swd_oracle.cpp`` (loaded through ctypes as
+``oracle/_build/libswd_oracle.so``); ``fd_forward_np``/``fd_adjoint_np`` below
+are a second, independent vectorised restatement of the same loops used to
+cross-check the C++ one bit-for-bit on small grids.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libswd_oracle.so")
+_lib = None
+
+
+def lib():
+    """Load the compiled C++ oracle (``make -C oracle``)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            raise RuntimeError(f"oracle library not built: {_LIB_PATH} (run make -C oracle)")
+        L = ctypes.CDLL(_LIB_PATH)
+        f32p = ctypes.POINTER(ctypes.c_float)
+        f64p = ctypes.POINTER(ctypes.c_double)
+        L.oracle_staggerfd_f32.argtypes = [f32p, ctypes.c_int] + [f32p] * 14
+        L.oracle_staggerfd_f64.argtypes = [f64p, ctypes.c_int] + [f64p] * 14
+        L.oracle_e2drtm_f32.argtypes = [f32p, ctypes.c_int] + [f32p] * 12 + [ctypes.c_int] + [f64p] * 3
+        L.oracle_e2drtm_f64.argtypes = [f64p, ctypes.c_int] + [f64p] * 12 + [f64p] * 3
+        for f in (L.oracle_staggerfd_f32, L.oracle_staggerfd_f64, L.oracle_e2drtm_f32, L.oracle_e2drtm_f64):
+            f.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    if a is None:
+        return None
+    t = ctypes.c_float if a.dtype == np.float32 else ctypes.c_double
+    return a.ctypes.data_as(ctypes.POINTER(t))
+
+
+def mround(x):
+    """MATLAB round(): half away from zero."""
+    x = float(x)
+    r = math.floor(abs(x))
+    if abs(x) - r >= 0.5:
+        r += 1
+    return int(math.copysign(r, x)) if r else 0
+
+
+# --------------------------------------------------------------------------------------
+# Model preparation (setup of the FD inputs)
+# --------------------------------------------------------------------------------------
+
+def calparam(vp, vs, den):
+    """core/calparam.m:3-5."""
+    ca = (vp ** 2) * den
+    cm = (vs ** 2) * den
+    cl = ca - 2 * cm
+    return ca, cm, cl
+
+
+def pad(p0, nbc, isfs, pad_top):
+    """core/pad.m:3-8: edge replication, pad_top rows on top when isfs."""
+    p = np.concatenate([np.repeat(p0[:, :1], nbc, 1), p0, np.repeat(p0[:, -1:], nbc, 1)], 1)
+    top = pad_top if isfs else nbc
+    return np.concatenate([np.repeat(p[:1, :], top, 0), p, np.repeat(p[-1:, :], nbc, 0)], 0)
+
+
+def damp_circle(vmin, nzbc, nxbc, nbc, dx, isfs, pad_top):
+    """core/damp_circle.m:5-71 (1-based loops restated 0-based)."""
+    nz = nzbc - nbc - pad_top
+    nx = nxbc - 2 * nbc
+    a = (nbc - 1) * dx
+    kappa = 3.0 * vmin * math.log(10000000.0) / (2.0 * a)
+    r = (np.arange(nbc, dtype=np.float64) * dx) / a
+    damp1d = kappa * (r * r)
+    damp = np.zeros((nzbc, nxbc))
+    for iz in range(pad_top, nz + pad_top):
+        damp[iz, 0:nbc] = damp1d[::-1]
+        damp[iz, nx + nbc:nx + 2 * nbc] = damp1d
+    for ix in range(nbc, nx + nbc):
+        damp[0:pad_top, ix] = 0.0 if isfs else damp1d[::-1]  # pad_top == nbc when isfs=0
+        damp[nzbc - nbc:nzbc, ix] = damp1d
+    def corner(iz1, ix1, cz, cx):
+        d = math.sqrt((ix1 - cx) ** 2 + (iz1 - cz) ** 2)
+        q = d / nbc
+        return kappa * (q * q)
+    if not isfs:
+        for iz1 in range(1, pad_top + 1):
+            for ix1 in range(1, nbc + 1):
+                damp[iz1 - 1, ix1 - 1] = corner(iz1, ix1, pad_top + 1, nbc + 1)
+            for ix1 in range(nx + nbc + 1, nxbc + 1):
+                damp[iz1 - 1, ix1 - 1] = corner(iz1, ix1, pad_top + 1, nx + nbc)
+    for iz1 in range(nz + pad_top + 1, nzbc + 1):
+        for ix1 in range(1, nbc + 1):
+            damp[iz1 - 1, ix1 - 1] = corner(iz1, ix1, nz + pad_top, nbc + 1)
+        for ix1 in range(nx + nbc + 1, nxbc + 1):
+            damp[iz1 - 1, ix1 - 1] = corner(iz1, ix1, nz + pad_top, nbc + nx)
+    return damp
+
+
+def ricker(f, dt, nt=None):
+    """core/ricker.m:18-38."""
+    nw = 2.2 / f / dt
+    nw = 2 * math.floor(nw / 2) + 1
+    nc = math.floor(nw / 2)
+    k = np.arange(1, nw + 1, dtype=np.float64)
+    alpha = (nc - k + 1) * f * dt * math.pi
+    beta = alpha * alpha
+    w0 = (1.0 - beta * 2) * np.exp(-beta)
+    if nt is None:
+        return w0
+    if nt < len(w0):
+        raise ValueError("nt is smaller than condition!")
+    w = np.zeros(nt)
+    w[: len(w0)] = w0
+    return w
+
+
+@dataclass
+class FdInputs:
+    """The padded material fields and input_vector a MEX call receives."""
+    iv: np.ndarray
+    temp: np.ndarray
+    ca: np.ndarray
+    cl: np.ndarray
+    cm: np.ndarray
+    cm1: np.ndarray
+    b: np.ndarray
+    b1: np.ndarray
+    nzbc: int
+    nxbc: int
+    pad_top: int
+
+
+def _prep(nbc, dtx, dx, dt, vp, vs, isfs, fd_order, dtype):
+    """Shared model prep of staggerfd_eigen.m:37-107 and e2drtm_eigen.m:44-101."""
+    nz, nx = vs.shape
+    one = dtype.type(1)
+    vp = np.asarray(vp, np.float64)
+    vs = np.asarray(vs, np.float64)
+    # calparam with den = ones(single|double): double squares, rounded to the class of den
+    ca = (vp * vp).astype(dtype) * one
+    cm = (vs * vs).astype(dtype) * one
+    cl = (ca - dtype.type(2) * cm).astype(dtype)
+    pad_top = (fd_order - 20) // 2 + 1 if isfs else nbc
+    cm = pad(cm, nbc, isfs, pad_top)
+    cl = pad(cl, nbc, isfs, pad_top)
+    den = pad(np.ones((nz, nx), dtype), nbc, isfs, pad_top)
+    nzbc, nxbc = cm.shape
+    vmin = float(min(vp.min(), vs.min()))
+    damp = damp_circle(vmin, nzbc, nxbc, nbc, dx, isfs, pad_top)
+    temp = (1 - damp * dt).astype(dtype)
+    if not isfs:
+        raise NotImplementedError("isfs=0 leaves b1/cm1 undefined in the reference wrappers")
+    ca = pad(ca, nbc, isfs, pad_top)
+    r = pad_top - 1
+    ca[r, :] = dtype.type(2) * cm[r, :]
+    cl[r, :] = 0
+    b = (dtype.type(dtx) / den).astype(dtype)
+    b[r, :] = dtype.type(2) * b[r, :]
+    return ca, cl, cm, cm.copy(), b, b.copy(), temp, nzbc, nxbc, pad_top
+
+
+_SRC = {"p": 1, "s": 2, "s1": 3, "z": 4, "w": 5}
+
+
+def fd_inputs(nbc, nt, dtx, dx, dt, sx, sz, gx, gz, vp, vs, isfs=1, fd_order=22, source_type="w",
+              in_wf=5, single=True, adjoint=False):
+    """Build the MEX inputs exactly as staggerfd_eigen.m:37-138 (forward) or e2drtm_eigen.m:44-121."""
+    dtype = np.dtype(np.float32 if single else np.float64)
+    ca, cl, cm, cm1, b, b1, temp, nzbc, nxbc, pad_top = _prep(nbc, dtx, dx, dt, vp, vs, isfs, fd_order, dtype)
+    nz, nx = vs.shape
+    gx = np.atleast_1d(np.asarray(gx, np.float64))
+    gz = np.atleast_1d(np.asarray(gz, np.float64))
+    ng = gx.size
+    gxp, gzp = gx + nbc, gz + pad_top
+    dg = gxp[1] - gxp[0] if ng > 1 else 1
+    if adjoint:
+        iv = [nt, nzbc, nxbc, dtx, ng, nbc, gzp[0], gxp[0], dg, fd_order, in_wf, nz, nx, dt]
+    else:
+        iv = [nt, nzbc, nxbc, dtx, ng, sz + pad_top, sx + nbc, gzp[0], gxp[0], dg,
+              _SRC[source_type], fd_order, in_wf, nz, nx, 3]
+    iv = np.asarray(iv, dtype)
+    F = lambda a: np.asfortranarray(a, dtype)
+    return FdInputs(iv, F(temp), F(ca), F(cl), F(cm), F(cm1), F(b), F(b1), nzbc, nxbc, pad_top)
+
+
+def mex_staggerfd(inp: FdInputs, s, want_wf=True):
+    """Call the C++ oracle with MEX arguments; returns (seismo_u, seismo_w, {fux,fuz,bwx,bwz})."""
+    dt_ = inp.temp.dtype
+    iv = inp.iv
+    nt, ng, nz, nx, ntwf = int(iv[0]), int(iv[4]), int(iv[13]), int(iv[14]), int(iv[12])
+    s = np.ascontiguousarray(np.asarray(s).reshape(-1)[:nt], dt_)
+    su = np.zeros((nt, ng), dt_, order="F")
+    sw = np.zeros((nt, ng), dt_, order="F")
+    nrec = nt // ntwf
+    wf = {k: (np.zeros((nz, nx, nrec), dt_, order="F") if want_wf else None) for k in ("fux", "fuz", "bwx", "bwz")}
+    fn = lib().oracle_staggerfd_f32 if dt_ == np.float32 else lib().oracle_staggerfd_f64
+    rc = fn(_p(np.ascontiguousarray(iv)), iv.size, _p(inp.temp), _p(inp.ca), _p(inp.cl), _p(inp.cm), _p(inp.cm1),
+            _p(inp.b), _p(inp.b1), _p(s), _p(su), _p(sw), _p(wf["fux"]), _p(wf["fuz"]), _p(wf["bwx"]), _p(wf["bwz"]))
+    if rc:
+        raise ValueError(f"oracle_staggerfd rc={rc}")
+    return su, sw, wf
+
+
+def mex_e2drtm(inp: FdInputs, res, wf, accum_fp64=True):
+    """Call the C++ adjoint oracle; returns (cl_img, cm_img, illum_div) as float64 arrays (nz x nx)."""
+    dt_ = inp.temp.dtype
+    iv = inp.iv
+    nz, nx = int(iv[11]), int(iv[12])
+    res = np.asfortranarray(res, dt_)
+    outs = [np.zeros((nz, nx), np.float64, order="F") for _ in range(3)]
+    W = [np.asfortranarray(wf[k], dt_) for k in ("fux", "fuz", "bwx", "bwz")]
+    args = [_p(np.ascontiguousarray(iv)), iv.size, _p(inp.temp), _p(inp.ca), _p(inp.cl), _p(inp.cm), _p(inp.cm1),
+            _p(inp.b), _p(inp.b1), _p(res)] + [_p(w) for w in W]
+    if dt_ == np.float32:
+        rc = lib().oracle_e2drtm_f32(*args, int(accum_fp64), *[_p(o) for o in outs])
+    else:
+        rc = lib().oracle_e2drtm_f64(*args, *[_p(o) for o in outs])
+    if rc:
+        raise ValueError(f"oracle_e2drtm rc={rc}")
+    return tuple(outs)
+
+
+def staggerfd_eigen(is_, nbc, nt, dtx, dx, dt, sx, sz, gx, gz, s, vp, vs, isfs=1, fd_order=22,
+                    source_type="w", parameter_type=0, in_wf=5, single=True):
+    """core/staggerfd_eigen.m:2-142 (single=False: staggerfd_eigend.m)."""
+    inp = fd_inputs(nbc, nt, dtx, dx, dt, sx, sz, gx, gz, vp, vs, isfs, fd_order, source_type, in_wf, single)
+    return mex_staggerfd(inp, s)
+
+
+def e2drtm_eigen(wavefield_gradient, seismo_w, is_, nbc, nt, dtx, dx, dt, gx, gz, s, vp, vs, isfs=1,
+                 fd_order=22, parameter_type=0, in_wf=5, single=True, accum_fp64=True):
+    """core/e2drtm_eigen.m:8-123 (single=False: e2drtm_eigend.m)."""
+    inp = fd_inputs(nbc, nt, dtx, dx, dt, 0, 0, gx, gz, vp, vs, isfs, fd_order, "w", in_wf, single, adjoint=True)
+    return mex_e2drtm(inp, seismo_w, wavefield_gradient, accum_fp64)
+
+
+# --------------------------------------------------------------------------------------
+# Independent vectorised FD restatement (small grids; cross-checks the C++ oracle)
+# --------------------------------------------------------------------------------------
+
+def fd_forward_np(inp: FdInputs, s):
+    """Vectorised restatement of core/eigen_staggerfd_single.cpp:207-357 (fd_order 22)."""
+    T = inp.temp.dtype.type
+    iv = inp.iv
+    nt, NZ, NX, dtx = int(iv[0]), int(iv[1]), int(iv[2]), T(iv[3])
+    ng, sz, sx, gz, gx, dg = int(iv[4]), int(iv[5]) - 1, int(iv[6]) - 1, int(iv[7]) - 1, int(iv[8]) - 1, int(iv[9])
+    st, ntwf, nz, nx = int(iv[10]), int(iv[12]), int(iv[13]), int(iv[14])
+    nbc = (NX - nx) // 2
+    z = np.zeros((NZ, NX), inp.temp.dtype)
+    uu, ww, xx, zz, xz = z.copy(), z.copy(), z.copy(), z.copy(), z.copy()
+    fux, fuz, bwx, bwz = z.copy(), z.copy(), z.copy(), z.copy()
+    te, b, b1, ca, cl, cm1 = (np.asarray(a) for a in (inp.temp, inp.b, inp.b1, inp.ca, inp.cl, inp.cm1))
+    su = np.zeros((nt, ng), z.dtype)
+    sw = np.zeros((nt, ng), z.dtype)
+    wf = {k: np.zeros((nz, nx, nt // ntwf), z.dtype) for k in ("fux", "fuz", "bwx", "bwz")}
+    C = (slice(1, NZ - 1), slice(1, NX - 1))
+    S = lambda dz, dx_: (slice(1 + dz, NZ - 1 + dz), slice(1 + dx_, NX - 1 + dx_))
+    cols = gx + dg * np.arange(ng)
+    for it in range(nt):
+        uu[C] = te[C] * uu[C] + b[C] * (((xx[S(0, 1)] - xx[C]) + xz[C]) - xz[S(-1, 0)])
+        ww[C] = te[C] * ww[C] + b1[C] * (((xz[C] - xz[S(0, -1)]) + zz[S(1, 0)]) - zz[C])
+        sv = T(s[it])
+        if st == 5:
+            ww[sz, sx] = sv
+        elif st == 1:
+            xx[sz, sx] += sv; zz[sz, sx] += sv
+        elif st == 2:
+            uu[sz, sx] += sv; uu[sz - 1, sx] -= sv; ww[sz, sx] += sv; ww[sz, sx + 1] += sv
+        elif st == 3:
+            uu[sz, sx] += sv; ww[sz, sx] += sv
+        elif st == 4:
+            zz[sz, sx] += sv
+        fux[C] = uu[C] - uu[S(0, -1)]
+        fuz[C] = uu[S(1, 0)] - uu[C]
+        bwx[C] = ww[S(0, 1)] - ww[C]
+        bwz[C] = ww[C] - ww[S(-1, 0)]
+        xx = te * xx + (ca * fux + cl * bwz) * dtx
+        zz = te * zz + (ca * bwz + cl * fux) * dtx
+        xz = te * xz + (cm1 * (fuz + bwx)) * dtx
+        zz[1, :] = 0
+        sw[it] = ww[gz, cols]
+        su[it] = uu[gz, cols]
+        if it % ntwf == 0:
+            k = it // ntwf
+            for name, a in (("fux", fux), ("fuz", fuz), ("bwx", bwx), ("bwz", bwz)):
+                wf[name][:, :, k] = a[2:2 + nz, nbc:nbc + nx]
+    return su, sw, wf
+
+
+def fd_adjoint_np(inp: FdInputs, res, wf, accum_fp64=True):
+    """Vectorised restatement of core/eigen_e2drtm_single.cpp:181-283 (fd_order 22)."""
+    dtp = inp.temp.dtype
+    T = dtp.type
+    iv = inp.iv
+    nt, NZ, NX, dtx = int(iv[0]), int(iv[1]), int(iv[2]), T(iv[3])
+    ng, nbc, gz, gx, dg = int(iv[4]), int(iv[5]), int(iv[6]) - 1, int(iv[7]) - 1, int(iv[8])
+    ntwf, nz, nx, dt = int(iv[10]), int(iv[11]), int(iv[12]), T(iv[13])
+    z = np.zeros((NZ, NX), dtp)
+    uu, ww, xx, zz, xz = z.copy(), z.copy(), z.copy(), z.copy(), z.copy()
+    te, b, b1, ca, cl, cm1 = (np.asarray(a) for a in (inp.temp, inp.b, inp.b1, inp.ca, inp.cl, inp.cm1))
+    acc = np.float64 if accum_fp64 else dtp
+    gcl, gcm, gil = (np.zeros((nz, nx), acc) for _ in range(3))
+    C = (slice(1, NZ - 1), slice(1, NX - 1))
+    S = lambda dz, dx_: (slice(1 + dz, NZ - 1 + dz), slice(1 + dx_, NX - 1 + dx_))
+    cols = gx + dg * np.arange(ng)
+    res = np.asarray(res, dtp)
+    for it in range(nt - 2, -1, -1):
+        du = ((ca[C] * xx[C] - ca[S(0, -1)] * xx[S(0, -1)]) + (cl[C] * zz[C] - cl[S(0, -1)] * zz[S(0, -1)])) + \
+             (cm1[C] * xz[C] - cm1[S(-1, 0)] * xz[S(-1, 0)])
+        dw = ((cl[S(1, 0)] * xx[S(1, 0)] - cl[C] * xx[C]) + (ca[S(1, 0)] * zz[S(1, 0)] - ca[C] * zz[C])) + \
+             (cm1[S(0, 1)] * xz[S(0, 1)] - cm1[C] * xz[C])
+        uu[C] = te[C] * uu[C] - b[C] * du
+        ww[C] = te[C] * ww[C] - b1[C] * dw
+        ww[gz, cols] = ww[gz, cols] + dt * res[it, :]
+        xx[C] = te[C] * xx[C] - dtx * (uu[S(0, 1)] - uu[C])
+        zz[C] = te[C] * zz[C] - dtx * (ww[C] - ww[S(-1, 0)])
+        xz[C] = (te[C] * xz[C] - dtx * (uu[S(1, 0)] - uu[C])) - dtx * (ww[C] - ww[S(0, -1)])
+        zz[1, :] = 0
+        if it % ntwf == 0:
+            k = it // ntwf
+            fx, fz, bx, bz = (np.asarray(wf[n][:, :, k], dtp) for n in ("fux", "fuz", "bwx", "bwz"))
+            I = (slice(2, 2 + nz), slice(nbc, nbc + nx))
+            F = fx + bz
+            tcl = F * (xx[I] + zz[I])
+            tcm = T(2) * ((xx[I] * fx + zz[I] * bz) + T(0.5) * (xz[I] * (fz + bx)))
+            til = F * F
+            gcl = gcl + tcl.astype(acc)
+            gcm = gcm + tcm.astype(acc)
+            gil = gil + til.astype(acc)
+    return gcl.astype(np.float64), gcm.astype(np.float64), gil.astype(np.float64)
+
+
+# --------------------------------------------------------------------------------------
+# Linear Radon transform (dispersion spectrum) and its saved state
+# --------------------------------------------------------------------------------------
+
+def radon_window(is_, b, offset, m, M, side):
+    """Trace window of RTr.m:5-12 (side='r') or RTl.m:5-12 (side='l'); 1-based columns in order."""
+    if side == "r":
+        c0 = M * is_ - M + 1 + m
+        nend = min(m + offset - 1 + M * is_ - M + 1, b)
+        cols = list(range(c0, nend + 1))
+    else:
+        nend = M * is_ - M + 1 - offset - m
+        if nend < 1:
+            nend = 0
+        cols = list(range(nend + 1, M * is_ - M + 1 - m + 1))
+        cols = cols[::-1]  # fliplr
+    return cols
+
+
+def velocities(vmin, vmax, dv=1.0):
+    """The phase-velocity axis: vmin:vmax in the reference (RTr.m:21); vmin:dv:vmax in general."""
+    n = int(math.floor((vmax - vmin) / dv + 1e-9)) + 1
+    return vmin + dv * np.arange(n, dtype=np.float64)
+
+
+def radon(seismo, is_, df, dt, vmin, vmax, fmin, fmax, b, ds, offset, m, M, side, dv=1.0):
+    """RTrAD.m:2-35 / RTlAD.m:2-36 (ml is also RTr/RTl's output).
+
+    Returns ml (np x npair, column-max normalised), dataLen and saveForBackward
+    {mm (np x nf complex), ll0, lf, nf, ccn, ml_raw (np x npair), uxtpos (1-based cols, ascending)}.
+    """
+    cols = radon_window(is_, b, offset, m, M, side)
+    uxt = np.asarray(seismo, np.float64)[:, [c - 1 for c in cols]]
+    noff = uxt.shape[1]
+    x = (m + np.arange(noff, dtype=np.float64)) * ds
+    ccn = int(math.trunc(1.0 / df / dt))
+    nt = uxt.shape[0]
+    u = np.zeros((ccn, noff))
+    u[: min(nt, ccn)] = uxt[: min(nt, ccn)]
+    d = np.fft.fft(u, axis=0).T  # noff x ccn
+    lf = mround(fmin / df) + 1
+    nf = mround(fmax / df) + 1
+    pp = 1.0 / velocities(vmin, vmax, dv)
+    w0 = 2.0 * math.pi * df
+    th0 = w0 * np.outer(pp, x)                      # imag part of ll0 (np x noff)
+    ll0 = 1j * th0
+    mm = np.zeros((pp.size, nf), np.complex128)
+    for j in range(lf, nf + 1):
+        l = np.exp(1j * (th0 * (j - 1)))
+        mm[:, j - 1] = l @ d[:, j - 1]
+    mlraw = np.abs(mm[:, lf - 1:nf])
+    ml = mlraw / mlraw.max(axis=0, keepdims=True)
+    pos = sorted(cols)
+    return ml, noff, dict(mm=mm, ll0=ll0, lf=lf, nf=nf, ccn=ccn, ml_raw=mlraw, uxtpos=pos, x=x)
+
+
+# --------------------------------------------------------------------------------------
+# Dispersion picking
+# --------------------------------------------------------------------------------------
+
+def findpeaks_locs(y):
+    """1-based locations of MATLAB findpeaks(y) (no options), finite input."""
+    y = np.asarray(y, np.float64)
+    n = y.size
+    locs = []
+    k = 1
+    while k < n - 1:
+        if y[k] > y[k - 1]:
+            j = k + 1
+            while j < n and y[j] == y[k]:
+                j += 1
+            if j < n and y[j] < y[k]:
+                locs.append(k + 1)
+            k = j
+        else:
+            k += 1
+    return locs
+
+
+def _argmax1(v):
+    return int(np.argmax(v)) + 1  # first index of the max, 1-based
+
+
+def pickFDC1(ml, lp, fg, lfg):
+    """core/pickFDC1.m:1-131; returns (cr_0 after interpolation, dvmin, dvmax, raw idx, chazhi)."""
+    ml = np.asarray(ml, np.float64)
+    if np.isnan(ml).any():
+        raise ValueError("pickFDC1: NaN in the spectrum is not supported")
+    a, b = ml.shape
+    idx = np.zeros(b + 1, np.int64)          # 1-based arrays, index 0 unused
+    dvmax = np.zeros(b + 1, np.int64)
+    dvmin = np.zeros(b + 1, np.int64)
+    qujian = np.full(b + 1, np.nan)
+    chazhi = np.ones(b + 1, np.int64)
+    col = lambda i: ml[:, i - 1]
+    idx[lp] = _argmax1(col(lp))                                  # :19
+    for i in range(lp - 1, 0, -1):                               # :21-77
+        if idx[i + 1] == a:
+            idx[i] = a
+            dvmax[i] = dvmax[i + 1]
+            dvmin[i] = dvmin[i + 1]
+            continue
+        if idx[i + 1] > a - 3:
+            dvmax[i] = a
+        else:
+            mlmax = findpeaks_locs(-col(i)[idx[i + 1] - 1:a])
+            dvmax[i] = a if not mlmax else idx[i + 1] + min(mlmax)
+        if idx[i + 1] < 3:
+            dvmin[i] = 1
+        else:
+            mlmin = findpeaks_locs(-col(i)[0:idx[i + 1]])
+            dvmin[i] = 1 if not mlmin else max(mlmin)
+        qujian[i] = dvmax[i] - dvmin[i]
+        if qujian[i] > qujian[i + 1] * lfg:
+            idx[i] = idx[i + 1]
+            chazhi[i] = 0
+            dvmax[i] = dvmax[i + 1]
+            dvmin[i] = dvmin[i + 1]
+            qujian[i] = dvmax[i] - dvmin[i]
+        else:
+            idx[i] = dvmin[i] + _argmax1(col(i)[dvmin[i] - 1:dvmax[i]]) - 1
+    for i in range(lp + 1, b + 1):                               # :79-128
+        if idx[i - 1] > a - 3:
+            dvmax[i] = a
+        else:
+            mlmax = findpeaks_locs(-col(i)[idx[i - 1] - 1:a])
+            dvmax[i] = a if not mlmax else idx[i - 1] + min(mlmax)
+        if idx[i - 1] < 3:
+            dvmin[i] = 1
+        else:
+            mlmin = findpeaks_locs(-col(i)[0:idx[i - 1]])
+            dvmin[i] = 1 if not mlmin else max(mlmin)
+        qujian[i] = dvmax[i] - dvmin[i]
+        if qujian[i] > fg * qujian[i - 1]:
+            idx[i] = idx[i - 1]
+            chazhi[i] = 0
+            dvmax[i] = dvmax[i - 1]
+            dvmin[i] = dvmin[i - 1]
+            qujian[i] = dvmax[i] - dvmin[i]
+        else:
+            idx[i] = dvmin[i] + _argmax1(col(i)[dvmin[i] - 1:dvmax[i]]) - 1
+    cr = interp_picks(idx[1:], chazhi[1:])                       # :129-131
+    return cr, dvmin[1:], dvmax[1:], idx[1:], chazhi[1:]
+
+
+def interp_picks(idx, chazhi):
+    """interp1(que, idx(que), 1:b, 'linear') then interp1(..., 'nearest', 'extrap') (pickFDC1.m:129-131)."""
+    b = idx.size
+    que = np.nonzero(chazhi == 1)[0] + 1
+    if que.size < 2:
+        raise ValueError("pickFDC1: interp1 needs at least two retained picks")
+    q = np.arange(1, b + 1, dtype=np.float64)
+    yv = idx[que - 1].astype(np.float64)
+    out = np.full(b, np.nan)
+    for t in range(b):
+        xq = q[t]
+        if xq < que[0] or xq > que[-1]:
+            continue
+        k = int(np.searchsorted(que, xq, side="right")) - 1
+        if k >= que.size - 1:
+            out[t] = yv[-1]
+            continue
+        x0, x1, y0, y1 = float(que[k]), float(que[k + 1]), yv[k], yv[k + 1]
+        if xq == x0:
+            out[t] = y0
+        else:
+            out[t] = y0 + (xq - x0) * ((y1 - y0) / (x1 - x0))
+    lo, hi = int(que[0]) - 1, int(que[-1]) - 1
+    out[:lo] = out[lo]
+    out[hi + 1:] = out[hi]
+    return out
+
+
+def LHDispPick(ml, vmin, cr_0, method=1, ini=10):
+    """core/LHDispPick.m:2-13."""
+    if method == 1:
+        cr, *_ = pickFDC1(ml, ini, 2, 4)
+        cr_pre = cr + vmin
+    else:
+        cr_pre = np.argmax(ml, axis=0) + 1 + vmin
+    res = float(np.mean((cr_pre - np.asarray(cr_0, np.float64)) ** 2))
+    return res, cr_pre
+
+
+# --------------------------------------------------------------------------------------
+# SoftMax misfit gradient -> time-domain adjoint source
+# --------------------------------------------------------------------------------------
+
+def softmax_cols(z):
+    """Column-wise softmax, max-shifted (MATLAB Deep Learning Toolbox softmax on an N-by-Q matrix)."""
+    zm = z - z.max(axis=0, keepdims=True)
+    e = np.exp(zm)
+    return e / e.sum(axis=0, keepdims=True)
+
+
+def adwd_side(nt, ng, npair, soft_arg_norm, grad_output, save, side, a_data_res):
+    """One side of core/ADWDgrad_1.m:15-44 (right) / :47-77 (left), written into a_data_res."""
+    lf, nf, ccn = save["lf"], save["nf"], save["ccn"]
+    pos = save["uxtpos"]
+    noff = len(pos)
+    mlr = save["ml_raw"] ** (1.0 / 40.0)
+    E = softmax_cols(mlr * soft_arg_norm)
+    npv = E.shape[0]
+    space = np.arange(1, npv + 1, dtype=np.float64)[:, None]
+    go = np.array(grad_output, np.float64).copy()
+    go[go == 0] = 1
+    mean_s = (space * E).sum(axis=0, keepdims=True)
+    test3 = E * space - mean_s * E
+    gradml = test3 * 2 * go[None, :npair] * soft_arg_norm
+    mm = save["mm"][:, lf - 1:nf]
+    with np.errstate(invalid="ignore", divide="ignore"):
+        ph = mm / np.abs(mm)
+    ph[np.isnan(ph)] = 0
+    gm = ph * gradml
+    th0 = save["ll0"].imag
+    G = np.zeros((noff, ccn), np.complex128)
+    for j in range(lf, nf + 1):
+        K = np.exp(1j * (th0 * (j - 1)))
+        G[:, j - 1] = K.conj().T @ gm[:, j - lf]
+    g = np.real(np.fft.ifft(G, ccn, axis=1))[:, :nt]      # noff x nt
+    if side == "r":
+        a_data_res[:, [p - 1 for p in pos]] = g.T
+    else:
+        # uxtposl ascending; row 1 of g is the source trace (fliplr); ADWDgrad_1.m:76
+        a_data_res[:, [p - 1 for p in pos[:-1]]] = g[:0:-1, :].T
+    return a_data_res
+
+
+def has_right(is_, ns, m, M, w):
+    return is_ <= ns - math.floor(m / M) - mround(w / M)
+
+
+def has_left(is_, m, M, w):
+    return is_ >= mround(w / M) + math.floor(m / M) + 1
+
+
+def ADWDgrad_1(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, saver, savel):
+    """core/ADWDgrad_1.m:1-81."""
+    a = np.zeros((nt, ng))
+    if has_right(is_, ns, m, M, w):
+        adwd_side(nt, ng, npair, SoftArgNorm, grad_outputr, saver, "r", a)
+    if has_left(is_, m, M, w):
+        adwd_side(nt, ng, npair, SoftArgNorm, grad_outputl, savel, "l", a)
+    return a
+
+
+# --------------------------------------------------------------------------------------
+# Gradient assembly
+# --------------------------------------------------------------------------------------
+
+def smooth2a(A, Nr, Nc):
+    """core/smooth2a.m:38-76: (2Nr+1)x(2Nc+1) box mean with shrinking edges (finite input)."""
+    A = np.asarray(A, np.float64)
+    r, c = A.shape
+    eL = (np.abs(np.arange(r)[:, None] - np.arange(r)[None, :]) <= Nr).astype(np.float64)
+    eR = (np.abs(np.arange(c)[:, None] - np.arange(c)[None, :]) <= Nc).astype(np.float64)
+    nrm = eL @ np.ones_like(A) @ eR
+    return (eL @ A @ eR) / nrm
+
+
+def assemble(vs, g_cl, g_cm, g_illum, smoothZ=1, smoothX=2):
+    """SWD.m:199-201: illumination normalisation, Vs gradient, smoothing."""
+    g_cl = g_cl / g_illum
+    g_cm = g_cm / g_illum
+    dk = -4 * vs * g_cl + 2 * vs * g_cm
+    return smooth2a(dk, smoothZ, smoothX)

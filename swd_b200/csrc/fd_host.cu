@@ -1,0 +1,382 @@
+// Host side of the FD kernels: geometry planning, launchers, MATLAB-layout
+// conversion and the MEX-convention C entry points (swd_staggerfd_*, swd_e2drtm_*).
+// Compiled with -fmad=false (see fd_kernels.cuh).
+#include <cstdarg>
+#include <cstring>
+#include <atomic>
+#include <vector>
+
+#include "fd_host.cuh"
+#include "fd_kernels.cuh"
+
+namespace swd {
+
+static thread_local char g_err[1024] = "";
+static std::atomic<uint64_t> g_launches{0};
+
+void set_error(const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+void clear_error() { g_err[0] = 0; }
+void count_launch(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// ------------------------------------------------------------ layout kernels
+
+// out[bo*ob + c*R + r] = in[bi*ib + r*C + c]: batched transpose of R x C planes.
+template <typename Ti, typename To>
+__global__ void transpose_kernel(const Ti* __restrict__ in, size_t ib, To* __restrict__ out, size_t ob, int R, int C) {
+  __shared__ Ti tile[32][33];
+  const int b = blockIdx.z;
+  const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+  const Ti* src = in + (size_t)b * ib;
+  To* dst = out + (size_t)b * ob;
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    int r = r0 + i, c = c0 + threadIdx.x;
+    if (r < R && c < C) tile[i][threadIdx.x] = src[(size_t)r * C + c];
+  }
+  __syncthreads();
+  for (int i = threadIdx.y; i < 32; i += blockDim.y) {
+    int c = c0 + i, r = r0 + threadIdx.x;
+    if (r < R && c < C) dst[(size_t)c * R + r] = (To)tile[threadIdx.x][i];
+  }
+}
+
+template <typename Ti, typename To>
+int transpose(const Ti* in, size_t ib, To* out, size_t ob, int B, int R, int C, cudaStream_t st) {
+  if (B <= 0 || R <= 0 || C <= 0) return SWD_OK;
+  dim3 grid((C + 31) / 32, (R + 31) / 32, B), block(32, 8);
+  transpose_kernel<Ti, To><<<grid, block, 0, st>>>(in, ib, out, ob, R, C);
+  count_launch(1);
+  SWD_CUDA(cudaGetLastError());
+  return SWD_OK;
+}
+template int transpose<float, float>(const float*, size_t, float*, size_t, int, int, int, cudaStream_t);
+template int transpose<double, double>(const double*, size_t, double*, size_t, int, int, int, cudaStream_t);
+template int transpose<double, float>(const double*, size_t, float*, size_t, int, int, int, cudaStream_t);
+template int transpose<float, double>(const float*, size_t, double*, size_t, int, int, int, cudaStream_t);
+
+// Pack the MATLAB column-major material fields (nzbc x nxbc) into the row-major
+// vector layout the step kernels read: m1 = {temp, b, b1, 0}, m2 = {ca, cl, cm1, 0}.
+template <typename T>
+__global__ void pack_materials_cm(const T* __restrict__ temp, const T* __restrict__ b, const T* __restrict__ b1,
+                                  const T* __restrict__ ca, const T* __restrict__ cl, const T* __restrict__ cm1,
+                                  typename Vec4<T>::type* m1, typename Vec4<T>::type* m2, int NZ, int NX, int pitch) {
+  const int z = blockIdx.x * blockDim.x + threadIdx.x;  // z fastest: coalesced reads
+  const int x = blockIdx.y;
+  if (z >= NZ || x >= NX) return;
+  const size_t c = (size_t)x * NZ + z;
+  typename Vec4<T>::type u, v;
+  u.x = temp[c]; u.y = b[c]; u.z = b1[c]; u.w = 0;
+  v.x = ca[c]; v.y = cl[c]; v.z = cm1[c]; v.w = 0;
+  m1[(size_t)z * pitch + x] = u;
+  m2[(size_t)z * pitch + x] = v;
+}
+
+template <typename T>
+int pack_materials(const T* temp, const T* b, const T* b1, const T* ca, const T* cl, const T* cm1,
+                   typename Vec4<T>::type* m1, typename Vec4<T>::type* m2, int NZ, int NX, int pitch,
+                   cudaStream_t st) {
+  dim3 grid((NZ + 127) / 128, NX), block(128);
+  pack_materials_cm<T><<<grid, block, 0, st>>>(temp, b, b1, ca, cl, cm1, m1, m2, NZ, NX, pitch);
+  count_launch(1);
+  SWD_CUDA(cudaGetLastError());
+  return SWD_OK;
+}
+template int pack_materials<float>(const float*, const float*, const float*, const float*, const float*,
+                                   const float*, float4*, float4*, int, int, int, cudaStream_t);
+template int pack_materials<double>(const double*, const double*, const double*, const double*,
+                                    const double*, const double*, double4*, double4*, int, int, int,
+                                    cudaStream_t);
+
+// ------------------------------------------------------------ planning
+
+void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
+  const int rows = g.NZ - 2;
+  g.n_strips = (g.NX - 2 + kStrip - 1) / kStrip;
+  if (chunk_rows <= 0) {
+    // aim for about one full wave of warps (148 SMs x 32 resident warps)
+    const long target = 148L * 32;
+    long per = (long)g.n_strips * n_shots;
+    int nch = (int)((target + per - 1) / per);
+    nch = std::max(1, std::min(nch, std::max(1, rows / 8)));
+    chunk_rows = (rows + nch - 1) / nch;
+  }
+  g.chunk = std::max(1, std::min(chunk_rows, rows));
+  g.n_chunks = (rows + g.chunk - 1) / g.chunk;
+}
+
+template <typename T, int NF>
+int launch_fwd_step(const FwdArgs<T>& a, int it, cudaStream_t st) {
+  constexpr int WPB = 4;
+  const long warps = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
+  const int blocks = (int)((warps + WPB - 1) / WPB);
+  fd_fwd_step<T, NF, WPB><<<blocks, WPB * 32, 0, st>>>(a, it);
+  count_launch(1);
+  return SWD_OK;
+}
+template <typename T, int NF>
+int launch_adj_step(const AdjArgs<T>& a, int it, cudaStream_t st) {
+  constexpr int WPB = 4;
+  const long warps = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
+  const int blocks = (int)((warps + WPB - 1) / WPB);
+  fd_adj_step<T, NF, WPB><<<blocks, WPB * 32, 0, st>>>(a, it);
+  count_launch(1);
+  return SWD_OK;
+}
+template int launch_fwd_step<float, 3>(const FwdArgs<float>&, int, cudaStream_t);
+template int launch_fwd_step<float, 4>(const FwdArgs<float>&, int, cudaStream_t);
+template int launch_fwd_step<double, 4>(const FwdArgs<double>&, int, cudaStream_t);
+template int launch_adj_step<float, 3>(const AdjArgs<float>&, int, cudaStream_t);
+template int launch_adj_step<float, 4>(const AdjArgs<float>&, int, cudaStream_t);
+template int launch_adj_step<double, 4>(const AdjArgs<double>&, int, cudaStream_t);
+
+// ------------------------------------------------------------ MEX-convention entry points
+
+namespace {
+
+struct FwdIv {
+  int nt, nzbc, nxbc, ng, sz, sx, gz, gx, dg, src_type, fd_order, nt_wf, nz, nx, fmt;
+  double dtx;
+};
+
+template <typename T>
+int parse_fwd_iv(const T* iv, int n_iv, FwdIv& p) {
+  SWD_CHECK(iv != nullptr && n_iv >= 16, "input_vector needs 16 entries (got %d)", n_iv);
+  // core/eigen_staggerfd_single.cpp:98-115 reads the entries by truncation, 1-based positions
+  p.nt = (int)iv[0]; p.nzbc = (int)iv[1]; p.nxbc = (int)iv[2]; p.dtx = (double)iv[3];
+  p.ng = (int)iv[4]; p.sz = (int)iv[5] - 1; p.sx = (int)iv[6] - 1; p.gz = (int)iv[7] - 1;
+  p.gx = (int)iv[8] - 1; p.dg = (int)iv[9]; p.src_type = (int)iv[10]; p.fd_order = (int)iv[11];
+  p.nt_wf = (int)iv[12]; p.nz = (int)iv[13]; p.nx = (int)iv[14]; p.fmt = (int)iv[15];
+  return SWD_OK;
+}
+
+int validate_geom(int nt, int NZ, int NX, int nz, int nx, int nbc, int nt_wf, int fd_order, int ng, int gz,
+                  int gx, int dg) {
+  if (fd_order == 24 || fd_order == 26 || fd_order == 28) {
+    set_error("fd_order %d is accepted by the reference MEX but only fd_order 22 (the one SWD.m uses) is built",
+              fd_order);
+    return SWD_ERR_UNSUPPORTED;
+  }
+  SWD_CHECK(fd_order == 22, "fd_order must be 22 (got %d)", fd_order);
+  SWD_CHECK(nt >= 2, "nt must be >= 2 (got %d)", nt);
+  SWD_CHECK(nt_wf >= 1 && nt % nt_wf == 0, "nt (%d) must be a multiple of nt_wf (%d)", nt, nt_wf);
+  SWD_CHECK(NZ >= 3 && NX >= 3, "padded grid %d x %d too small", NZ, NX);
+  SWD_CHECK(nz >= 1 && nx >= 1 && nbc >= 1 && NX == nx + 2 * nbc && NZ >= nz + 3,
+            "interior %d x %d (nbc %d) does not fit the padded grid %d x %d", nz, nx, nbc, NZ, NX);
+  SWD_CHECK(ng >= 1 && dg >= 1, "need ng >= 1 and dg >= 1 (ng %d, dg %d)", ng, dg);
+  SWD_CHECK(gz >= 1 && gz <= NZ - 2 && gx >= 1 && gx + (long)(ng - 1) * dg <= NX - 2,
+            "receivers (row %d, cols %d..%ld) must lie inside rows/cols 1..n-2 of the padded grid", gz + 1,
+            gx + 1, gx + 1 + (long)(ng - 1) * dg);
+  return SWD_OK;
+}
+
+int validate_source(int st, int sz, int sx, int NZ, int NX) {
+  SWD_CHECK(st >= 1 && st <= 5, "source_type must be 1..5 (got %d)", st);
+  const int zlo = (st == 2) ? 2 : 1, xhi = (st == 2) ? NX - 3 : NX - 2;
+  SWD_CHECK(sz >= zlo && sz <= NZ - 2 && sx >= 1 && sx <= xhi,
+            "source (%d,%d) and its stencil taps must lie inside rows/cols 1..n-2", sz + 1, sx + 1);
+  return SWD_OK;
+}
+
+template <typename T>
+int fill_geom(FdGeom& g, int NZ, int NX, int nz, int nx, int nbc, int nt, int nt_wf, int ng, int gz, int gx,
+              int dg) {
+  g.NZ = NZ; g.NX = NX;
+  g.pitch = round_up(NX, 128 / (int)sizeof(T));
+  g.nz = nz; g.nx = nx; g.nbc = nbc; g.pad_top = 1;
+  g.nt = nt; g.nt_wf = nt_wf; g.nrec = nt / nt_wf;
+  g.ng = ng; g.gz = gz; g.gx = gx; g.dg = dg;
+  g.field = (size_t)NZ * g.pitch;
+  return SWD_OK;
+}
+
+template <typename T>
+int staggerfd_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, const T* cm, const T* cm1,
+                  const T* b, const T* b1, const T* s, T* seis_u, T* seis_w, T* fux, T* fuz, T* bwx, T* bwz) {
+  clear_error();
+  (void)cm;  // passed by the reference, unused by its kernel (cm1 carries mu)
+  FwdIv p;
+  SWD_TRY(parse_fwd_iv(iv, n_iv, p));
+  const int nbc = (p.nxbc - p.nx) / 2;  // core/eigen_staggerfd_single.cpp:116
+  SWD_TRY(validate_geom(p.nt, p.nzbc, p.nxbc, p.nz, p.nx, nbc, p.nt_wf, p.fd_order, p.ng, p.gz, p.gx, p.dg));
+  SWD_TRY(validate_source(p.src_type, p.sz, p.sx, p.nzbc, p.nxbc));
+  SWD_CHECK(temp && ca && cl && cm1 && b && b1 && s && seis_w, "null input/output pointer");
+  const bool want_wf = fux || fuz || bwx || bwz;
+  SWD_CHECK(!want_wf || (fux && fuz && bwx && bwz), "fux/fuz/bwx/bwz must all be given or all be NULL");
+  FdGeom g{};
+  fill_geom<T>(g, p.nzbc, p.nxbc, p.nz, p.nx, nbc, p.nt, p.nt_wf, p.ng, p.gz, p.gx, p.dg);
+  plan_decomposition(g, 1, 0);
+  using V = typename Vec4<T>::type;
+  const size_t NN = (size_t)p.nzbc * p.nxbc, plane = (size_t)p.nz * p.nx;
+  DevBuf d_in, d_m1, d_m2, d_state, d_seis, d_seis_t, d_snap, d_snap_t, d_src;
+  SWD_TRY(d_in.alloc(6 * NN * sizeof(T) + p.nt * sizeof(T)));
+  SWD_TRY(d_m1.alloc(g.field * sizeof(V)));
+  SWD_TRY(d_m2.alloc(g.field * sizeof(V)));
+  SWD_TRY(d_state.alloc(2 * 5 * g.field * sizeof(T)));
+  SWD_TRY(d_seis.alloc(2 * (size_t)p.nt * p.ng * sizeof(T)));
+  SWD_TRY(d_seis_t.alloc(2 * (size_t)p.nt * p.ng * sizeof(T)));
+  SWD_TRY(d_src.alloc(sizeof(int2)));
+  if (want_wf) {
+    SWD_TRY(d_snap.alloc((size_t)g.nrec * 4 * plane * sizeof(T)));
+    SWD_TRY(d_snap_t.alloc((size_t)g.nrec * plane * sizeof(T)));
+  }
+  cudaStream_t st = 0;
+  T* din = d_in.as<T>();
+  const T* hsrc[6] = {temp, b, b1, ca, cl, cm1};
+  for (int i = 0; i < 6; ++i) SWD_CUDA(cudaMemcpyAsync(din + i * NN, hsrc[i], NN * sizeof(T), cudaMemcpyHostToDevice, st));
+  T* d_s = din + 6 * NN;
+  SWD_CUDA(cudaMemcpyAsync(d_s, s, p.nt * sizeof(T), cudaMemcpyHostToDevice, st));
+  int2 sp = make_int2(p.sz, p.sx);
+  SWD_CUDA(cudaMemcpyAsync(d_src.p, &sp, sizeof(int2), cudaMemcpyHostToDevice, st));
+  SWD_TRY(pack_materials<T>(din, din + NN, din + 2 * NN, din + 3 * NN, din + 4 * NN, din + 5 * NN, d_m1.as<V>(),
+                            d_m2.as<V>(), p.nzbc, p.nxbc, g.pitch, st));
+  SWD_CUDA(cudaMemsetAsync(d_state.p, 0, d_state.bytes, st));
+  SWD_CUDA(cudaMemsetAsync(d_seis.p, 0, d_seis.bytes, st));
+  FwdArgs<T> a{};
+  a.g = g; a.m1 = d_m1.as<V>(); a.m2 = d_m2.as<V>();
+  a.src = d_src.as<int2>(); a.src_type = p.src_type; a.s = d_s; a.dtx = (T)p.dtx;
+  a.seis_w = d_seis.as<T>(); a.seis_u = a.seis_w + (size_t)p.nt * p.ng;
+  a.snap = want_wf ? d_snap.as<T>() : nullptr;
+  a.n_shots = 1;
+  T* bufs[2] = {d_state.as<T>(), d_state.as<T>() + 5 * g.field};
+  for (int it = 0; it < p.nt; ++it) {
+    a.in = bufs[it & 1];
+    a.out = bufs[(it + 1) & 1];
+    launch_fwd_step<T, 4>(a, it, st);
+  }
+  SWD_CUDA(cudaGetLastError());
+  // seismograms: [2][nt][ng] -> MATLAB nt x ng (column-major) each
+  SWD_TRY(transpose<T, T>(d_seis.as<T>(), (size_t)p.nt * p.ng, d_seis_t.as<T>(), (size_t)p.nt * p.ng, 2, p.nt, p.ng, st));
+  SWD_CUDA(cudaMemcpyAsync(seis_w, d_seis_t.as<T>(), (size_t)p.nt * p.ng * sizeof(T), cudaMemcpyDeviceToHost, st));
+  if (seis_u)
+    SWD_CUDA(cudaMemcpyAsync(seis_u, d_seis_t.as<T>() + (size_t)p.nt * p.ng, (size_t)p.nt * p.ng * sizeof(T),
+                             cudaMemcpyDeviceToHost, st));
+  if (want_wf) {
+    // snapshots [nrec][f][nz][nx] -> MATLAB nz x nx x nrec per field
+    T* outs[4] = {fux, fuz, bwx, bwz};
+    for (int f = 0; f < 4; ++f) {
+      SWD_TRY(transpose<T, T>(d_snap.as<T>() + f * plane, 4 * plane, d_snap_t.as<T>(), plane, g.nrec, p.nz, p.nx, st));
+      SWD_CUDA(cudaMemcpyAsync(outs[f], d_snap_t.p, (size_t)g.nrec * plane * sizeof(T), cudaMemcpyDeviceToHost, st));
+    }
+  }
+  SWD_CUDA(cudaStreamSynchronize(st));
+  return SWD_OK;
+}
+
+template <typename T, typename TO>
+int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, const T* cm, const T* cm1,
+               const T* b, const T* b1, const T* res, const T* fux, const T* fuz, const T* bwx, const T* bwz,
+               TO* cl_img, TO* cm_img, TO* illum) {
+  clear_error();
+  (void)cm;
+  SWD_CHECK(iv != nullptr && n_iv >= 14, "input_vector needs 14 entries (got %d)", n_iv);
+  // core/eigen_e2drtm_single.cpp:69-84
+  const int nt = (int)iv[0], NZ = (int)iv[1], NX = (int)iv[2], ng = (int)iv[4], nbc = (int)iv[5];
+  const int gz = (int)iv[6] - 1, gx = (int)iv[7] - 1, dg = (int)iv[8], fd_order = (int)iv[9];
+  const int nt_wf = (int)iv[10], nz = (int)iv[11], nx = (int)iv[12];
+  const T dtx = iv[3], dt = iv[13];
+  SWD_TRY(validate_geom(nt, NZ, NX, nz, nx, nbc, nt_wf, fd_order, ng, gz, gx, dg));
+  SWD_CHECK(temp && ca && cl && cm1 && b && b1 && res && fux && fuz && bwx && bwz && cl_img && cm_img && illum,
+            "null input/output pointer");
+  FdGeom g{};
+  fill_geom<T>(g, NZ, NX, nz, nx, nbc, nt, nt_wf, ng, gz, gx, dg);
+  plan_decomposition(g, 1, 0);
+  using V = typename Vec4<T>::type;
+  const size_t NN = (size_t)NZ * NX, plane = (size_t)nz * nx, nsnap = (size_t)g.nrec * plane;
+  DevBuf d_in, d_m1, d_m2, d_state, d_res, d_snap, d_img, d_out;
+  SWD_TRY(d_in.alloc(std::max(6 * NN, nsnap) * sizeof(T) + (size_t)nt * ng * sizeof(T)));
+  SWD_TRY(d_m1.alloc(g.field * sizeof(V)));
+  SWD_TRY(d_m2.alloc(g.field * sizeof(V)));
+  SWD_TRY(d_state.alloc(2 * 5 * g.field * sizeof(T)));
+  SWD_TRY(d_res.alloc((size_t)nt * ng * sizeof(T)));
+  SWD_TRY(d_snap.alloc(4 * nsnap * sizeof(T)));
+  SWD_TRY(d_img.alloc(3 * plane * sizeof(double)));
+  SWD_TRY(d_out.alloc(3 * plane * sizeof(TO)));
+  cudaStream_t st = 0;
+  T* din = d_in.as<T>();
+  T* dstage = din + std::max(6 * NN, nsnap);
+  const T* hsrc[6] = {temp, b, b1, ca, cl, cm1};
+  for (int i = 0; i < 6; ++i) SWD_CUDA(cudaMemcpyAsync(din + i * NN, hsrc[i], NN * sizeof(T), cudaMemcpyHostToDevice, st));
+  SWD_TRY(pack_materials<T>(din, din + NN, din + 2 * NN, din + 3 * NN, din + 4 * NN, din + 5 * NN, d_m1.as<V>(),
+                            d_m2.as<V>(), NZ, NX, g.pitch, st));
+  // residual: MATLAB nt x ng -> [nt][ng]
+  SWD_CUDA(cudaMemcpyAsync(dstage, res, (size_t)nt * ng * sizeof(T), cudaMemcpyHostToDevice, st));
+  SWD_TRY(transpose<T, T>(dstage, 0, d_res.as<T>(), 0, 1, ng, nt, st));
+  // snapshots: MATLAB nz x nx x nrec per field -> [nrec][f][nz][nx]
+  const T* wf[4] = {fux, fuz, bwx, bwz};
+  for (int f = 0; f < 4; ++f) {
+    SWD_CUDA(cudaMemcpyAsync(din, wf[f], nsnap * sizeof(T), cudaMemcpyHostToDevice, st));
+    SWD_TRY(transpose<T, T>(din, plane, d_snap.as<T>() + f * plane, 4 * plane, g.nrec, nx, nz, st));
+  }
+  SWD_CUDA(cudaMemsetAsync(d_state.p, 0, d_state.bytes, st));
+  SWD_CUDA(cudaMemsetAsync(d_img.p, 0, d_img.bytes, st));
+  AdjArgs<T> a{};
+  a.g = g; a.m1 = d_m1.as<V>(); a.m2 = d_m2.as<V>();
+  a.res = d_res.as<T>(); a.snap = d_snap.as<T>(); a.img = d_img.as<double>();
+  a.dtx = dtx; a.dt = dt; a.n_shots = 1;
+  T* bufs[2] = {d_state.as<T>(), d_state.as<T>() + 5 * g.field};
+  int cur = 0;
+  for (int it = nt - 2; it >= 0; --it) {  // core/eigen_e2drtm_single.cpp:181
+    a.in = bufs[cur];
+    a.out = bufs[cur ^ 1];
+    launch_adj_step<T, 4>(a, it, st);
+    cur ^= 1;
+  }
+  SWD_CUDA(cudaGetLastError());
+  // images [3][nz][nx] (double) -> MATLAB nz x nx each, in the output type
+  SWD_TRY(transpose<double, TO>(d_img.as<double>(), plane, d_out.as<TO>(), plane, 3, nz, nx, st));
+  TO* outs[3] = {cl_img, cm_img, illum};
+  for (int i = 0; i < 3; ++i)
+    SWD_CUDA(cudaMemcpyAsync(outs[i], d_out.as<TO>() + i * plane, plane * sizeof(TO), cudaMemcpyDeviceToHost, st));
+  SWD_CUDA(cudaStreamSynchronize(st));
+  return SWD_OK;
+}
+
+}  // namespace
+}  // namespace swd
+
+using namespace swd;
+
+extern "C" {
+
+const char* swd_last_error(void) { return g_err; }
+int swd_version(void) { return 100; }
+uint64_t swd_kernel_launches(void) { return g_launches.load(); }
+
+int swd_staggerfd_single(const float* iv, int n_iv, const float* temp, const float* ca, const float* cl,
+                         const float* cm, const float* cm1, const float* b, const float* b1, const float* s,
+                         float* seismo_u, float* seismo_w, float* fux, float* fuz, float* bwx, float* bwz) {
+  return staggerfd_mex<float>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, s, seismo_u, seismo_w, fux, fuz, bwx, bwz);
+}
+int swd_staggerfd_double(const double* iv, int n_iv, const double* temp, const double* ca, const double* cl,
+                         const double* cm, const double* cm1, const double* b, const double* b1, const double* s,
+                         double* seismo_u, double* seismo_w, double* fux, double* fuz, double* bwx,
+                         double* bwz) {
+  return staggerfd_mex<double>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, s, seismo_u, seismo_w, fux, fuz, bwx, bwz);
+}
+int swd_e2drtm_single(const float* iv, int n_iv, const float* temp, const float* ca, const float* cl,
+                      const float* cm, const float* cm1, const float* b, const float* b1, const float* seismo_w,
+                      const float* fux, const float* fuz, const float* bwx, const float* bwz, float* cl_img,
+                      float* cm_img, float* illum_div) {
+  return e2drtm_mex<float, float>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, seismo_w, fux, fuz, bwx, bwz, cl_img,
+                                  cm_img, illum_div);
+}
+int swd_e2drtm_single_f64out(const float* iv, int n_iv, const float* temp, const float* ca, const float* cl,
+                             const float* cm, const float* cm1, const float* b, const float* b1,
+                             const float* seismo_w, const float* fux, const float* fuz, const float* bwx,
+                             const float* bwz, double* cl_img, double* cm_img, double* illum_div) {
+  return e2drtm_mex<float, double>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, seismo_w, fux, fuz, bwx, bwz, cl_img,
+                                   cm_img, illum_div);
+}
+int swd_e2drtm_double(const double* iv, int n_iv, const double* temp, const double* ca, const double* cl,
+                      const double* cm, const double* cm1, const double* b, const double* b1,
+                      const double* seismo_w, const double* fux, const double* fuz, const double* bwx,
+                      const double* bwz, double* cl_img, double* cm_img, double* illum_div) {
+  return e2drtm_mex<double, double>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, seismo_w, fux, fuz, bwx, bwz, cl_img,
+                                    cm_img, illum_div);
+}
+
+}  // extern "C"

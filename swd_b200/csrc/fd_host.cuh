@@ -1,0 +1,31 @@
+// Host-side helpers shared by the FD, Radon and batched-engine translation units.
+#pragma once
+#include <algorithm>
+
+#include "swd_common.cuh"
+#include "fd_kernels.cuh"
+
+namespace swd {
+
+void clear_error();
+void count_launch(uint64_t n);
+
+// Batched transpose: out[b*ob + c*R + r] = in[b*ib + r*C + c] for B planes of R x C.
+template <typename Ti, typename To>
+int transpose(const Ti* in, size_t ib, To* out, size_t ob, int B, int R, int C, cudaStream_t st);
+
+// MATLAB column-major materials -> packed row-major {temp,b,b1,0} / {ca,cl,cm1,0}.
+template <typename T>
+int pack_materials(const T* temp, const T* b, const T* b1, const T* ca, const T* cl, const T* cm1,
+                   typename Vec4<T>::type* m1, typename Vec4<T>::type* m2, int NZ, int NX, int pitch,
+                   cudaStream_t st);
+
+// Choose strips/chunks for a launch over n_shots shots (chunk_rows <= 0: heuristic).
+void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows);
+
+template <typename T, int NF>
+int launch_fwd_step(const FwdArgs<T>& a, int it, cudaStream_t st);
+template <typename T, int NF>
+int launch_adj_step(const AdjArgs<T>& a, int it, cudaStream_t st);
+
+}  // namespace swd
