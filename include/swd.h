@@ -90,6 +90,61 @@ int swd_e2drtm_double(const double* iv, int n_iv, const double* temp, const doub
                       const double* fuz, const double* bwx, const double* bwz, double* cl_img,
                       double* cm_img, double* illum_div);
 
+/* Padded FD inputs from (vp, vs), as core/staggerfd_eigen.m:37-107 builds them
+ * (calparam, pad, damp_circle, free-surface row edits), computed on the GPU.
+ * vp, vs: nz x nx (double).  Outputs: nzbc x nxbc with nzbc = nz+pad_top+nbc,
+ * nxbc = nx+2*nbc, pad_top = (fd_order-20)/2+1.  isfs must be 1. */
+int swd_prep_model_single(int nz, int nx, int nbc, int isfs, int fd_order, double dx, double dt, double dtx,
+                          const double* vp, const double* vs, float* temp, float* ca, float* cl, float* cm,
+                          float* cm1, float* b, float* b1);
+int swd_prep_model_double(int nz, int nx, int nbc, int isfs, int fd_order, double dx, double dt, double dtx,
+                          const double* vp, const double* vs, double* temp, double* ca, double* cl, double* cm,
+                          double* cm1, double* b, double* b1);
+
+/* ------------------------------------------------------------------------
+ * Dispersion spectrum, picking and SoftMax gradient (host pointers).
+ * ------------------------------------------------------------------------ */
+
+/* Arguments shared by RTr/RTl/RTrAD/RTlAD (core/RTrAD.m:2) and ADWDgrad_1. */
+typedef struct {
+  double df, dt;       /* frequency step, time step */
+  double fmin, fmax;   /* kept band: bins round(fmin/df)+1 .. round(fmax/df)+1 */
+  double vmin, vmax;   /* phase-velocity axis vmin:dv:vmax */
+  double dv;           /* 1 in the reference (pp=1./(vmin:vmax)') */
+  double ds;           /* trace spacing in metres */
+  int nt, ng;          /* seismogram size (a, b) */
+  int offset, m, M;    /* window length, minimum offset, shot spacing in traces */
+  int precision;       /* SWD_PREC_*; the per-shot entry points compute in FP64 */
+} swd_radon_params;
+
+/* np (velocities), npair (kept bins), lf, nf and ccn = fix(1/df/dt) for p. */
+int swd_radon_sizes(const swd_radon_params* p, int* np, int* npair, int* lf, int* nf, int* ccn);
+
+/* Replaces RTrAD (side 0, core/RTrAD.m:2-35) and RTlAD (side 1, core/RTlAD.m:2-36);
+ * ml is also the output of RTr/RTl (core/RTr.m:2-32, core/RTl.m:2-32).
+ * seismo: nt x ng.  ml, ml_raw: np x npair (ml_raw = saveForBackward.mlr/mll).
+ * mm: np x nf complex, interleaved re/im (saveForBackward.mm).  uxtpos: data_len
+ * 1-based trace columns, ascending (uxtposr/uxtposl).  ml_raw, mm, data_len and
+ * uxtpos may be NULL. */
+int swd_radon(const swd_radon_params* p, int side, int is, const double* seismo, double* ml, double* ml_raw,
+              double* mm, int* data_len, int* uxtpos);
+
+/* Replaces LHDispPick(ml,vmin,cr_0,method,ini) (core/LHDispPick.m:2-13) with the
+ * guided picker pickFDC1(ml,ini,2,4) (core/pickFDC1.m:1-131) for method 1.
+ * ml: np x npair; cr_0, cr_pre: npair; res: scalar misfit (may be NULL). */
+int swd_pick(const double* ml, int np, int npair, double vmin, const double* cr_0, int method, int ini,
+             double* res, double* cr_pre);
+
+/* Replaces ADWDgrad_1(nt,ng,ns,npair,is,w,m,M,SoftArgNorm,grad_outputr,grad_outputl,
+ * space_M,saveForBackwardr,saveForBackwardl) (core/ADWDgrad_1.m:1-81).
+ * grad_output_*: npair; space_m: np x npair (NULL = 1..np per column, SWD.m:133-136);
+ * mm_*: np x nf interleaved complex; ml_raw_*: np x npair; a side the reference
+ * skips for this shot may pass NULLs.  a_data_res: nt x ng (out). */
+int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
+                 const double* grad_output_r, const double* grad_output_l, const double* space_m,
+                 const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
+                 double* a_data_res);
+
 #ifdef __cplusplus
 }
 #endif

@@ -612,12 +612,16 @@ def ADWDgrad_1(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_
 # --------------------------------------------------------------------------------------
 
 def smooth2a(A, Nr, Nc):
-    """core/smooth2a.m:38-76: (2Nr+1)x(2Nc+1) box mean with shrinking edges (finite input)."""
-    A = np.asarray(A, np.float64)
+    """core/smooth2a.m:38-76: (2Nr+1)x(2Nc+1) box mean with shrinking edges; NaNs are left out of
+    the sums and counts and stay NaN in the output."""
+    A = np.array(A, np.float64)
     r, c = A.shape
     eL = (np.abs(np.arange(r)[:, None] - np.arange(r)[None, :]) <= Nr).astype(np.float64)
     eR = (np.abs(np.arange(c)[:, None] - np.arange(c)[None, :]) <= Nc).astype(np.float64)
-    nrm = eL @ np.ones_like(A) @ eR
+    nan = np.isnan(A)
+    A[nan] = 0
+    nrm = eL @ (~nan).astype(np.float64) @ eR
+    nrm[nan] = np.nan
     return (eL @ A @ eR) / nrm
 
 

@@ -20,6 +20,17 @@ _c_int = ctypes.c_int
 _c_dbl = ctypes.c_double
 _vp = ctypes.c_void_p
 
+
+class RadonParams(ctypes.Structure):
+    """swd_radon_params of include/swd.h."""
+    _fields_ = [("df", ctypes.c_double), ("dt", ctypes.c_double), ("fmin", ctypes.c_double),
+                ("fmax", ctypes.c_double), ("vmin", ctypes.c_double), ("vmax", ctypes.c_double),
+                ("dv", ctypes.c_double), ("ds", ctypes.c_double), ("nt", ctypes.c_int), ("ng", ctypes.c_int),
+                ("offset", ctypes.c_int), ("m", ctypes.c_int), ("M", ctypes.c_int), ("precision", ctypes.c_int)]
+
+
+_rpp = ctypes.POINTER(RadonParams)
+
 # name -> argtypes (all return int status unless listed in _RESTYPE)
 _SIGS = {
     "swd_last_error": [],
@@ -32,6 +43,10 @@ _SIGS = {
     "swd_e2drtm_double": [_f64p, _c_int] + [_f64p] * 15,
     "swd_prep_model_single": [_c_int] * 5 + [_c_dbl] * 3 + [_f64p] * 2 + [_f32p] * 7,
     "swd_prep_model_double": [_c_int] * 5 + [_c_dbl] * 3 + [_f64p] * 2 + [_f64p] * 7,
+    "swd_radon_sizes": [_rpp] + [_i32p] * 5,
+    "swd_radon": [_rpp, _c_int, _c_int] + [_f64p] * 4 + [_i32p] * 2,
+    "swd_pick": [_f64p, _c_int, _c_int, _c_dbl, _f64p, _c_int, _c_int, _f64p, _f64p],
+    "swd_adwdgrad": [_rpp, _c_int, _c_int, _c_int, _c_dbl] + [_f64p] * 8,
 }
 _RESTYPE = {"swd_last_error": ctypes.c_char_p, "swd_kernel_launches": ctypes.c_uint64}
 

@@ -26,6 +26,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path
 SOURCES = {
     "fd_host.cu": ["-fmad=false"],
     "model_prep.cu": ["-fmad=false"],
+    "radon.cu": [],
 }
 
 

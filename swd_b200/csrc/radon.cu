@@ -1,0 +1,722 @@
+// Radon dispersion spectrum, guided picker and SoftMax misfit gradient (FP64 path).
+//
+// Reference:  core/RTrAD.m:2-35, core/RTlAD.m:2-36 (spectrum and saved state),
+//             core/LHDispPick.m:2-13 + core/pickFDC1.m:1-131 (picker),
+//             core/ADWDgrad_1.m:1-81 (SoftMax gradient, adjoint Radon, inverse FFT).
+// All gathers of a batch run in one launch per stage.  The DFT evaluates only
+// the bins lf..nf that the reference keeps; the Radon sum runs in double like
+// MATLAB; the SoftMax uses a max-shifted FP64 log-sum-exp.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "fd_host.cuh"
+#include "radon.cuh"
+
+namespace swd {
+
+static int mround(double x) {  // MATLAB round: half away from zero
+  double r = std::floor(std::fabs(x));
+  if (std::fabs(x) - r >= 0.5) r += 1;
+  return (int)std::copysign(r, x);
+}
+
+int radon_geom(const swd_radon_params* p, RadonGeom& g) {
+  SWD_CHECK(p != nullptr, "null radon params");
+  SWD_CHECK(p->df > 0 && p->dt > 0 && p->ds > 0, "df, dt and ds must be positive");
+  SWD_CHECK(p->nt >= 1 && p->ng >= 1, "seismogram must be non-empty");
+  SWD_CHECK(p->offset >= 1 && p->M >= 1 && p->m >= 0, "offset >= 1, M >= 1, m >= 0 required");
+  SWD_CHECK(p->dv > 0 && p->vmax >= p->vmin && p->vmin > 0, "velocity axis vmin:dv:vmax must be positive");
+  g.nt = p->nt; g.ng = p->ng;
+  const double cc = std::trunc(1.0 / p->df / p->dt);  // fix(1./df./dt)
+  SWD_CHECK(cc >= 1 && cc < 2147483647.0, "ccn = fix(1/df/dt) out of range");
+  g.ccn = (int)cc;
+  g.ntd = std::min(g.nt, g.ccn);
+  g.lf = mround(p->fmin / p->df) + 1;
+  g.nf = mround(p->fmax / p->df) + 1;
+  SWD_CHECK(g.lf >= 1 && g.nf >= g.lf && g.nf <= g.ccn, "frequency bins %d..%d outside 1..ccn (%d)", g.lf, g.nf, g.ccn);
+  g.npair = g.nf - g.lf + 1;
+  g.np = (int)std::floor((p->vmax - p->vmin) / p->dv + 1e-9) + 1;
+  g.offset = p->offset; g.m = p->m; g.M = p->M;
+  g.df = p->df; g.dt = p->dt; g.ds = p->ds; g.vmin = p->vmin; g.dv = p->dv;
+  return SWD_OK;
+}
+
+bool side_active(int is, int side, int ns, int m, int M, int w) {
+  // ADWDgrad_1.m:15 (right) and :47 (left); SWD.m:175, 181
+  if (side == 0) return is <= ns - (int)std::floor((double)m / M) - mround((double)w / M);
+  return is >= mround((double)w / M) + (int)std::floor((double)m / M) + 1;
+}
+
+Gather make_gather(const RadonGeom& g, int is, int side, int shot_index, int ns, int w) {
+  Gather r{};
+  r.shot = shot_index;
+  r.side = side;
+  r.valid = side_active(is, side, ns, g.m, g.M, w) ? 1 : 0;
+  if (side == 0) {  // RTrAD.m:4-9
+    const int c0 = g.M * is - g.M + 1 + g.m;
+    const int nend = std::min(g.m + g.offset - 1 + g.M * is - g.M + 1, g.ng);
+    r.c0 = c0 - 1;
+    r.dir = 1;
+    r.noff = nend - c0 + 1;
+  } else {          // RTlAD.m:4-9: fliplr(seismo(:, nend+1 : M*is-M+1-m))
+    int nend = g.M * is - g.M + 1 - g.offset - g.m;
+    if (nend < 1) nend = 0;
+    const int last = g.M * is - g.M + 1 - g.m;
+    r.c0 = last - 1;
+    r.dir = -1;
+    r.noff = last - nend;
+  }
+  if (r.noff < 1 || r.c0 < 0 || r.c0 >= g.ng || r.c0 + r.dir * (r.noff - 1) < 0 ||
+      r.c0 + r.dir * (r.noff - 1) >= g.ng)
+    r.valid = r.valid ? -1 : 0;  // empty or out-of-range window where the reference would compute one
+  return r;
+}
+
+// ------------------------------------------------------------------ tables
+
+__global__ void w_table_kernel(RadonGeom g, double2* W) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x, f = blockIdx.y;
+  if (t >= g.ntd) return;
+  const long long k = g.lf - 1 + f;
+  const long long r = (k * (long long)t) % g.ccn;
+  double s, c;
+  sincospi(2.0 * (double)r / (double)g.ccn, &s, &c);
+  W[(size_t)f * g.ntd + t] = make_double2(c, -s);
+}
+
+__global__ void k_table_kernel(RadonGeom g, double2* K) {
+  const int p = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y, f = blockIdx.z;
+  if (p >= g.np) return;
+  // RTrAD.m:13,20-21: x=(m+(0:off-1))*ds, pp=1./v, ll0 = 1i*2*pi*df*(pp*x), l = exp(ll0*(j-1))
+  const double v = g.vmin + g.dv * p;
+  const double pp = 1.0 / v;
+  const double xx = (g.m + x) * g.ds;
+  const double w0 = 2.0 * 3.141592653589793 * g.df;
+  const double th = (w0 * (pp * xx)) * (double)(g.lf - 1 + f);
+  double s, c;
+  sincos(th, &s, &c);
+  K[((size_t)f * g.offset + x) * g.np + p] = make_double2(c, s);
+}
+
+int radon_tables(const RadonGeom& g, double2* W, double2* K, cudaStream_t st) {
+  if (W) {
+    dim3 grid((g.ntd + 255) / 256, g.npair);
+    w_table_kernel<<<grid, 256, 0, st>>>(g, W);
+    count_launch(1);
+  }
+  if (K) {
+    dim3 grid((g.np + 127) / 128, g.offset, g.npair);
+    k_table_kernel<<<grid, 128, 0, st>>>(g, K);
+    count_launch(1);
+  }
+  SWD_CUDA(cudaGetLastError());
+  return SWD_OK;
+}
+
+// ------------------------------------------------------------------ DFT at the kept bins
+
+constexpr int kDftF = 8, kDftT = 64;
+
+template <typename S>
+__global__ void __launch_bounds__(256) dft_kernel(RadonGeom g, const Gather* gs, const S* seis, size_t sstride,
+                                                  const double2* __restrict__ W, double2* D) {
+  __shared__ double su[kDftT][33];
+  __shared__ double2 sw[kDftF][kDftT];
+  const Gather gg = gs[blockIdx.z];
+  if (gg.valid <= 0) return;
+  const int f0 = blockIdx.x * kDftF, x0 = blockIdx.y * 32;
+  if (x0 >= gg.noff) return;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  const S* src = seis + (size_t)gg.shot * sstride;
+  double2 acc = make_double2(0.0, 0.0);
+  const int f = f0 + wp, x = x0 + lane;
+  for (int t0 = 0; t0 < g.ntd; t0 += kDftT) {
+    for (int i = threadIdx.x; i < kDftT * 32; i += 256) {
+      const int tt = i >> 5, xx = i & 31, t = t0 + tt, xg = x0 + xx;
+      double v = 0.0;
+      if (t < g.ntd && xg < gg.noff) v = (double)src[(size_t)t * g.ng + (gg.c0 + gg.dir * xg)];
+      su[tt][xx] = v;
+    }
+    for (int i = threadIdx.x; i < kDftF * kDftT; i += 256) {
+      const int ff = i / kDftT, tt = i % kDftT, t = t0 + tt, fg = f0 + ff;
+      sw[ff][tt] = (t < g.ntd && fg < g.npair) ? W[(size_t)fg * g.ntd + t] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll 8
+    for (int tt = 0; tt < kDftT; ++tt) {
+      const double u = su[tt][lane];
+      const double2 w = sw[wp][tt];
+      acc.x += w.x * u;
+      acc.y += w.y * u;
+    }
+    __syncthreads();
+  }
+  if (f < g.npair && x < gg.noff) D[((size_t)blockIdx.z * g.npair + f) * g.offset + x] = acc;
+}
+
+template <typename S>
+int radon_dft(const RadonGeom& g, const Gather* d_gath, int G, const S* seis, size_t sstride, const double2* W,
+              double2* D, cudaStream_t st) {
+  dim3 grid((g.npair + kDftF - 1) / kDftF, (g.offset + 31) / 32, G);
+  dft_kernel<S><<<grid, 256, 0, st>>>(g, d_gath, seis, sstride, W, D);
+  count_launch(1);
+  SWD_CUDA(cudaGetLastError());
+  return SWD_OK;
+}
+template int radon_dft<float>(const RadonGeom&, const Gather*, int, const float*, size_t, const double2*, double2*,
+                              cudaStream_t);
+template int radon_dft<double>(const RadonGeom&, const Gather*, int, const double*, size_t, const double2*,
+                               double2*, cudaStream_t);
+
+// ------------------------------------------------------------------ Radon sum, |mm|, column normalisation
+
+__device__ double block_max(double v, double* sm) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  v = threadIdx.x < nw ? sm[threadIdx.x] : -1.0 / 0.0;
+  if (threadIdx.x < 32)
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  if (threadIdx.x == 0) sm[32] = v;
+  __syncthreads();
+  v = sm[32];
+  __syncthreads();
+  return v;
+}
+
+__device__ double block_sum(double v, double* sm) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  v = threadIdx.x < nw ? sm[threadIdx.x] : 0.0;
+  if (threadIdx.x < 32)
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if (threadIdx.x == 0) sm[32] = v;
+  __syncthreads();
+  v = sm[32];
+  __syncthreads();
+  return v;
+}
+
+__global__ void __launch_bounds__(256) contract_kernel(RadonGeom g, const Gather* gs, const double2* __restrict__ K,
+                                                       const double2* __restrict__ D, double2* MM, double* mlraw,
+                                                       double* ml) {
+  extern __shared__ double2 sd[];
+  __shared__ double red[33];
+  const int f = blockIdx.x, gi = blockIdx.y;
+  const Gather gg = gs[gi];
+  if (gg.valid <= 0) return;
+  const size_t col = ((size_t)gi * g.npair + f);
+  for (int x = threadIdx.x; x < gg.noff; x += blockDim.x) sd[x] = D[col * g.offset + x];
+  __syncthreads();
+  const double2* Kf = K + (size_t)f * g.offset * g.np;
+  double mx = -1.0 / 0.0;
+  for (int p = threadIdx.x; p < g.np; p += blockDim.x) {
+    double re = 0.0, im = 0.0;
+    for (int x = 0; x < gg.noff; ++x) {
+      const double2 k = Kf[(size_t)x * g.np + p];
+      const double2 d = sd[x];
+      re += k.x * d.x - k.y * d.y;
+      im += k.x * d.y + k.y * d.x;
+    }
+    MM[col * g.np + p] = make_double2(re, im);
+    const double a = hypot(re, im);
+    mlraw[col * g.np + p] = a;
+    mx = fmax(mx, a);
+  }
+  mx = block_max(mx, red);
+  for (int p = threadIdx.x; p < g.np; p += blockDim.x) ml[col * g.np + p] = mlraw[col * g.np + p] / mx;
+}
+
+int radon_contract(const RadonGeom& g, const Gather* d_gath, int G, const double2* K, const double2* D, double2* MM,
+                   double* mlraw, double* ml, cudaStream_t st) {
+  dim3 grid(g.npair, G);
+  const size_t smem = (size_t)g.offset * sizeof(double2);
+  if (smem > 48 * 1024) SWD_CUDA(cudaFuncSetAttribute(contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  contract_kernel<<<grid, 256, smem, st>>>(g, d_gath, K, D, MM, mlraw, ml);
+  count_launch(1);
+  SWD_CUDA(cudaGetLastError());
+  return SWD_OK;
+}
+
+// ------------------------------------------------------------------ guided picker (one warp per gather)
+
+// First q in (s, e) (1-based, inclusive segment [s, e]) where y has a findpeaks(-y) peak; 0 if none.
+__device__ int first_local_min(const double* y, int s, int e, int lane) {
+  for (int base = s + 1; base < e; base += 32) {
+    const int q = base + lane;
+    bool ok = false;
+    if (q < e) {
+      const double yq = y[q - 1];
+      if (yq < y[q - 2]) {
+        int r = q + 1;
+        while (r <= e && y[r - 1] == yq) ++r;
+        ok = (r <= e) && (y[r - 1] > yq);
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (m) return base + __ffs(m) - 1;
+  }
+  return 0;
+}
+
+// Last such q in (1, e) for the segment [1, e]; 0 if none.
+__device__ int last_local_min(const double* y, int e, int lane) {
+  for (int top = e - 1; top >= 2; top -= 32) {
+    const int q = top - lane;
+    bool ok = false;
+    if (q >= 2) {
+      const double yq = y[q - 1];
+      if (yq < y[q - 2]) {
+        int r = q + 1;
+        while (r <= e && y[r - 1] == yq) ++r;
+        ok = (r <= e) && (y[r - 1] > yq);
+      }
+    }
+    const unsigned m = __ballot_sync(0xffffffffu, ok);
+    if (m) return top - (__ffs(m) - 1);
+  }
+  return 0;
+}
+
+// MATLAB [~,i]=max(y(lo:hi)): first index of the maximum, returned 1-based absolute.
+__device__ int warp_argmax(const double* y, int lo, int hi, int lane) {
+  double bv = -1.0 / 0.0;
+  int bi = 0x7fffffff;
+  for (int q = lo + lane; q <= hi; q += 32) {
+    const double v = y[q - 1];
+    if (v > bv || (v == bv && q < bi)) { bv = v; bi = q; }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+  }
+  return bi;
+}
+
+__global__ void pick_kernel(int np, int npair, int G, int lp, int method, double fg, double lfg, double vmin,
+                            const double* ml, const double* cr0, double* cr_pre, double* dc, double* res,
+                            int* status) {
+  extern __shared__ int psm[];
+  const int gi = blockIdx.x;
+  const int lane = threadIdx.x;
+  int* idx = psm;                  // 1-based column arrays, entry 0 unused
+  int* dvmin = idx + (npair + 1);
+  int* dvmax = dvmin + (npair + 1);
+  int* chazhi = dvmax + (npair + 1);
+  double* qj = (double*)(psm + 4 * (npair + 1));  // 16*(npair+1) bytes in: 8-byte aligned
+  const double* mlg = ml + (size_t)gi * npair * np;
+  auto col = [&](int i) { return mlg + (size_t)(i - 1) * np; };
+  const int a = np, b = npair;
+  // NaN columns are not supported (findpeaks semantics would need them)
+  bool bad = false;
+  for (int i = lane; i < np * npair; i += 32) bad |= isnan(mlg[i]);
+  if (__any_sync(0xffffffffu, bad)) {
+    if (lane == 0) status[gi] = 1;
+    return;
+  }
+  double* crp = cr_pre + (size_t)gi * npair;
+  if (method != 1) {  // LHDispPick.m:8-9: plain argmax per column
+    for (int i = 1; i <= b; ++i) {
+      const int q = warp_argmax(col(i), 1, a, lane);
+      if (lane == 0) crp[i - 1] = q + vmin;
+    }
+  } else {
+    for (int i = lane; i <= b; i += 32) { idx[i] = 0; dvmin[i] = 0; dvmax[i] = 0; chazhi[i] = 1; qj[i] = 0.0 / 0.0; }
+    __syncwarp();
+    const double nanv = 0.0 / 0.0;
+    int cur = warp_argmax(col(lp), 1, a, lane);  // pickFDC1.m:19
+    if (lane == 0) idx[lp] = cur;
+    for (int i = lp - 1; i >= 1; --i) {          // pickFDC1.m:21-77
+      __syncwarp();
+      const int prev = idx[i + 1];
+      if (prev == a) {
+        if (lane == 0) { idx[i] = a; dvmax[i] = dvmax[i + 1]; dvmin[i] = dvmin[i + 1]; qj[i] = nanv; }
+        continue;
+      }
+      int vmx, vmn;
+      if (prev > a - 3) vmx = a;
+      else { const int q = first_local_min(col(i), prev, a, lane); vmx = q ? q + 1 : a; }
+      if (prev < 3) vmn = 1;
+      else { const int q = last_local_min(col(i), prev, lane); vmn = q ? q : 1; }
+      const double qi = (double)(vmx - vmn);
+      const double qn = qj[i + 1];
+      int newidx;
+      if (qi > qn * lfg) {  // NaN compares false
+        newidx = prev;
+        vmx = dvmax[i + 1];
+        vmn = dvmin[i + 1];
+        if (lane == 0) { chazhi[i] = 0; }
+      } else {
+        newidx = warp_argmax(col(i), vmn, vmx, lane);
+      }
+      __syncwarp();
+      if (lane == 0) { idx[i] = newidx; dvmax[i] = vmx; dvmin[i] = vmn; qj[i] = (double)(vmx - vmn); }
+    }
+    for (int i = lp + 1; i <= b; ++i) {          // pickFDC1.m:79-128
+      __syncwarp();
+      const int prev = idx[i - 1];
+      int vmx, vmn;
+      if (prev > a - 3) vmx = a;
+      else { const int q = first_local_min(col(i), prev, a, lane); vmx = q ? q + 1 : a; }
+      if (prev < 3) vmn = 1;
+      else { const int q = last_local_min(col(i), prev, lane); vmn = q ? q : 1; }
+      const double qi = (double)(vmx - vmn);
+      const double qp = qj[i - 1];
+      int newidx;
+      if (qi > fg * qp) {
+        newidx = prev;
+        vmx = dvmax[i - 1];
+        vmn = dvmin[i - 1];
+        if (lane == 0) chazhi[i] = 0;
+      } else {
+        newidx = warp_argmax(col(i), vmn, vmx, lane);
+      }
+      __syncwarp();
+      if (lane == 0) { idx[i] = newidx; dvmax[i] = vmx; dvmin[i] = vmn; qj[i] = (double)(vmx - vmn); }
+    }
+    __syncwarp();
+    if (lane == 0) {  // pickFDC1.m:129-131: linear interp over held columns, then nearest + extrap
+      int nq = 0, qfirst = 0, qlast = 0;
+      for (int i = 1; i <= b; ++i)
+        if (chazhi[i] == 1) { if (!nq) qfirst = i; qlast = i; ++nq; }
+      if (nq < 2) {
+        status[gi] = 2;
+      } else {
+        int k0 = qfirst;
+        for (int t = 1; t <= b; ++t) {
+          double v;
+          if (t <= qfirst) v = idx[qfirst];
+          else if (t >= qlast) v = idx[qlast];
+          else {
+            while (true) {  // advance to the retained sample interval [k0, k1] containing t
+              int k1 = k0 + 1;
+              while (chazhi[k1] != 1) ++k1;
+              if (t < k1) break;
+              k0 = k1;
+            }
+            int k1 = k0 + 1;
+            while (chazhi[k1] != 1) ++k1;
+            if (t == k0) v = idx[k0];
+            else {
+              const double x0 = k0, x1 = k1, y0 = idx[k0], y1 = idx[k1];
+              v = y0 + ((double)t - x0) * ((y1 - y0) / (x1 - x0));
+            }
+          }
+          crp[t - 1] = v + vmin;
+        }
+      }
+    }
+  }
+  __syncwarp();
+  if (lane == 0 && status[gi] == 0) {
+    double s = 0.0;
+    for (int i = 0; i < b; ++i) {
+      const double d = crp[i] - cr0[(size_t)gi * npair + i];
+      dc[(size_t)gi * npair + i] = d;
+      s += d * d;
+    }
+    res[gi] = s / b;
+  }
+}
+
+int pick_batch(int np, int npair, int G, int ini, int method, double vmin, const double* ml, const double* cr0,
+               double* cr_pre, double* dc, double* res, int* status, cudaStream_t st) {
+  SWD_CHECK(ini >= 1 && ini <= npair, "ini (%d) must lie in 1..npair (%d)", ini, npair);
+  const size_t smem = (size_t)(npair + 1) * (4 * sizeof(int) + sizeof(double));
+  SWD_CUDA(cudaMemsetAsync(status, 0, G * sizeof(int), st));
+  pick_kernel<<<G, 32, smem, st>>>(np, npair, G, ini, method, 2.0, 4.0, vmin, ml, cr0, cr_pre, dc, res, status);
+  count_launch(1);
+  SWD_CUDA(cudaGetLastError());
+  return SWD_OK;
+}
+
+// ------------------------------------------------------------------ SoftMax gradient + adjoint Radon
+
+__global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const Gather* gs,
+                                                              const double* __restrict__ mlraw,
+                                                              const double2* __restrict__ MM,
+                                                              const double* __restrict__ dc,
+                                                              const double* __restrict__ space_m, double beta,
+                                                              const double2* __restrict__ K, double2* Gx) {
+  extern __shared__ double2 sgm[];
+  __shared__ double red[33];
+  const int f = blockIdx.x, gi = blockIdx.y;
+  const Gather gg = gs[gi];
+  if (gg.valid <= 0) return;
+  const size_t col = (size_t)gi * g.npair + f;
+  const double* mr = mlraw + col * g.np;
+  // E = softmax(beta * mlr.^(1/40)) over p (ADWDgrad_1.m:22-23), max-shifted in FP64
+  double zmax = -1.0 / 0.0;
+  for (int p = threadIdx.x; p < g.np; p += blockDim.x) zmax = fmax(zmax, pow(mr[p], 1.0 / 40.0) * beta);
+  zmax = block_max(zmax, red);
+  double se = 0.0;
+  for (int p = threadIdx.x; p < g.np; p += blockDim.x) se += exp(pow(mr[p], 1.0 / 40.0) * beta - zmax);
+  se = block_sum(se, red);
+  double sm = 0.0;
+  for (int p = threadIdx.x; p < g.np; p += blockDim.x) {
+    const double E = exp(pow(mr[p], 1.0 / 40.0) * beta - zmax) / se;
+    const double s = space_m ? space_m[(size_t)f * g.np + p] : (double)(p + 1);
+    sm += s * E;
+  }
+  sm = block_sum(sm, red);
+  double d = dc[(size_t)gi * g.npair + f];
+  if (d == 0.0) d = 1.0;  // grad_output(grad_output==0)=1 (ADWDgrad_1.m:26)
+  for (int p = threadIdx.x; p < g.np; p += blockDim.x) {
+    const double E = exp(pow(mr[p], 1.0 / 40.0) * beta - zmax) / se;
+    const double s = space_m ? space_m[(size_t)f * g.np + p] : (double)(p + 1);
+    const double gml = (((E * s - sm * E) * 2.0) * d) * beta;   // :28-31
+    const double2 m = MM[col * g.np + p];
+    const double mag = hypot(m.x, m.y);
+    double2 ph = make_double2(m.x / mag, m.y / mag);              // :32-33
+    if (isnan(ph.x) || isnan(ph.y)) ph = make_double2(0.0, 0.0);
+    sgm[p] = make_double2(ph.x * gml, ph.y * gml);
+  }
+  __syncthreads();
+  // G(x) = sum_p conj(K_f(p,x)) gm(p)   (:36-40)
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const double2* Kf = K + (size_t)f * g.offset * g.np;
+  for (int x = wp; x < gg.noff; x += nw) {
+    double re = 0.0, im = 0.0;
+    for (int p = lane; p < g.np; p += 32) {
+      const double2 k = Kf[(size_t)x * g.np + p];
+      const double2 v = sgm[p];
+      re += k.x * v.x + k.y * v.y;
+      im += k.x * v.y - k.y * v.x;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      re += __shfl_xor_sync(0xffffffffu, re, o);
+      im += __shfl_xor_sync(0xffffffffu, im, o);
+    }
+    if (lane == 0) Gx[col * g.offset + x] = make_double2(re, im);
+  }
+}
+
+int softmax_adjoint(const RadonGeom& g, const Gather* d_gath, int G, const double* mlraw, const double2* MM,
+                    const double* dc, const double* space_m, double beta, const double2* K, double2* Gx,
+                    cudaStream_t st) {
+  dim3 grid(g.npair, G);
+  const size_t smem = (size_t)g.np * sizeof(double2);
+  if (smem > 48 * 1024)
+    SWD_CUDA(cudaFuncSetAttribute(softmax_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  softmax_adjoint_kernel<<<grid, 256, smem, st>>>(g, d_gath, mlraw, MM, dc, space_m, beta, K, Gx);
+  count_launch(1);
+  SWD_CUDA(cudaGetLastError());
+  return SWD_OK;
+}
+
+// ------------------------------------------------------------------ inverse DFT into the adjoint source
+
+constexpr int kIdftT = 64;
+
+template <typename O>
+__global__ void __launch_bounds__(256) idft_kernel(RadonGeom g, const Gather* gs, const double2* __restrict__ Gx,
+                                                   const double2* __restrict__ W, O* out, size_t ostride) {
+  extern __shared__ double2 sg[];  // [npair][32]
+  const Gather gg = gs[blockIdx.z];
+  if (gg.valid <= 0) return;
+  const int x0 = blockIdx.y * 32;
+  if (x0 >= gg.noff) return;
+  const int lane = threadIdx.x & 31, wp = threadIdx.x >> 5;
+  const int x = x0 + lane;
+  for (int i = threadIdx.x; i < g.npair * 32; i += blockDim.x) {
+    const int f = i >> 5, xx = x0 + (i & 31);
+    sg[i] = xx < gg.noff ? Gx[((size_t)blockIdx.z * g.npair + f) * g.offset + xx] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  const int t0 = blockIdx.x * kIdftT;
+  const double inv = (double)g.ccn;
+  // ADWDgrad_1.m:76 writes the left side without its source trace (x = 0)
+  const bool write = x < gg.noff && !(gg.side == 1 && x == 0);
+  const int colx = gg.c0 + gg.dir * x;
+  O* o = out + (size_t)gg.shot * ostride;
+  for (int tt = wp; tt < kIdftT; tt += 8) {
+    const int t = t0 + tt;
+    if (t >= g.nt) break;
+    double acc = 0.0;
+    for (int f = 0; f < g.npair; ++f) {
+      const double2 w = W[(size_t)f * g.ntd + t];  // exp(-i th); ifft uses exp(+i th) = conj(w)
+      const double2 v = sg[f * 32 + lane];
+      acc += v.x * w.x + v.y * w.y;
+    }
+    if (write) o[(size_t)t * g.ng + colx] = (O)(acc / inv);
+  }
+}
+
+template <typename O>
+int radon_idft_scatter(const RadonGeom& g, const Gather* d_gath, int G, const double2* Gx, const double2* W, O* out,
+                       size_t ostride, cudaStream_t st) {
+  SWD_CHECK(g.ccn >= g.nt, "ADWDgrad_1 needs ccn = fix(1/df/dt) (%d) >= nt (%d)", g.ccn, g.nt);
+  dim3 grid((g.nt + kIdftT - 1) / kIdftT, (g.offset + 31) / 32, G);
+  const size_t smem = (size_t)g.npair * 32 * sizeof(double2);
+  if (smem > 48 * 1024)
+    SWD_CUDA(cudaFuncSetAttribute(idft_kernel<O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  idft_kernel<O><<<grid, 256, smem, st>>>(g, d_gath, Gx, W, out, ostride);
+  count_launch(1);
+  SWD_CUDA(cudaGetLastError());
+  return SWD_OK;
+}
+template int radon_idft_scatter<float>(const RadonGeom&, const Gather*, int, const double2*, const double2*, float*,
+                                       size_t, cudaStream_t);
+template int radon_idft_scatter<double>(const RadonGeom&, const Gather*, int, const double2*, const double2*,
+                                        double*, size_t, cudaStream_t);
+
+}  // namespace swd
+
+// ====================================================================== C ABI (host pointers)
+
+using namespace swd;
+
+extern "C" {
+
+int swd_radon_sizes(const swd_radon_params* p, int* np_out, int* npair, int* lf, int* nf, int* ccn) {
+  clear_error();
+  RadonGeom g{};
+  SWD_TRY(radon_geom(p, g));
+  if (np_out) *np_out = g.np;
+  if (npair) *npair = g.npair;
+  if (lf) *lf = g.lf;
+  if (nf) *nf = g.nf;
+  if (ccn) *ccn = g.ccn;
+  return SWD_OK;
+}
+
+int swd_radon(const swd_radon_params* p, int side, int is, const double* seismo, double* ml, double* ml_raw,
+              double* mm, int* data_len, int* uxtpos) {
+  clear_error();
+  RadonGeom g{};
+  SWD_TRY(radon_geom(p, g));
+  SWD_CHECK(side == 0 || side == 1, "side must be 0 (right, RTrAD) or 1 (left, RTlAD)");
+  SWD_CHECK(seismo && ml, "null seismo/ml");
+  Gather gg = make_gather(g, is, side, 0, 1 << 30, 0);
+  SWD_CHECK(gg.noff >= 1 && gg.c0 >= 0 && gg.c0 < g.ng && gg.c0 + gg.dir * (gg.noff - 1) >= 0 &&
+                gg.c0 + gg.dir * (gg.noff - 1) < g.ng,
+            "shot %d has an empty or out-of-range %s window", is, side ? "left" : "right");
+  gg.valid = 1;
+  const size_t nsz = (size_t)g.nt * g.ng, spec = (size_t)g.npair * g.np;
+  DevBuf b_seis, b_seis_t, b_W, b_K, b_D, b_MM, b_raw, b_ml, b_g;
+  SWD_TRY(b_seis.alloc(nsz * sizeof(double)));
+  SWD_TRY(b_seis_t.alloc(nsz * sizeof(double)));
+  SWD_TRY(b_W.alloc((size_t)g.npair * g.ntd * sizeof(double2)));
+  SWD_TRY(b_K.alloc((size_t)g.npair * g.offset * g.np * sizeof(double2)));
+  SWD_TRY(b_D.alloc((size_t)g.npair * g.offset * sizeof(double2)));
+  SWD_TRY(b_MM.alloc(spec * sizeof(double2)));
+  SWD_TRY(b_raw.alloc(spec * sizeof(double)));
+  SWD_TRY(b_ml.alloc(spec * sizeof(double)));
+  SWD_TRY(b_g.alloc(sizeof(Gather)));
+  cudaStream_t st = 0;
+  SWD_CUDA(cudaMemcpyAsync(b_seis.p, seismo, nsz * sizeof(double), cudaMemcpyHostToDevice, st));
+  SWD_CUDA(cudaMemcpyAsync(b_g.p, &gg, sizeof(Gather), cudaMemcpyHostToDevice, st));
+  SWD_TRY(transpose<double, double>(b_seis.as<double>(), 0, b_seis_t.as<double>(), 0, 1, g.ng, g.nt, st));
+  SWD_TRY(radon_tables(g, b_W.as<double2>(), b_K.as<double2>(), st));
+  SWD_TRY(radon_dft<double>(g, b_g.as<Gather>(), 1, b_seis_t.as<double>(), 0, b_W.as<double2>(), b_D.as<double2>(), st));
+  SWD_TRY(radon_contract(g, b_g.as<Gather>(), 1, b_K.as<double2>(), b_D.as<double2>(), b_MM.as<double2>(),
+                         b_raw.as<double>(), b_ml.as<double>(), st));
+  SWD_CUDA(cudaMemcpyAsync(ml, b_ml.p, spec * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (ml_raw) SWD_CUDA(cudaMemcpyAsync(ml_raw, b_raw.p, spec * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (mm) {  // np x nf interleaved complex, columns before lf are zero (RTrAD.m:22)
+    std::memset(mm, 0, (size_t)(g.lf - 1) * g.np * 2 * sizeof(double));
+    SWD_CUDA(cudaMemcpyAsync(mm + (size_t)(g.lf - 1) * g.np * 2, b_MM.p, spec * sizeof(double2),
+                             cudaMemcpyDeviceToHost, st));
+  }
+  SWD_CUDA(cudaStreamSynchronize(st));
+  if (data_len) *data_len = gg.noff;
+  if (uxtpos) {  // RTrAD.m:33 / RTlAD.m:34, ascending 1-based
+    for (int x = 0; x < gg.noff; ++x) {
+      const int c = gg.c0 + gg.dir * x + 1;
+      uxtpos[side == 0 ? x : gg.noff - 1 - x] = c;
+    }
+  }
+  return SWD_OK;
+}
+
+int swd_pick(const double* ml, int np_, int npair, double vmin, const double* cr_0, int method, int ini, double* res,
+             double* cr_pre) {
+  clear_error();
+  SWD_CHECK(ml && cr_0 && cr_pre && np_ >= 1 && npair >= 1, "bad pick arguments");
+  const size_t spec = (size_t)np_ * npair;
+  DevBuf b;
+  SWD_TRY(b.alloc((spec + 3 * (size_t)npair + 1) * sizeof(double) + sizeof(int)));
+  double* d_ml = b.as<double>();
+  double* d_cr0 = d_ml + spec;
+  double* d_crp = d_cr0 + npair;
+  double* d_dc = d_crp + npair;
+  double* d_res = d_dc + npair;
+  int* d_st = (int*)(d_res + 1);
+  cudaStream_t st = 0;
+  SWD_CUDA(cudaMemcpyAsync(d_ml, ml, spec * sizeof(double), cudaMemcpyHostToDevice, st));
+  SWD_CUDA(cudaMemcpyAsync(d_cr0, cr_0, npair * sizeof(double), cudaMemcpyHostToDevice, st));
+  SWD_TRY(pick_batch(np_, npair, 1, ini, method, vmin, d_ml, d_cr0, d_crp, d_dc, d_res, d_st, st));
+  int status = 0;
+  SWD_CUDA(cudaMemcpyAsync(&status, d_st, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SWD_CUDA(cudaMemcpyAsync(cr_pre, d_crp, npair * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (res) SWD_CUDA(cudaMemcpyAsync(res, d_res, sizeof(double), cudaMemcpyDeviceToHost, st));
+  SWD_CUDA(cudaStreamSynchronize(st));
+  if (status == 1) { set_error("NaN in the dispersion spectrum"); return SWD_ERR_NUMERIC; }
+  if (status == 2) { set_error("interp1 needs at least two retained picks (pickFDC1.m:129)"); return SWD_ERR_NUMERIC; }
+  return SWD_OK;
+}
+
+int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm, const double* grad_output_r,
+                 const double* grad_output_l, const double* space_m, const double* mm_r, const double* ml_raw_r,
+                 const double* mm_l, const double* ml_raw_l, double* a_data_res) {
+  clear_error();
+  RadonGeom g{};
+  SWD_TRY(radon_geom(p, g));
+  SWD_CHECK(a_data_res, "null a_data_res");
+  SWD_CHECK(g.ccn >= g.nt, "ADWDgrad_1 needs ccn = fix(1/df/dt) (%d) >= nt (%d)", g.ccn, g.nt);
+  Gather gg[2];
+  const double* mm[2] = {mm_r, mm_l};
+  const double* raw[2] = {ml_raw_r, ml_raw_l};
+  const double* go[2] = {grad_output_r, grad_output_l};
+  for (int s = 0; s < 2; ++s) {
+    gg[s] = make_gather(g, is, s, 0, ns, w);
+    if (gg[s].valid) {
+      SWD_CHECK(gg[s].valid == 1, "shot %d: %s window is empty", is, s ? "left" : "right");
+      SWD_CHECK(mm[s] && raw[s] && go[s], "missing saved state for the %s side", s ? "left" : "right");
+    }
+  }
+  const size_t spec = (size_t)g.npair * g.np, nsz = (size_t)g.nt * g.ng;
+  DevBuf b_W, b_K, b_MM, b_raw, b_dc, b_sm, b_Gx, b_out, b_out_t, b_g;
+  SWD_TRY(b_W.alloc((size_t)g.npair * g.ntd * sizeof(double2)));
+  SWD_TRY(b_K.alloc((size_t)g.npair * g.offset * g.np * sizeof(double2)));
+  SWD_TRY(b_MM.alloc(2 * spec * sizeof(double2)));
+  SWD_TRY(b_raw.alloc(2 * spec * sizeof(double)));
+  SWD_TRY(b_dc.alloc(2 * (size_t)g.npair * sizeof(double)));
+  SWD_TRY(b_Gx.alloc(2 * (size_t)g.npair * g.offset * sizeof(double2)));
+  SWD_TRY(b_out.alloc(nsz * sizeof(double)));
+  SWD_TRY(b_out_t.alloc(nsz * sizeof(double)));
+  SWD_TRY(b_g.alloc(2 * sizeof(Gather)));
+  if (space_m) SWD_TRY(b_sm.alloc(spec * sizeof(double)));
+  cudaStream_t st = 0;
+  for (int s = 0; s < 2; ++s) {
+    if (gg[s].valid != 1) continue;
+    SWD_CUDA(cudaMemcpyAsync(b_MM.as<double2>() + s * spec, mm[s] + (size_t)(g.lf - 1) * g.np * 2,
+                             spec * sizeof(double2), cudaMemcpyHostToDevice, st));
+    SWD_CUDA(cudaMemcpyAsync(b_raw.as<double>() + s * spec, raw[s], spec * sizeof(double), cudaMemcpyHostToDevice, st));
+    SWD_CUDA(cudaMemcpyAsync(b_dc.as<double>() + s * g.npair, go[s], g.npair * sizeof(double),
+                             cudaMemcpyHostToDevice, st));
+  }
+  if (space_m) SWD_CUDA(cudaMemcpyAsync(b_sm.p, space_m, spec * sizeof(double), cudaMemcpyHostToDevice, st));
+  gg[0].shot = 0;
+  gg[1].shot = 0;
+  SWD_CUDA(cudaMemcpyAsync(b_g.p, gg, 2 * sizeof(Gather), cudaMemcpyHostToDevice, st));
+  SWD_CUDA(cudaMemsetAsync(b_out.p, 0, nsz * sizeof(double), st));
+  SWD_TRY(radon_tables(g, b_W.as<double2>(), b_K.as<double2>(), st));
+  SWD_TRY(softmax_adjoint(g, b_g.as<Gather>(), 2, b_raw.as<double>(), b_MM.as<double2>(), b_dc.as<double>(),
+                          space_m ? b_sm.as<double>() : nullptr, soft_arg_norm, b_K.as<double2>(),
+                          b_Gx.as<double2>(), st));
+  SWD_TRY(radon_idft_scatter<double>(g, b_g.as<Gather>(), 2, b_Gx.as<double2>(), b_W.as<double2>(),
+                                     b_out.as<double>(), 0, st));
+  // [nt][ng] -> MATLAB nt x ng
+  SWD_TRY(transpose<double, double>(b_out.as<double>(), 0, b_out_t.as<double>(), 0, 1, g.nt, g.ng, st));
+  SWD_CUDA(cudaMemcpyAsync(a_data_res, b_out_t.p, nsz * sizeof(double), cudaMemcpyDeviceToHost, st));
+  SWD_CUDA(cudaStreamSynchronize(st));
+  return SWD_OK;
+}
+
+}  // extern "C"

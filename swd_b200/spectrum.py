@@ -1,0 +1,112 @@
+"""Dispersion spectrum, picking and SoftMax gradient behind the reference's .m interfaces.
+
+    RTr / RTl / RTrAD / RTlAD   core/RTr.m:2, core/RTl.m:2, core/RTrAD.m:2, core/RTlAD.m:2
+    LHDispPick                  core/LHDispPick.m:2 (pickFDC1, core/pickFDC1.m:1)
+    ADWDgrad_1                  core/ADWDgrad_1.m:1
+
+Each call runs on the GPU through libswd.so (FP64, like the reference's MATLAB
+code).  Arrays use MATLAB's layout; saveForBackward is a dict with the
+reference's field names plus the transform parameters.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import RadonParams, call, ptr
+
+
+def radon_params(df, dt, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0) -> RadonParams:
+    return RadonParams(float(df), float(dt), float(fmin), float(fmax), float(vmin), float(vmax), float(dv),
+                       float(ds), int(a), int(b), int(offset), int(m), int(M), 0)
+
+
+def sizes(p: RadonParams):
+    out = [ctypes.c_int() for _ in range(5)]
+    call("swd_radon_sizes", ctypes.byref(p), *[ctypes.byref(o) for o in out])
+    return tuple(o.value for o in out)  # np, npair, lf, nf, ccn
+
+
+def _radon(side, seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv):
+    seis = np.asfortranarray(np.asarray(seismo_v1, np.float64))
+    if seis.shape != (int(a), int(b)):
+        raise ValueError(f"seismogram is {seis.shape}, expected a x b = {(a, b)}")
+    p = radon_params(df, dt, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv)
+    nv, npair, lf, nf, ccn = sizes(p)
+    if np_ is not None and int(np_) != nv:
+        raise ValueError(f"np={np_} but the velocity axis has {nv} entries")
+    ml = np.zeros((nv, npair), order="F")
+    raw = np.zeros((nv, npair), order="F")
+    mm = np.zeros((nv, nf), np.complex128, order="F")
+    n = ctypes.c_int()
+    pos = np.zeros(int(offset) + 1, np.int32)
+    call("swd_radon", ctypes.byref(p), side, int(is_), ptr(seis), ptr(ml), ptr(raw),
+         mm.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), ctypes.byref(n), ptr(pos))
+    pos = pos[: n.value].astype(np.float64)
+    v = float(vmin) + float(dv) * np.arange(nv)
+    x = (int(m) + np.arange(n.value)) * float(ds)
+    save = {"mm": mm, "ll0": 1j * (2 * np.pi * float(df)) * np.outer(1.0 / v, x), "lf": lf, "nf": nf, "ccn": ccn,
+            ("mlr" if side == 0 else "mll"): raw, ("uxtposr" if side == 0 else "uxtposl"): pos, "params": p}
+    return ml, n.value, save
+
+
+def RTrAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0):
+    """[ml,dataLen,saveForBackward]=RTrAD(...) (core/RTrAD.m:2)."""
+    return _radon(0, seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv)
+
+
+def RTlAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0):
+    """[ml,dataLen,saveForBackward]=RTlAD(...) (core/RTlAD.m:2)."""
+    return _radon(1, seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv)
+
+
+def RTr(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0):
+    """[ml,dataLen]=RTr(...) (core/RTr.m:2)."""
+    ml, n, _ = RTrAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv)
+    return ml, n
+
+
+def RTl(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0):
+    """[ml,dataLen]=RTl(...) (core/RTl.m:2)."""
+    ml, n, _ = RTlAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv)
+    return ml, n
+
+
+def LHDispPick(ml, vmin, cr_0, method=1, ini=10):
+    """[res,cr_pre]=LHDispPick(ml,vmin,cr_0,method,ini) (core/LHDispPick.m:2)."""
+    ml = np.asfortranarray(np.asarray(ml, np.float64))
+    nv, npair = ml.shape
+    cr0 = np.ascontiguousarray(np.broadcast_to(np.asarray(cr_0, np.float64).reshape(-1), (npair,)))
+    cr = np.zeros(npair)
+    res = ctypes.c_double()
+    call("swd_pick", ptr(ml), nv, npair, float(vmin), ptr(cr0), int(method), int(ini), ctypes.byref(res), ptr(cr))
+    return res.value, cr
+
+
+def ADWDgrad_1(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
+               saveForBackwardr, saveForBackwardl):
+    """[a_data_res]=ADWDgrad_1(...) (core/ADWDgrad_1.m:1)."""
+    sr = saveForBackwardr if isinstance(saveForBackwardr, dict) else None
+    sl = saveForBackwardl if isinstance(saveForBackwardl, dict) else None
+    p = (sr or sl)["params"]
+    if int(p.nt) != int(nt) or int(p.ng) != int(ng) or int(p.m) != int(m) or int(p.M) != int(M):
+        raise ValueError("nt/ng/m/M differ from the ones the spectrum was computed with")
+    a = np.zeros((int(nt), int(ng)), order="F")
+    dp = ctypes.POINTER(ctypes.c_double)
+
+    def side(s, go, rawkey):
+        if s is None:
+            return None, None, None
+        mm = np.asfortranarray(s["mm"].astype(np.complex128))
+        raw = np.asfortranarray(np.asarray(s[rawkey], np.float64))
+        g = np.ascontiguousarray(np.asarray(go, np.float64).reshape(-1)[: int(npair)])
+        return mm, raw, g
+
+    mmr, rawr, gr = side(sr, grad_outputr, "mlr")
+    mml, rawl, gl = side(sl, grad_outputl, "mll")
+    spm = None if space_M is None else np.asfortranarray(np.asarray(space_M, np.float64))
+    cp = lambda x: None if x is None else x.ctypes.data_as(dp)
+    call("swd_adwdgrad", ctypes.byref(p), int(ns), int(is_), int(w), float(SoftArgNorm), cp(gr), cp(gl), cp(spm),
+         cp(mmr), cp(rawr), cp(mml), cp(rawl), ptr(a))
+    return a
