@@ -145,6 +145,90 @@ int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_a
                  const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
                  double* a_data_res);
 
+/* ------------------------------------------------------------------------
+ * Batched gradient engine: the per-iteration shot loops of SWD.m run as one
+ * batched GPU pipeline (replaces the parfor loops SWD.m:155-162 observed curves,
+ * SWD.m:171-201 gradient, SWD.m:215-304 forward-only misfits).
+ * ------------------------------------------------------------------------ */
+
+typedef struct swd_engine swd_engine;
+
+/* Survey of one inversion (the top-of-file variables of SWD.m:73-116).
+ * Positions are the reference's 1-based model coordinates. */
+typedef struct {
+  int nz, nx, nbc, nt, nt_wf, fd_order, isfs, source_type; /* source_type 1..5 ('w' = 5) */
+  double dx, dt;
+  int ns;
+  const int* sx; /* ns shot columns */
+  const int* sz; /* ns shot rows */
+  int ng, gx0, dgx, gz; /* receivers gx0, gx0+dgx, ... on row gz */
+  double df, fmin, fmax, vmin, vmax, dv; /* Radon axes (dv = 1 in the reference) */
+  int offset, m, M, w, ini, pick_method;
+  double soft_arg_norm;  /* SoftArgNorm, 1e4 in SWD.m:114 */
+  int smooth_z, smooth_x;
+} swd_survey;
+
+typedef struct {
+  size_t hbm_budget;  /* bytes the engine may allocate (0: 92% of free memory) */
+  int max_batch;      /* shots per batch (0: as many as fit) */
+  int snapshot_mode;  /* 0 auto, 1 keep every strain snapshot, 2 checkpoint + recompute */
+  int ckpt_interval;  /* steps between forward checkpoints (mode 2; rounded to nt_wf) */
+  int use_graphs;     /* capture the time loops in CUDA graphs */
+  int chunk_rows;     /* rows per warp in the FD kernels (0: heuristic) */
+  int device;
+} swd_engine_opts;
+
+typedef struct {
+  int batch, nbatch, mode, ckpt_interval;
+  size_t bytes;
+  int npair, np, ccn, nzbc, nxbc, chunk_rows;
+} swd_engine_info_t;
+
+/* Gradient outputs (host pointers, nz x nx column-major; NULL entries skipped). */
+typedef struct {
+  double* g_cl;      /* sum over shots of cl_img (SWD.m:193) */
+  double* g_cm;      /* sum over shots of cm_img */
+  double* g_illum;   /* sum over shots of illum_div */
+  double* dk_vs;     /* smooth2a(-4 vs g_cl/g_illum + 2 vs g_cm/g_illum) (SWD.m:199-201) */
+  double* res_r;     /* ns: right-side misfits (NaN where skipped) */
+  double* res_l;     /* ns: left-side misfits */
+  double* cr_pre_r;  /* npair x ns predicted picks */
+  double* cr_pre_l;
+  double residual;   /* mean(res_r) over the right-side shots (SWD.m:196) */
+} swd_gradient_out;
+
+int swd_engine_create(const swd_survey* survey, const swd_engine_opts* opts, swd_engine** out);
+int swd_engine_destroy(swd_engine* e);
+int swd_engine_info(const swd_engine* e, swd_engine_info_t* info);
+/* Source wavelet s (nt samples), rounded to float as SWD_single.m:92 does. */
+int swd_engine_set_source(swd_engine* e, const double* s);
+/* Observed picks cr_0 / cr_0l (npair x ns), as SWD.m:155-162 computes them. */
+int swd_engine_set_observed(swd_engine* e, const double* cr0_r, const double* cr0_l);
+/* Observed curves of a model (SWD.m:155-162): forward, RTr/RTl, LHDispPick. */
+int swd_engine_observed_curves(swd_engine* e, const double* vp, const double* vs, double* cr0_r, double* cr0_l);
+/* Forward-only misfits of a model (the line-search passes, SWD.m:215-228). */
+int swd_engine_misfit(swd_engine* e, const double* vp, const double* vs, double* res_r, double* res_l,
+                      double* cr_pre_r, double* cr_pre_l, double* residual);
+/* One gradient of SWD.m:171-201 for model (vp, vs) (host pointers, nz x nx). */
+int swd_engine_gradient(swd_engine* e, const double* vp, const double* vs, swd_gradient_out* out);
+/* As swd_engine_gradient with device-resident vp, vs and dk_vs (device pointers). */
+int swd_engine_gradient_device(swd_engine* e, const double* d_vp, const double* d_vs, double* d_dk_vs,
+                               double* residual);
+/* The engine's CUDA stream (a cudaStream_t). */
+int swd_engine_stream(const swd_engine* e, void** stream);
+/* Split form of the gradient for several GPUs (shots sharded across ranks; the
+ * parfor sum of SWD.m:193 becomes one all-reduce): the shot sums g_cl, g_cm,
+ * g_illum of this engine's shots go to d_gsum (3*nz*nx doubles, opaque layout)
+ * with the right-side misfit sum and count; after the caller has summed d_gsum
+ * over ranks, swd_engine_assemble_device forms dk_vs (SWD.m:199-201). */
+int swd_engine_shot_sums_device(swd_engine* e, const double* d_vp, const double* d_vs, double* d_gsum,
+                                double* res_sum, int* res_count);
+int swd_engine_assemble_device(swd_engine* e, const double* d_gsum, double* d_dk_vs);
+/* Per-phase CUDA-event timing of later calls (forward, spectra+picks+adjoint
+ * sources, adjoint+imaging), summed over batches, in milliseconds. */
+int swd_engine_set_timing(swd_engine* e, int on);
+int swd_engine_phase_times(const swd_engine* e, double* fwd_ms, double* spec_ms, double* adj_ms);
+
 #ifdef __cplusplus
 }
 #endif

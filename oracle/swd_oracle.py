@@ -631,3 +631,84 @@ def assemble(vs, g_cl, g_cm, g_illum, smoothZ=1, smoothX=2):
     g_cm = g_cm / g_illum
     dk = -4 * vs * g_cl + 2 * vs * g_cm
     return smooth2a(dk, smoothZ, smoothX)
+
+
+# --------------------------------------------------------------------------------------
+# Whole shot loops of SWD.m / SWD_single.m
+# --------------------------------------------------------------------------------------
+
+def _survey_fd(s, is_, vs, single=True, adjoint=False):
+    return fd_inputs(s.nbc, s.nt, s.dtx, s.dx, s.dt, int(s.sx[is_ - 1]), 1, s.gx, np.ones(s.ng),
+                     s.vp_ratio * vs, vs, s.isfs, s.fd_order, s.source_type, s.nt_wf, single, adjoint)
+
+
+def _sides(s, is_):
+    return has_right(is_, s.ns, s.m, s.M, s.w), has_left(is_, s.m, s.M, s.w)
+
+
+def _spectra(s, seis, is_):
+    out = {}
+    r_on, l_on = _sides(s, is_)
+    for side, on in (("r", r_on), ("l", l_on)):
+        if on:
+            out[side] = radon(seis, is_, s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.ng, s.ds, s.offset, s.m,
+                              s.M, side, s.dv)
+    return out
+
+
+def observed_curves(s, vs, single=True):
+    """SWD.m:150-162 (SWD_single.m in single precision): picks of the data of model vs."""
+    npair = s.npair
+    cr = np.ones((npair, s.ns))
+    cl = np.ones((npair, s.ns))
+    for is_ in range(1, s.ns + 1):
+        _, sw, _ = mex_staggerfd(_survey_fd(s, is_, vs, single), s.source(), want_wf=False)
+        sp = _spectra(s, sw.astype(np.float64), is_)
+        if "r" in sp:
+            cr[:, is_ - 1] = LHDispPick(sp["r"][0], s.vmin, cr[:, is_ - 1], 1, s.ini)[1]
+        if "l" in sp:
+            cl[:, is_ - 1] = LHDispPick(sp["l"][0], s.vmin, cl[:, is_ - 1], 1, s.ini)[1]
+    return cr, cl
+
+
+def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True):
+    """SWD_single.m:172-193 for one shot: forward (FP32), spectra, picks, ADWDgrad_1, adjoint."""
+    inp = _survey_fd(s, is_, vs)
+    _, sw, wf = mex_staggerfd(inp, s.source())
+    sp = _spectra(s, sw.astype(np.float64), is_)
+    npair = s.npair
+    out = {"res_r": np.nan, "res_l": np.nan, "crp_r": np.ones(npair), "crp_l": np.ones(npair)}
+    if "r" in sp:
+        out["res_r"], out["crp_r"] = LHDispPick(sp["r"][0], s.vmin, cr0_r[:, is_ - 1], 1, s.ini)
+    if "l" in sp:
+        out["res_l"], out["crp_l"] = LHDispPick(sp["l"][0], s.vmin, cr0_l[:, is_ - 1], 1, s.ini)
+    gr = out["crp_r"] - cr0_r[:, is_ - 1]
+    gl = out["crp_l"] - cr0_l[:, is_ - 1]
+    a = ADWDgrad_1(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl,
+                   sp.get("r", (0, 0, None))[2], sp.get("l", (0, 0, None))[2])
+    out["adj_src"] = a.astype(np.float32)
+    ainp = _survey_fd(s, is_, vs, adjoint=True)
+    out["cl"], out["cm"], out["il"] = mex_e2drtm(ainp, out["adj_src"], wf, accum_fp64)
+    return out
+
+
+def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=True):
+    """SWD_single.m:171-201 with the shot sum in FP64 in shot order."""
+    from concurrent.futures import ThreadPoolExecutor
+    shots = list(range(1, s.ns + 1))
+    if threads > 1:
+        with ThreadPoolExecutor(threads) as ex:
+            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64), shots))
+    else:
+        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64) for i in shots]
+    g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
+    for p in per:
+        for k in g:
+            g[k] = g[k] + p[k]
+    res_r = np.array([p["res_r"] for p in per])
+    out = {"g_cl": g["cl"], "g_cm": g["cm"], "g_illum": g["il"],
+           "dk_vs": assemble(vs, g["cl"], g["cm"], g["il"], s.smooth_z, s.smooth_x),
+           "res_r": res_r, "res_l": np.array([p["res_l"] for p in per]),
+           "cr_pre_r": np.stack([p["crp_r"] for p in per], 1), "cr_pre_l": np.stack([p["crp_l"] for p in per], 1),
+           "residual": float(np.nanmean(res_r)), "per_shot": per}
+    return out

@@ -82,7 +82,9 @@ def lib():
 
 
 def declared_symbols():
-    return list(_SIGS)
+    """Every C entry point the Python package binds (here and in engine.py)."""
+    from .engine import ENGINE_SYMBOLS
+    return list(_SIGS) + ENGINE_SYMBOLS
 
 
 def call(name, *args):

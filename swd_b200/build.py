@@ -27,6 +27,7 @@ SOURCES = {
     "fd_host.cu": ["-fmad=false"],
     "model_prep.cu": ["-fmad=false"],
     "radon.cu": [],
+    "engine.cu": ["-fmad=false"],
 }
 
 

@@ -50,8 +50,9 @@ struct FwdArgs {
   const T* s;                         // wavelet [nt]
   T dtx;
   T* seis_u;                          // [shot][nt][ng] (may be null)
-  T* seis_w;                          // [shot][nt][ng]
+  T* seis_w;                          // [shot][nt][ng] (may be null)
   T* snap;                            // [shot][nrec][NF][nz][nx] (may be null)
+  int rec0;                           // snapshot it/nt_wf is stored at index it/nt_wf - rec0
   int n_shots;
 };
 
@@ -66,6 +67,7 @@ struct AdjArgs {
   const T* snap;                      // forward strain snapshots [shot][nrec][NF][nz][nx]
   double* img;                        // [shot][cl,cm,illum][nz][nx]
   T dtx, dt;
+  int rec0;                           // snapshot it/nt_wf is read from index it/nt_wf - rec0
   int n_shots;
 };
 
@@ -209,14 +211,14 @@ fd_fwd_step(FwdArgs<T> a, int it) {
       xx_o[o] = xxn;
       zz_o[o] = zzn;
       xz_o[o] = xzn;
-      if (k == g.gz && recj >= 0) {  // :342-345
+      if (k == g.gz && recj >= 0 && a.seis_w) {  // :342-345
         const size_t r = ((size_t)shot * g.nt + it) * g.ng + recj;
         a.seis_w[r] = wn;
         if (a.seis_u) a.seis_u[r] = un_cur;
       }
       if (snap && ximg && k >= z_img0 && k < z_img1) {  // :346-351
         const size_t plane = (size_t)g.nz * g.nx;
-        T* sp0 = a.snap + ((size_t)shot * g.nrec + it / g.nt_wf) * NF * plane +
+        T* sp0 = a.snap + ((size_t)shot * g.nrec + (it / g.nt_wf - a.rec0)) * NF * plane +
                  (size_t)(k - z_img0) * g.nx + (x - g.nbc);
         if (NF == 4) {
           sp0[0] = fux; sp0[plane] = fuz; sp0[2 * plane] = bwx; sp0[3 * plane] = bwz;
@@ -340,7 +342,7 @@ fd_adj_step(AdjArgs<T> a, int it) {
       if (img && ximg && k >= z_img0 && k < z_img1) {  // imaging condition (:274-279)
         const size_t plane = (size_t)g.nz * g.nx;
         const size_t cell = (size_t)(k - z_img0) * g.nx + (x - g.nbc);
-        const T* s0 = a.snap + ((size_t)shot * g.nrec + it / g.nt_wf) * NF * plane + cell;
+        const T* s0 = a.snap + ((size_t)shot * g.nrec + (it / g.nt_wf - a.rec0)) * NF * plane + cell;
         T fx, bz, sg;
         if (NF == 4) {
           fx = s0[0]; bz = s0[3 * plane]; sg = s0[plane] + s0[2 * plane];

@@ -299,11 +299,15 @@ __device__ int warp_argmax(const double* y, int lo, int hi, int lane) {
 }
 
 __global__ void pick_kernel(int np, int npair, int G, int lp, int method, double fg, double lfg, double vmin,
-                            const double* ml, const double* cr0, double* cr_pre, double* dc, double* res,
-                            int* status) {
+                            const Gather* gs, const double* ml, const double* cr0, double* cr_pre, double* dc,
+                            double* res, int* status) {
   extern __shared__ int psm[];
   const int gi = blockIdx.x;
   const int lane = threadIdx.x;
+  if (gs && gs[gi].valid <= 0) {  // side not computed for this shot
+    if (lane == 0) res[gi] = 0.0 / 0.0;
+    return;
+  }
   int* idx = psm;                  // 1-based column arrays, entry 0 unused
   int* dvmin = idx + (npair + 1);
   int* dvmax = dvmin + (npair + 1);
@@ -424,12 +428,13 @@ __global__ void pick_kernel(int np, int npair, int G, int lp, int method, double
   }
 }
 
-int pick_batch(int np, int npair, int G, int ini, int method, double vmin, const double* ml, const double* cr0,
-               double* cr_pre, double* dc, double* res, int* status, cudaStream_t st) {
+int pick_batch(int np, int npair, int G, int ini, int method, double vmin, const Gather* d_gath, const double* ml,
+               const double* cr0, double* cr_pre, double* dc, double* res, int* status, cudaStream_t st) {
   SWD_CHECK(ini >= 1 && ini <= npair, "ini (%d) must lie in 1..npair (%d)", ini, npair);
   const size_t smem = (size_t)(npair + 1) * (4 * sizeof(int) + sizeof(double));
   SWD_CUDA(cudaMemsetAsync(status, 0, G * sizeof(int), st));
-  pick_kernel<<<G, 32, smem, st>>>(np, npair, G, ini, method, 2.0, 4.0, vmin, ml, cr0, cr_pre, dc, res, status);
+  pick_kernel<<<G, 32, smem, st>>>(np, npair, G, ini, method, 2.0, 4.0, vmin, d_gath, ml, cr0, cr_pre, dc, res,
+                                   status);
   count_launch(1);
   SWD_CUDA(cudaGetLastError());
   return SWD_OK;
@@ -650,7 +655,7 @@ int swd_pick(const double* ml, int np_, int npair, double vmin, const double* cr
   cudaStream_t st = 0;
   SWD_CUDA(cudaMemcpyAsync(d_ml, ml, spec * sizeof(double), cudaMemcpyHostToDevice, st));
   SWD_CUDA(cudaMemcpyAsync(d_cr0, cr_0, npair * sizeof(double), cudaMemcpyHostToDevice, st));
-  SWD_TRY(pick_batch(np_, npair, 1, ini, method, vmin, d_ml, d_cr0, d_crp, d_dc, d_res, d_st, st));
+  SWD_TRY(pick_batch(np_, npair, 1, ini, method, vmin, nullptr, d_ml, d_cr0, d_crp, d_dc, d_res, d_st, st));
   int status = 0;
   SWD_CUDA(cudaMemcpyAsync(&status, d_st, sizeof(int), cudaMemcpyDeviceToHost, st));
   SWD_CUDA(cudaMemcpyAsync(cr_pre, d_crp, npair * sizeof(double), cudaMemcpyDeviceToHost, st));

@@ -42,8 +42,9 @@ int radon_dft(const RadonGeom& g, const Gather* d_gath, int G, const S* seis, si
 int radon_contract(const RadonGeom& g, const Gather* d_gath, int G, const double2* K, const double2* D, double2* MM,
                    double* mlraw, double* ml, cudaStream_t st);
 // pickFDC1 + LHDispPick per gather: cr_pre = picks + vmin, res = mean((cr_pre-cr0)^2), dc = cr_pre - cr0.
-int pick_batch(int np, int npair, int G, int ini, int method, double vmin, const double* ml, const double* cr0,
-               double* cr_pre, double* dc, double* res, int* status, cudaStream_t st);
+// Gathers with valid <= 0 are skipped (res = NaN); d_gath may be null (all gathers picked).
+int pick_batch(int np, int npair, int G, int ini, int method, double vmin, const Gather* d_gath, const double* ml,
+               const double* cr0, double* cr_pre, double* dc, double* res, int* status, cudaStream_t st);
 // SoftMax gradient + adjoint Radon: Gx[g][f][x] = sum_p conj(K[f][x][p]) * gm[g][f][p]
 int softmax_adjoint(const RadonGeom& g, const Gather* d_gath, int G, const double* mlraw, const double2* MM,
                     const double* dc, const double* space_m, double beta, const double2* K, double2* Gx,
