@@ -48,6 +48,10 @@ def parse():
     p.add_argument("--cpu-shots", type=int, default=0, help="CPU baseline sample size (0: one per host thread)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--snapshot-mode", type=int, default=0)
+    p.add_argument("--warps", type=int, default=0, help="FD kernel CTA shape (0: planner default)")
+    p.add_argument("--cells", type=int, default=0)
+    p.add_argument("--ring", type=int, default=0)
+    p.add_argument("--chunk", type=int, default=0)
     return p.parse_args()
 
 
@@ -192,7 +196,8 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     s = survey(args)
-    eng = GradientEngine(s, snapshot_mode=args.snapshot_mode, device=local)
+    eng = GradientEngine(s, snapshot_mode=args.snapshot_mode, device=local, warps=args.warps, cells=args.cells,
+                         ring_fwd=args.ring, ring_adj=args.ring, chunk_rows=args.chunk)
     info = eng.info
     # observed curves of the "true" model (setup, SWD.m:155-162), then resident inputs
     cr0_r, cr0_l = eng.observed_curves(s.vp_true, s.vs_true)

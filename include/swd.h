@@ -174,14 +174,18 @@ typedef struct {
   int snapshot_mode;  /* 0 auto, 1 keep every strain snapshot, 2 checkpoint + recompute */
   int ckpt_interval;  /* steps between forward checkpoints (mode 2; rounded to nt_wf) */
   int use_graphs;     /* capture the time loops in CUDA graphs */
-  int chunk_rows;     /* rows per warp in the FD kernels (0: heuristic) */
+  int chunk_rows;     /* rows per CTA in the FD kernels (0: heuristic) */
   int device;
+  int warps, cells;   /* FD kernels: warps per CTA and output columns per thread; (w,c) in
+                         (1,2), (1,3), (2,1), (3,1), (4,1); others: (3,1) */
+  int ring_fwd, ring_adj; /* rows in the forward / adjoint shared-memory ring: 4, 6 or 8 (6 at most
+                             for (1,3)); anything else: 4 */
 } swd_engine_opts;
 
 typedef struct {
   int batch, nbatch, mode, ckpt_interval;
   size_t bytes;
-  int npair, np, ccn, nzbc, nxbc, chunk_rows;
+  int npair, np, ccn, nzbc, nxbc, chunk_rows, warps, cells, ring_fwd, ring_adj;
 } swd_engine_info_t;
 
 /* Gradient outputs (host pointers, nz x nx column-major; NULL entries skipped). */

@@ -86,7 +86,7 @@ struct swd_engine {
   int device = 0;
   // device memory
   DevBuf model;        // vp, vs (nz*nx each) + vmin
-  DevBuf m1, m2;       // packed materials
+  DevBuf mat;          // packed materials {temp, ca, cl, cm1}
   DevBuf fstate;       // forward state ping-pong [2][B][5][field]
   DevBuf astate;       // adjoint state ping-pong (checkpoint mode)
   DevBuf ckbuf;        // checkpoints [nseg][B][5][field]
@@ -167,8 +167,7 @@ static int alloc_all(swd_engine* e) {
   const size_t n = (size_t)e->sv.nz * e->sv.nx, B = e->B, plane = e->plane;
   const size_t fieldB = (size_t)B * 5 * g.field;
   SWD_TRY(e->model.alloc((2 * n + 1) * sizeof(double)));
-  SWD_TRY(e->m1.alloc(g.field * sizeof(float4)));
-  SWD_TRY(e->m2.alloc(g.field * sizeof(float4)));
+  SWD_TRY(e->mat.alloc(g.field * sizeof(float4)));
   SWD_TRY(e->fstate.alloc(2 * fieldB * sizeof(float)));
   if (e->mode == 2) {
     SWD_TRY(e->astate.alloc(2 * fieldB * sizeof(float)));
@@ -231,8 +230,8 @@ static int run_seq(swd_engine* e, long key, uint64_t nkernels, F&& body) {
 static FwdArgs<float> fwd_args(swd_engine* e, const FdGeom& g, int s0, int nb) {
   FwdArgs<float> a{};
   a.g = g;
-  a.m1 = e->m1.as<float4>();
-  a.m2 = e->m2.as<float4>();
+  a.mat = e->mat.as<float4>();
+  a.mb = nullptr;
   a.src = e->src.as<int2>() + s0;
   a.src_type = e->sv.source_type;
   a.s = e->wav.as<float>();
@@ -244,8 +243,8 @@ static FwdArgs<float> fwd_args(swd_engine* e, const FdGeom& g, int s0, int nb) {
 static AdjArgs<float> adj_args(swd_engine* e, const FdGeom& g, int nb) {
   AdjArgs<float> a{};
   a.g = g;
-  a.m1 = e->m1.as<float4>();
-  a.m2 = e->m2.as<float4>();
+  a.mat = e->mat.as<float4>();
+  a.mb = nullptr;
   a.res = e->res.as<float>();
   a.img = e->img.as<double>();
   a.dtx = (float)(e->sv.dt / e->sv.dx);
@@ -369,7 +368,7 @@ static int load_model(swd_engine* e, const double* vp, const double* vs, bool de
   SWD_CUDA(cudaMemcpyAsync(d, vp, n * sizeof(double), kind, e->st));
   SWD_CUDA(cudaMemcpyAsync(d + n, vs, n * sizeof(double), kind, e->st));
   SWD_TRY(vmin_device(d, d + n, n, d + 2 * n, e->st));
-  SWD_TRY(prep_packed<float>(e->pp, d, d + n, d + 2 * n, e->m1.as<float4>(), e->m2.as<float4>(), e->g.pitch, e->st));
+  SWD_TRY(prep_packed<float>(e->pp, d, d + n, d + 2 * n, e->mat.as<float4>(), e->g.pitch, e->st));
   return SWD_OK;
 }
 
@@ -515,6 +514,10 @@ static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engi
     hsrc[i] = make_int2(z, x);
   }
   e->plane = (size_t)g.nz * g.nx;
+  g.warps = e->opt.warps;
+  g.cells = e->opt.cells;
+  g.ring_fwd = e->opt.ring_fwd;
+  g.ring_adj = e->opt.ring_adj;
   plan_decomposition(g, std::max(1, std::min(e->opt.max_batch > 0 ? e->opt.max_batch : e->ns, e->ns)),
                      e->opt.chunk_rows);
   // Radon geometry
@@ -527,6 +530,7 @@ static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engi
   SWD_CHECK(s->ini >= 1 && s->ini <= e->rg.npair, "ini (%d) must lie in 1..npair (%d)", s->ini, e->rg.npair);
   SWD_TRY(plan(e));
   plan_decomposition(g, e->B, e->opt.chunk_rows);
+
   e->gseg = g;
   e->gseg.nrec = e->ckpt / g.nt_wf;
   SWD_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
@@ -584,6 +588,10 @@ int swd_engine_info(const swd_engine* e, swd_engine_info_t* info) {
   info->nzbc = e->g.NZ;
   info->nxbc = e->g.NX;
   info->chunk_rows = e->g.chunk;
+  info->warps = e->g.warps;
+  info->cells = e->g.cells;
+  info->ring_fwd = e->g.ring_fwd;
+  info->ring_adj = e->g.ring_adj;
   return SWD_OK;
 }
 

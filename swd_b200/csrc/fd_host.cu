@@ -8,6 +8,7 @@
 
 #include "fd_host.cuh"
 #include "fd_kernels.cuh"
+#include "fd_smem.cuh"
 
 namespace swd {
 
@@ -59,47 +60,66 @@ template int transpose<double, float>(const double*, size_t, float*, size_t, int
 template int transpose<float, double>(const float*, size_t, double*, size_t, int, int, int, cudaStream_t);
 
 // Pack the MATLAB column-major material fields (nzbc x nxbc) into the row-major
-// vector layout the step kernels read: m1 = {temp, b, b1, 0}, m2 = {ca, cl, cm1, 0}.
+// vector layout the step kernels read: mat = {temp, ca, cl, cm1}, mb = {b, b1}.
 template <typename T>
 __global__ void pack_materials_cm(const T* __restrict__ temp, const T* __restrict__ b, const T* __restrict__ b1,
                                   const T* __restrict__ ca, const T* __restrict__ cl, const T* __restrict__ cm1,
-                                  typename Vec4<T>::type* m1, typename Vec4<T>::type* m2, int NZ, int NX, int pitch) {
+                                  typename Vec4<T>::type* mat, typename Vec2<T>::type* mb, int NZ, int NX,
+                                  int pitch) {
   const int z = blockIdx.x * blockDim.x + threadIdx.x;  // z fastest: coalesced reads
   const int x = blockIdx.y;
   if (z >= NZ || x >= NX) return;
   const size_t c = (size_t)x * NZ + z;
-  typename Vec4<T>::type u, v;
-  u.x = temp[c]; u.y = b[c]; u.z = b1[c]; u.w = 0;
-  v.x = ca[c]; v.y = cl[c]; v.z = cm1[c]; v.w = 0;
-  m1[(size_t)z * pitch + x] = u;
-  m2[(size_t)z * pitch + x] = v;
+  typename Vec4<T>::type u;
+  typename Vec2<T>::type v;
+  u.x = temp[c]; u.y = ca[c]; u.z = cl[c]; u.w = cm1[c];
+  v.x = b[c]; v.y = b1[c];
+  mat[(size_t)z * pitch + x] = u;
+  mb[(size_t)z * pitch + x] = v;
 }
 
 template <typename T>
 int pack_materials(const T* temp, const T* b, const T* b1, const T* ca, const T* cl, const T* cm1,
-                   typename Vec4<T>::type* m1, typename Vec4<T>::type* m2, int NZ, int NX, int pitch,
+                   typename Vec4<T>::type* mat, typename Vec2<T>::type* mb, int NZ, int NX, int pitch,
                    cudaStream_t st) {
   dim3 grid((NZ + 127) / 128, NX), block(128);
-  pack_materials_cm<T><<<grid, block, 0, st>>>(temp, b, b1, ca, cl, cm1, m1, m2, NZ, NX, pitch);
+  pack_materials_cm<T><<<grid, block, 0, st>>>(temp, b, b1, ca, cl, cm1, mat, mb, NZ, NX, pitch);
   count_launch(1);
   SWD_CUDA(cudaGetLastError());
   return SWD_OK;
 }
 template int pack_materials<float>(const float*, const float*, const float*, const float*, const float*,
-                                   const float*, float4*, float4*, int, int, int, cudaStream_t);
+                                   const float*, float4*, float2*, int, int, int, cudaStream_t);
 template int pack_materials<double>(const double*, const double*, const double*, const double*,
-                                    const double*, const double*, double4*, double4*, int, int, int,
+                                    const double*, const double*, double4*, double2*, int, int, int,
                                     cudaStream_t);
 
 // ------------------------------------------------------------ planning
 
+// (warps, cells, ring depth) variants built for the engine path.  The kernels unroll the row
+// loop by the ring depth, so it is even; depth 4 is the fastest on the 100 x 600 survey.
+#define SWD_SHAPES(X) \
+  X(1, 2, 4) X(1, 2, 6) X(1, 2, 8) X(1, 3, 4) X(1, 3, 6) X(2, 1, 4) X(2, 1, 6) X(2, 1, 8) X(3, 1, 4) X(3, 1, 6) \
+  X(3, 1, 8) X(4, 1, 4) X(4, 1, 6) X(4, 1, 8)
+
+static bool variant_built(int w, int c, int d) {
+#define X(W, C, D) if (w == W && c == C && d == D) return true;
+  SWD_SHAPES(X)
+#undef X
+  return false;
+}
+
 void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
   const int rows = g.NZ - 2;
-  g.n_strips = (g.NX - 2 + kStrip - 1) / kStrip;
+  if (!variant_built(g.warps, g.cells, 4)) { g.warps = 3; g.cells = 1; }
+  if (!variant_built(g.warps, g.cells, g.ring_fwd)) g.ring_fwd = 4;
+  if (!variant_built(g.warps, g.cells, g.ring_adj)) g.ring_adj = 4;
+  const int cols = 32 * g.warps * g.cells;
+  g.n_strips = (g.NX - 2 + cols - 1) / cols;
   if (chunk_rows <= 0) {
-    // aim for about one full wave of warps (148 SMs x 32 resident warps)
-    const long target = 148L * 32;
-    long per = (long)g.n_strips * n_shots;
+    // aim for about one full wave of CTAs (148 SMs x ~(32 / warps) resident CTAs)
+    const long target = 148L * (32 / g.warps) / 2;
+    const long per = (long)g.n_strips * n_shots;
     int nch = (int)((target + per - 1) / per);
     nch = std::max(1, std::min(nch, std::max(1, rows / 8)));
     chunk_rows = (rows + nch - 1) / nch;
@@ -108,23 +128,80 @@ void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
   g.n_chunks = (rows + g.chunk - 1) / g.chunk;
 }
 
-template <typename T, int NF>
-int launch_fwd_step(const FwdArgs<T>& a, int it, cudaStream_t st) {
-  constexpr int WPB = 4;
-  const long warps = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
-  const int blocks = (int)((warps + WPB - 1) / WPB);
-  fd_fwd_step<T, NF, WPB><<<blocks, WPB * 32, 0, st>>>(a, it);
+template <typename K>
+static int set_smem(K kernel, size_t bytes) {
+  if (bytes > 48 * 1024) SWD_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return SWD_OK;
+}
+
+template <typename T, int NF, int W, int C, int D, bool GB, bool SNAP>
+static int fwd_launch(const FwdArgs<T>& a, int it, cudaStream_t st) {
+  constexpr size_t smem = smem_bytes<T, W, C, D, GB>();
+  static int ready = set_smem(fd_fwd_smem<T, NF, W, C, D, GB, SNAP>, smem);
+  if (ready != SWD_OK) return ready;
+  const long blocks = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
+  fd_fwd_smem<T, NF, W, C, D, GB, SNAP><<<(unsigned)blocks, 32 * W, smem, st>>>(a, it);
   count_launch(1);
   return SWD_OK;
 }
-template <typename T, int NF>
-int launch_adj_step(const AdjArgs<T>& a, int it, cudaStream_t st) {
-  constexpr int WPB = 4;
-  const long warps = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
-  const int blocks = (int)((warps + WPB - 1) / WPB);
-  fd_adj_step<T, NF, WPB><<<blocks, WPB * 32, 0, st>>>(a, it);
+// strain snapshots are written every nt_wf steps: a separate variant keeps the code off the other steps
+template <typename T, int NF, int W, int C, int D, bool GB>
+static int fwd_impl(const FwdArgs<T>& a, int it, cudaStream_t st) {
+  if (a.snap && it % a.g.nt_wf == 0) return fwd_launch<T, NF, W, C, D, GB, true>(a, it, st);
+  return fwd_launch<T, NF, W, C, D, GB, false>(a, it, st);
+}
+
+template <typename T, int NF, int W, int C, int D, bool GB, bool IMG>
+static int adj_impl(const AdjArgs<T>& a, int it, cudaStream_t st) {
+  constexpr size_t smem = smem_bytes<T, W, C, D, GB>();
+  static int ready = set_smem(fd_adj_smem<T, NF, W, C, D, GB, IMG>, smem);
+  if (ready != SWD_OK) return ready;
+  const long blocks = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
+  fd_adj_smem<T, NF, W, C, D, GB, IMG><<<(unsigned)blocks, 32 * W, smem, st>>>(a, it);
   count_launch(1);
   return SWD_OK;
+}
+
+// Engine path (FP32, 3 snapshot fields, b/b1 from the row index): CTA shape and ring depth are
+// runtime choices.  MEX path (general b/b1 arrays, 4 snapshot fields, FP32 or FP64): 4 warps x 1.
+template <typename T, int NF>
+int launch_fwd_step(const FwdArgs<T>& a, int it, cudaStream_t st) {
+  if (a.mb) return fwd_impl<T, NF, 4, 1, 4, true>(a, it, st);
+  if constexpr (NF == 3 && sizeof(T) == 4) {
+    const int key = a.g.warps * 100 + a.g.cells * 10 + a.g.ring_fwd;
+    switch (key) {
+#define X(w, c, d) case w * 100 + c * 10 + d: return fwd_impl<T, NF, w, c, d, false>(a, it, st);
+      SWD_SHAPES(X)
+#undef X
+      default: break;
+    }
+  }
+  set_error("internal: unsupported FD kernel variant");
+  return SWD_ERR_INVALID;
+}
+
+template <typename T, int NF, bool IMG>
+static int adj_dispatch(const AdjArgs<T>& a, int it, cudaStream_t st) {
+  if (a.mb) return adj_impl<T, NF, 4, 1, 4, true, IMG>(a, it, st);
+  if constexpr (NF == 3 && sizeof(T) == 4) {
+    const int key = a.g.warps * 100 + a.g.cells * 10 + a.g.ring_adj;
+    switch (key) {
+#define X(w, c, d) case w * 100 + c * 10 + d: return adj_impl<T, NF, w, c, d, false, IMG>(a, it, st);
+      SWD_SHAPES(X)
+#undef X
+      default: break;
+    }
+  }
+  set_error("internal: unsupported FD kernel variant");
+  return SWD_ERR_INVALID;
+}
+
+template <typename T, int NF>
+int launch_adj_step(const AdjArgs<T>& a, int it, cudaStream_t st) {
+  // the imaging condition only runs every nt_wf steps: a separate variant keeps the
+  // other steps free of its registers
+  if (it % a.g.nt_wf == 0) return adj_dispatch<T, NF, true>(a, it, st);
+  return adj_dispatch<T, NF, false>(a, it, st);
 }
 template int launch_fwd_step<float, 3>(const FwdArgs<float>&, int, cudaStream_t);
 template int launch_fwd_step<float, 4>(const FwdArgs<float>&, int, cudaStream_t);
@@ -190,6 +267,10 @@ int fill_geom(FdGeom& g, int NZ, int NX, int nz, int nx, int nbc, int nt, int nt
   g.nt = nt; g.nt_wf = nt_wf; g.nrec = nt / nt_wf;
   g.ng = ng; g.gz = gz; g.gx = gx; g.dg = dg;
   g.field = (size_t)NZ * g.pitch;
+  g.warps = 4;
+  g.cells = 1;
+  g.ring_fwd = 4;
+  g.ring_adj = 4;
   return SWD_OK;
 }
 
@@ -210,11 +291,12 @@ int staggerfd_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl
   fill_geom<T>(g, p.nzbc, p.nxbc, p.nz, p.nx, nbc, p.nt, p.nt_wf, p.ng, p.gz, p.gx, p.dg);
   plan_decomposition(g, 1, 0);
   using V = typename Vec4<T>::type;
+  using V2 = typename Vec2<T>::type;
   const size_t NN = (size_t)p.nzbc * p.nxbc, plane = (size_t)p.nz * p.nx;
   DevBuf d_in, d_m1, d_m2, d_state, d_seis, d_seis_t, d_snap, d_snap_t, d_src;
   SWD_TRY(d_in.alloc(6 * NN * sizeof(T) + p.nt * sizeof(T)));
   SWD_TRY(d_m1.alloc(g.field * sizeof(V)));
-  SWD_TRY(d_m2.alloc(g.field * sizeof(V)));
+  SWD_TRY(d_m2.alloc(g.field * sizeof(V2)));
   SWD_TRY(d_state.alloc(2 * 5 * g.field * sizeof(T)));
   SWD_TRY(d_seis.alloc(2 * (size_t)p.nt * p.ng * sizeof(T)));
   SWD_TRY(d_seis_t.alloc(2 * (size_t)p.nt * p.ng * sizeof(T)));
@@ -232,11 +314,11 @@ int staggerfd_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl
   int2 sp = make_int2(p.sz, p.sx);
   SWD_CUDA(cudaMemcpyAsync(d_src.p, &sp, sizeof(int2), cudaMemcpyHostToDevice, st));
   SWD_TRY(pack_materials<T>(din, din + NN, din + 2 * NN, din + 3 * NN, din + 4 * NN, din + 5 * NN, d_m1.as<V>(),
-                            d_m2.as<V>(), p.nzbc, p.nxbc, g.pitch, st));
+                            d_m2.as<V2>(), p.nzbc, p.nxbc, g.pitch, st));
   SWD_CUDA(cudaMemsetAsync(d_state.p, 0, d_state.bytes, st));
   SWD_CUDA(cudaMemsetAsync(d_seis.p, 0, d_seis.bytes, st));
   FwdArgs<T> a{};
-  a.g = g; a.m1 = d_m1.as<V>(); a.m2 = d_m2.as<V>();
+  a.g = g; a.mat = d_m1.as<V>(); a.mb = d_m2.as<V2>();
   a.src = d_src.as<int2>(); a.src_type = p.src_type; a.s = d_s; a.dtx = (T)p.dtx;
   a.seis_w = d_seis.as<T>(); a.seis_u = a.seis_w + (size_t)p.nt * p.ng;
   a.snap = want_wf ? d_snap.as<T>() : nullptr;
@@ -285,11 +367,12 @@ int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, c
   fill_geom<T>(g, NZ, NX, nz, nx, nbc, nt, nt_wf, ng, gz, gx, dg);
   plan_decomposition(g, 1, 0);
   using V = typename Vec4<T>::type;
+  using V2 = typename Vec2<T>::type;
   const size_t NN = (size_t)NZ * NX, plane = (size_t)nz * nx, nsnap = (size_t)g.nrec * plane;
   DevBuf d_in, d_m1, d_m2, d_state, d_res, d_snap, d_img, d_out;
   SWD_TRY(d_in.alloc(std::max(6 * NN, nsnap) * sizeof(T) + (size_t)nt * ng * sizeof(T)));
   SWD_TRY(d_m1.alloc(g.field * sizeof(V)));
-  SWD_TRY(d_m2.alloc(g.field * sizeof(V)));
+  SWD_TRY(d_m2.alloc(g.field * sizeof(V2)));
   SWD_TRY(d_state.alloc(2 * 5 * g.field * sizeof(T)));
   SWD_TRY(d_res.alloc((size_t)nt * ng * sizeof(T)));
   SWD_TRY(d_snap.alloc(4 * nsnap * sizeof(T)));
@@ -301,7 +384,7 @@ int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, c
   const T* hsrc[6] = {temp, b, b1, ca, cl, cm1};
   for (int i = 0; i < 6; ++i) SWD_CUDA(cudaMemcpyAsync(din + i * NN, hsrc[i], NN * sizeof(T), cudaMemcpyHostToDevice, st));
   SWD_TRY(pack_materials<T>(din, din + NN, din + 2 * NN, din + 3 * NN, din + 4 * NN, din + 5 * NN, d_m1.as<V>(),
-                            d_m2.as<V>(), NZ, NX, g.pitch, st));
+                            d_m2.as<V2>(), NZ, NX, g.pitch, st));
   // residual: MATLAB nt x ng -> [nt][ng]
   SWD_CUDA(cudaMemcpyAsync(dstage, res, (size_t)nt * ng * sizeof(T), cudaMemcpyHostToDevice, st));
   SWD_TRY(transpose<T, T>(dstage, 0, d_res.as<T>(), 0, 1, ng, nt, st));
@@ -314,7 +397,7 @@ int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, c
   SWD_CUDA(cudaMemsetAsync(d_state.p, 0, d_state.bytes, st));
   SWD_CUDA(cudaMemsetAsync(d_img.p, 0, d_img.bytes, st));
   AdjArgs<T> a{};
-  a.g = g; a.m1 = d_m1.as<V>(); a.m2 = d_m2.as<V>();
+  a.g = g; a.mat = d_m1.as<V>(); a.mb = d_m2.as<V2>();
   a.res = d_res.as<T>(); a.snap = d_snap.as<T>(); a.img = d_img.as<double>();
   a.dtx = dtx; a.dt = dt; a.n_shots = 1;
   T* bufs[2] = {d_state.as<T>(), d_state.as<T>() + 5 * g.field};

@@ -14,10 +14,10 @@ void count_launch(uint64_t n);
 template <typename Ti, typename To>
 int transpose(const Ti* in, size_t ib, To* out, size_t ob, int B, int R, int C, cudaStream_t st);
 
-// MATLAB column-major materials -> packed row-major {temp,b,b1,0} / {ca,cl,cm1,0}.
+// MATLAB column-major materials -> packed row-major mat {temp,ca,cl,cm1} and mb {b,b1}.
 template <typename T>
 int pack_materials(const T* temp, const T* b, const T* b1, const T* ca, const T* cl, const T* cm1,
-                   typename Vec4<T>::type* m1, typename Vec4<T>::type* m2, int NZ, int NX, int pitch,
+                   typename Vec4<T>::type* mat, typename Vec2<T>::type* mb, int NZ, int NX, int pitch,
                    cudaStream_t st);
 
 // Choose strips/chunks for a launch over n_shots shots (chunk_rows <= 0: heuristic).

@@ -94,20 +94,19 @@ __global__ void prep_cm_kernel(PrepParams p, const double* vp, const double* vs,
   temp[c] = t; ca[c] = a_; cl[c] = l; cm[c] = m; cm1[c] = m; b[c] = bb; b1[c] = bb;
 }
 
-// Packed row-major outputs read by the step kernels.
+// Packed row-major {temp, ca, cl, cm1} read by the step kernels (b = b1 = dtx, doubled on the
+// free-surface row, is formed in the kernels from the row index).
 template <typename T>
 __global__ void prep_packed_kernel(PrepParams p, const double* vp, const double* vs, const double* vmin,
-                                   typename Vec4<T>::type* m1, typename Vec4<T>::type* m2, int pitch) {
+                                   typename Vec4<T>::type* mat, int pitch) {
   const int x = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y;
   if (x >= p.NX) return;
   const double kappa = kappa_of(p, *vmin);
   T t, a_, l, m, bb;
   prep_cell<T>(p, kappa, vp, vs, z, x, t, a_, l, m, bb);
-  typename Vec4<T>::type u, v;
-  u.x = t; u.y = bb; u.z = bb; u.w = 0;
-  v.x = a_; v.y = l; v.z = m; v.w = 0;
-  m1[(size_t)z * pitch + x] = u;
-  m2[(size_t)z * pitch + x] = v;
+  typename Vec4<T>::type u;
+  u.x = t; u.y = a_; u.z = l; u.w = m;
+  mat[(size_t)z * pitch + x] = u;
 }
 
 int prep_check(const PrepParams& p) {
@@ -134,17 +133,17 @@ int vmin_device(const double* d_vp, const double* d_vs, size_t n, double* d_out,
 
 template <typename T>
 int prep_packed(const PrepParams& p, const double* d_vp, const double* d_vs, const double* d_vmin,
-                typename Vec4<T>::type* m1, typename Vec4<T>::type* m2, int pitch, cudaStream_t st) {
+                typename Vec4<T>::type* mat, int pitch, cudaStream_t st) {
   dim3 grid((p.NX + 127) / 128, p.NZ), block(128);
-  prep_packed_kernel<T><<<grid, block, 0, st>>>(p, d_vp, d_vs, d_vmin, m1, m2, pitch);
+  prep_packed_kernel<T><<<grid, block, 0, st>>>(p, d_vp, d_vs, d_vmin, mat, pitch);
   count_launch(1);
   SWD_CUDA(cudaGetLastError());
   return SWD_OK;
 }
-template int prep_packed<float>(const PrepParams&, const double*, const double*, const double*, float4*, float4*,
-                                int, cudaStream_t);
-template int prep_packed<double>(const PrepParams&, const double*, const double*, const double*, double4*,
-                                 double4*, int, cudaStream_t);
+template int prep_packed<float>(const PrepParams&, const double*, const double*, const double*, float4*, int,
+                                cudaStream_t);
+template int prep_packed<double>(const PrepParams&, const double*, const double*, const double*, double4*, int,
+                                 cudaStream_t);
 
 template <typename T>
 int prep_host(int nz, int nx, int nbc, int isfs, int fd_order, double dx, double dt, double dtx, const double* vp,

@@ -18,6 +18,6 @@ void prep_fill(PrepParams& p);
 int vmin_device(const double* d_vp, const double* d_vs, size_t n, double* d_out, cudaStream_t st);
 template <typename T>
 int prep_packed(const PrepParams& p, const double* d_vp, const double* d_vs, const double* d_vmin,
-                typename Vec4<T>::type* m1, typename Vec4<T>::type* m2, int pitch, cudaStream_t st);
+                typename Vec4<T>::type* mat, int pitch, cudaStream_t st);
 
 }  // namespace swd
