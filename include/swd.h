@@ -135,6 +135,19 @@ int swd_radon(const swd_radon_params* p, int side, int is, const double* seismo,
 int swd_pick(const double* ml, int np, int npair, double vmin, const double* cr_0, int method, int ini,
              double* res, double* cr_pre);
 
+/* Allocation-free variant of swd_pick; it has no counterpart in the reference.
+ * For callers that cannot allocate device memory: it calls no cudaMalloc, cudaFree or other
+ * allocating routine.  All arrays are caller-owned DEVICE memory: d_ml np x npair, d_cr_0 and
+ * d_cr_pre npair, d_res one double (may be NULL).  stream is a cudaStream_t (NULL: the legacy
+ * default stream); the call synchronises it to read the pick status.  The scratch lives in one
+ * static device array of libswd.so (16 KiB, held by every GPU that loads the library until the
+ * process exits), which limits npair to SWD_PICK_NOALLOC_MAX_NPAIR.  The first call on a device
+ * looks up the array's device address; make that call before any stream capture.  Every call
+ * shares the array: calls that overlap on the GPU race. */
+#define SWD_PICK_NOALLOC_MAX_NPAIR 2047
+int swd_pick_noalloc(const double* d_ml, int np, int npair, double vmin, const double* d_cr_0, int method,
+                     int ini, double* d_res, double* d_cr_pre, void* stream);
+
 /* Replaces ADWDgrad_1(nt,ng,ns,npair,is,w,m,M,SoftArgNorm,grad_outputr,grad_outputl,
  * space_M,saveForBackwardr,saveForBackwardl) (core/ADWDgrad_1.m:1-81).
  * grad_output_*: npair; space_m: np x npair (NULL = 1..np per column, SWD.m:133-136);

@@ -46,6 +46,8 @@ _SIGS = {
     "swd_radon_sizes": [_rpp] + [_i32p] * 5,
     "swd_radon": [_rpp, _c_int, _c_int] + [_f64p] * 4 + [_i32p] * 2,
     "swd_pick": [_f64p, _c_int, _c_int, _c_dbl, _f64p, _c_int, _c_int, _f64p, _f64p],
+    "swd_pick_noalloc": [ctypes.c_void_p, _c_int, _c_int, _c_dbl, ctypes.c_void_p, _c_int, _c_int,
+                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "swd_adwdgrad": [_rpp, _c_int, _c_int, _c_int, _c_dbl] + [_f64p] * 8,
 }
 _RESTYPE = {"swd_last_error": ctypes.c_char_p, "swd_kernel_launches": ctypes.c_uint64}

@@ -28,6 +28,7 @@ SOURCES = {
     "model_prep.cu": ["-fmad=false"],
     "radon.cu": [],
     "engine.cu": ["-fmad=false"],
+    "pick_noalloc.cu": [],
 }
 
 
