@@ -117,8 +117,9 @@ void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
   const int cols = 32 * g.warps * g.cells;
   g.n_strips = (g.NX - 2 + cols - 1) / cols;
   if (chunk_rows <= 0) {
-    // aim for about one full wave of CTAs (148 SMs x ~(32 / warps) resident CTAs)
-    const long target = 148L * (32 / g.warps) / 2;
+    // about 2.5 waves of CTAs (148 SMs x ~(30 / warps) resident CTAs at 64 registers): short
+    // chunks keep every SM busy through the tail of a step; 96 shots of 132 x 660 -> 22 rows
+    const long target = 148L * (30 / g.warps) * 5 / 2;
     const long per = (long)g.n_strips * n_shots;
     int nch = (int)((target + per - 1) / per);
     nch = std::max(1, std::min(nch, std::max(1, rows / 8)));
