@@ -8,7 +8,8 @@ assembled into the smoothed Vs gradient.  Inputs are seeded synthetic models.
 
     python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 
-Under torchrun every rank runs its own 96 shots (weak scaling); the shot sums
+Under torchrun the survey's shots are split round-robin over the ranks (strong
+scaling: the whole job is always the same 96 shots); each rank's FP64 shot sums
 are all-reduced over NCCL before the gradient is assembled (the parfor sum of
 SWD.m:193).  Rank 0 prints one JSON line.
 """
@@ -30,10 +31,14 @@ import numpy as np  # noqa: E402
 
 METRIC = "shot-gradients/s (fwd+adj)"
 UNIT = "shot-gradients/s"
-# DRAM traffic per padded cell and time step of the FD step kernels, from the ncu capture
-# summarised in profiles/fd_step_kernels_batched-100x600.md (dram__bytes_read.sum +
-# dram__bytes_write.sum per launch / cells per launch).  None until measured.
-NCU_BYTES_PER_CELL_STEP = {"fd_fwd_step": None, "fd_adj_step": None}
+# DRAM traffic per padded cell and time step of the FD step kernels (plain-step variants, 4 of
+# every 5 launches), from the ncu capture summarised in profiles/fd_step_kernels_batched-100x600.md:
+# (dram__bytes_read.sum + dram__bytes_write.sum) per launch / (96 shots x 132 x 660 cells).
+NCU_BYTES_PER_CELL_STEP = {"fd_fwd_step": 36.1, "fd_adj_step": 36.1}
+# Compulsory DRAM bytes of the fused one-sweep kernels: 5 state fields read + 5 written per
+# shot-cell-step (materials are shared by the shots of a launch), plus per interior cell every
+# nt_wf steps the 3-field snapshot write (forward) or snapshot read + FP64 image update (adjoint).
+COMPULSORY_STATE_B = 40
 
 
 def parse():
@@ -42,16 +47,24 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--shots", type=int, default=96, help="shots per GPU")
+    p.add_argument("--shots", type=int, default=96, help="shots in the survey (split over the GPUs)")
     p.add_argument("--nt", type=int, default=8000)
     p.add_argument("--plain-shots", type=int, default=8, help="shots timed on the one-shot-per-launch path")
     p.add_argument("--cpu-shots", type=int, default=0, help="CPU baseline sample size (0: one per host thread)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    p.add_argument("--snapshot-mode", type=int, default=0)
+    p.add_argument("--snapshot-mode", type=int, default=0, help="0 auto, 1 store snapshots, 2 checkpoint")
+    p.add_argument("--ckpt", type=int, default=50, help="steps between checkpoints (snapshot mode 2)")
     p.add_argument("--warps", type=int, default=0, help="FD kernel CTA shape (0: planner default)")
     p.add_argument("--cells", type=int, default=0)
     p.add_argument("--ring", type=int, default=0)
     p.add_argument("--chunk", type=int, default=0)
+    p.add_argument("--serve", type=int, default=0,
+                   help="served request stream: number of requests (0: run the gradient bench instead)")
+    p.add_argument("--rate", type=float, default=2.0, help="served stream: Poisson arrival rate, requests/s")
+    p.add_argument("--inflight", type=int, default=4, help="served stream: requests on the GPU at once")
+    p.add_argument("--surveys", type=int, default=16, help="served stream: distinct surveys (engine keys)")
+    p.add_argument("--plain-sample", type=int, default=8,
+                   help="served stream: requests re-run serially on the plain path for the comparison")
     return p.parse_args()
 
 
@@ -118,7 +131,7 @@ def workload_config(s, extra=None):
     c = {"workload": f"batched-{s.nz}x{s.nx}: nz={s.nz} nx={s.nx} dx={s.dx} nbc={s.nbc} nt={s.nt} dt={s.dt} "
                      f"{s.ns} shots x {s.ng} receivers, Ricker f0={s.f0}, Radon {s.fmin:g}-{s.fmax:g} Hz "
                      f"df={s.df:g}, {s.vmin:g}-{s.vmax:g} m/s step {s.dv:g}, offset {s.offset}",
-         "shots_per_gpu": s.ns, "grid_padded": [s.nzbc, s.nxbc], "nt": s.nt, "nt_wf": s.nt_wf,
+         "shots": s.ns, "grid_padded": [s.nzbc, s.nxbc], "nt": s.nt, "nt_wf": s.nt_wf,
          "l2": "inputs larger than L2 (state + snapshots >> 126 MB); no flush needed"}
     if extra:
         c.update(extra)
@@ -167,7 +180,7 @@ def run_reference(args):
     v = info["cores"] / statistics.mean(times)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(times) * 1e3,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(s, {"sample": info["sample"]}),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "port",
                              "sample": info["sample"]},
@@ -178,15 +191,85 @@ def run_reference(args):
 
 # ------------------------------------------------------------------ our arm
 
+def run_serve(args):
+    """Served request stream on one GPU: Poisson arrivals of gradient and misfit requests over
+    surveys of different grid sizes, shot counts and nt; p50/p99 latency and throughput, next to
+    the same kind of requests run one at a time on the plain one-shot-per-launch path."""
+    from swd_b200 import configs
+    from swd_b200.engine import GradientEngine
+    from swd_b200.serve import Server
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    surveys = configs.served_surveys(args.surveys)
+    stream = configs.served_stream(args.serve, len(surveys), args.rate)
+    cr0 = [configs.smooth_curve(s, i) for i, s in enumerate(surveys)]
+
+    def inputs(k, sc):
+        s = surveys[k]
+        vs = s.vs * sc
+        return s, s.vp_ratio * vs, vs
+
+    # warm: library load and one small request
+    with Server(max_inflight=1) as srv:
+        s, vp, vs = inputs(0, 1.0)
+        srv.wait(srv.submit(s, vp, vs, cr0[0], cr0[0], kind="misfit"))
+    with Server(max_inflight=args.inflight) as srv, ClockSampler(0) as clk:
+        t0 = time.perf_counter()
+        ids = []
+        for t, k, kind, sc in stream:
+            lag = t0 + t - time.perf_counter()
+            if lag > 0:
+                time.sleep(lag)
+            s, vp, vs = inputs(k, sc)
+            ids.append(srv.submit(s, vp, vs, cr0[k], cr0[k], kind=kind, key=k + 1))
+        results = [srv.wait(i) for i in ids]
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+    lat = np.array([r["total_ms"] for r in results])
+    shots = sum(surveys[k].ns for _, k, kind, _ in stream if kind == "gradient")
+    # the plain path, one request at a time, on every (n/sample)-th request of the same stream
+    step = max(1, len(stream) // max(1, args.plain_sample))
+    sample = stream[::step][: args.plain_sample]
+    tp = time.perf_counter()
+    for _, k, kind, sc in sample:
+        s, vp, vs = inputs(k, sc)
+        with GradientEngine(s, max_batch=1, use_graphs=False) as e:
+            e.set_observed(cr0[k], cr0[k])
+            (e.gradient if kind == "gradient" else e.misfit)(vp, vs)
+    tp = time.perf_counter() - tp
+    line = {"metric": "served requests/s", "value": len(stream) / wall, "unit": "requests/s", "n_gpus": 1,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded layered models + checkerboard)",
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "mean": float(lat.mean()), "max": float(lat.max())},
+            "shot_gradients_per_s": shots / wall,
+            "config": {"workload": f"{len(stream)} requests (gradient or line-search misfit), Poisson arrivals at "
+                                   f"{args.rate:g}/s over {len(surveys)} surveys: grids 60x200..300x1200 "
+                                   f"(log-uniform), 8-64 shots, nt 3000-10000, dx 0.5, nbc 30, dt 5e-5",
+                       "max_inflight": args.inflight, "arrival_span_s": stream[-1][0]},
+            "server": {k: st[k] for k in ("admitted", "completed", "waits_for_memory", "peak_inflight",
+                                          "peak_bytes", "budget")},
+            "engine_reuse": sum(r["reused_engine"] for r in results),
+            "plain_serial": {"requests": len(sample), "seconds": tp, "value": len(sample) / tp, "unit": "requests/s",
+                             "how": "same requests (every n-th of the stream), one at a time, one shot per launch, "
+                                    "no CUDA graphs"},
+            "clocks": clk.summary()}
+    line["served_over_plain"] = line["value"] / line["plain_serial"]["value"]
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.serve:
+        return run_serve(args)
     import torch
     import torch.distributed as dist
 
     import swd_b200 as S
     from swd_b200.engine import GradientEngine
+    from swd_b200.shots import ShardedGradient
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -196,29 +279,23 @@ def main():
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     s = survey(args)
-    eng = GradientEngine(s, snapshot_mode=args.snapshot_mode, device=local, warps=args.warps, cells=args.cells,
-                         ring_fwd=args.ring, ring_adj=args.ring, chunk_rows=args.chunk)
+    # this rank's share of the survey's shots (all of them at N=1)
+    sg = ShardedGradient(s, world, rank, device=local, snapshot_mode=args.snapshot_mode,
+                         ckpt_interval=args.ckpt, warps=args.warps, cells=args.cells, ring_fwd=args.ring,
+                         ring_adj=args.ring, chunk_rows=args.chunk)
+    eng = sg.engine
     info = eng.info
     # observed curves of the "true" model (setup, SWD.m:155-162), then resident inputs
-    cr0_r, cr0_l = eng.observed_curves(s.vp_true, s.vs_true)
-    eng.set_observed(cr0_r, cr0_l)
+    cr0_r, cr0_l = sg.set_observed_from_model(s.vp_true, s.vs_true)
     dev = torch.device("cuda", local)
     # MATLAB column-major nz x nx data == C-contiguous (nx, nz)
     d_vp = torch.from_numpy(np.ascontiguousarray(s.vp.T)).to(dev)
     d_vs = torch.from_numpy(np.ascontiguousarray(s.vs.T)).to(dev)
     d_dk = torch.zeros((s.nx, s.nz), dtype=torch.float64, device=dev)
-    d_gsum = torch.zeros(3 * s.nz * s.nx, dtype=torch.float64, device=dev)
-    red = torch.zeros(2, dtype=torch.float64, device=dev)
-    ext = torch.cuda.ExternalStream(eng.stream(), device=dev)
+    ext = sg.stream
 
     def step():
-        rsum, rcnt = eng.shot_sums_device(d_vp, d_vs, d_gsum)
-        if world > 1:
-            with torch.cuda.stream(ext):
-                dist.all_reduce(d_gsum)
-                red[0], red[1] = rsum, rcnt
-                dist.all_reduce(red)
-        eng.assemble_device(d_gsum, d_dk)
+        return sg.gradient_device(d_vp, d_vs, d_dk)
 
     for _ in range(args.warmup):
         step()
@@ -244,59 +321,83 @@ def main():
         ms = float(t.item())
         dist.barrier()
     ms_step = ms / args.steps
-    value = world * s.ns / (ms_step / 1e3)
+    value = s.ns / (ms_step / 1e3)  # the survey's shots, over all ranks
 
-    # e2e through the host-pointer C ABI from pinned host memory (inputs up, gradient + misfits down)
-    vp_h = torch.empty((s.nx, s.nz), dtype=torch.float64, pin_memory=True).numpy()
-    vs_h = torch.empty((s.nx, s.nz), dtype=torch.float64, pin_memory=True).numpy()
-    vp_h[:] = s.vp.T
-    vs_h[:] = s.vs.T
-    eng.gradient(vp_h.T, vs_h.T)  # warm
+    # e2e from pinned host memory: (vp, vs) up, gradient (+ images, picks, misfits at N=1) down.
+    # N=1: the host-pointer C ABI call swd_engine_gradient; N>1: copies around the sharded step.
+    vp_h = torch.empty((s.nx, s.nz), dtype=torch.float64, pin_memory=True)
+    vs_h = torch.empty((s.nx, s.nz), dtype=torch.float64, pin_memory=True)
+    dk_h = torch.empty((s.nx, s.nz), dtype=torch.float64, pin_memory=True)
+    vp_h.numpy()[:] = s.vp.T
+    vs_h.numpy()[:] = s.vs.T
+
+    def e2e_step():
+        if world == 1:
+            eng.gradient(vp_h.numpy().T, vs_h.numpy().T)
+            return
+        with torch.cuda.stream(ext):
+            d_vp.copy_(vp_h, non_blocking=True)
+            d_vs.copy_(vs_h, non_blocking=True)
+        sg.gradient_device(d_vp, d_vs, d_dk)
+        dk_h.copy_(d_dk)
+
+    e2e_step()  # warm
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()
     ne2e = max(1, min(args.steps, 3))
     for _ in range(ne2e):
-        out = eng.gradient(vp_h.T, vs_h.T)
+        e2e_step()
     e2e_s = (time.perf_counter() - t0) / ne2e
     if world > 1:
         t = torch.tensor([e2e_s], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
     h2d = 2 * s.nz * s.nx * 8
-    d2h = 4 * s.nz * s.nx * 8 + 2 * s.ns * 8 + 2 * info["npair"] * s.ns * 8
+    d2h = (4 * s.nz * s.nx * 8 + 2 * s.ns * 8 + 2 * info["npair"] * s.ns * 8) if world == 1 else s.nz * s.nx * 8 + 16
 
     # roofline of the FD step kernels from the per-phase CUDA events of the timed steps
     fwd_ms = statistics.mean(p[0] for p in phases)
     adj_ms = statistics.mean(p[2] for p in phases)
     spec_ms = statistics.mean(p[1] for p in phases)
-    cells = s.nzbc * s.nxbc * s.ns
-    inner = s.nz * s.nx * s.ns
-    fwd_bytes = cells * 84 + inner * 16 / s.nt_wf            # per launch (one time step of every shot)
+    nloc = sg.local.ns  # shots of this rank: one FD launch steps all of them
+    cells = s.nzbc * s.nxbc * nloc
+    inner = s.nz * s.nx * nloc
+    # algorithmic bytes per launch (one time step of every shot): the reference's two-phase
+    # schedule, 84 B per padded cell-step, plus 16 B snapshot write (forward) or 16 B snapshot
+    # read + 48 B FP64 image update (adjoint) per interior cell every nt_wf steps
+    fwd_bytes = cells * 84 + inner * 16 / s.nt_wf
     adj_bytes = cells * 84 + inner * (16 + 48) / s.nt_wf
+    fwd_comp = cells * COMPULSORY_STATE_B + inner * 12 / s.nt_wf
+    adj_comp = cells * COMPULSORY_STATE_B + inner * (12 + 48) / s.nt_wf
     fwd_launch_ms = fwd_ms / s.nt
-    adj_launch_ms = adj_ms / (s.nt - 1)
+    # checkpoint mode: the adjoint phase also re-runs the forward steps segment by segment
+    adj_launch_ms = ((adj_ms - fwd_ms) if info["mode"] == 2 else adj_ms) / (s.nt - 1)
     peak, peak_kind = peaks()
 
-    def roof(name, nbytes, launch_ms):
+    def roof(name, nbytes, comp, launch_ms):
         ach = nbytes / (launch_ms / 1e3) / 1e9
         tr = NCU_BYTES_PER_CELL_STEP.get(name)
         return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                 "fallback 6650 GB/s", "traffic": (tr * cells) if tr else None,
-                "algorithmic_bytes_per_launch": nbytes, "avg_launch_ms": launch_ms}
+                "traffic_source": "ncu, plain-step variant" if tr else None,
+                "algorithmic_bytes_per_launch": nbytes, "avg_launch_ms": launch_ms,
+                "compulsory_bytes_per_launch": comp,
+                "frac_compulsory": comp / (launch_ms / 1e3) / 1e9 / peak}
 
-    rf = roof("fd_fwd_step", fwd_bytes, fwd_launch_ms)
-    ra = roof("fd_adj_step", adj_bytes, adj_launch_ms)
+    rf = roof("fd_fwd_step", fwd_bytes, fwd_comp, fwd_launch_ms)
+    ra = roof("fd_adj_step", adj_bytes, adj_comp, adj_launch_ms)
     dominant, other = (ra, rf) if adj_ms >= fwd_ms else (rf, ra)
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model + Gaussian anomaly)",
             "config": workload_config(s, {"adjoint": {1: "stored strain snapshots", 2: "checkpoint+recompute"}[
                 info["mode"]], "batch": info["batch"], "engine_bytes": info["bytes"],
-                "parallelism": f"shots per GPU, {world} GPU(s)"}),
-            "e2e": {"value": world * s.ns / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
+                "parallelism": f"{s.ns} shots split round-robin over {world} GPU(s), one FP64 all-reduce of "
+                               f"the shot sums per step", "shots_this_rank": nloc}),
+            "e2e": {"value": s.ns / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
             "roofline": dominant, "roofline_other": other,
@@ -305,9 +406,8 @@ def main():
 
     # the plain one-shot-per-launch GPU path on a few shots (rank 0 only, N=1 only)
     if world == 1 and args.plain_shots > 0:
-        from swd_b200 import configs
-        ps = configs.batched_c2(ns=s.ns, nt=s.nt)
-        ps.sx = ps.sx[: args.plain_shots]
+        from swd_b200 import shots
+        ps = shots.subset(s, np.arange(1, args.plain_shots + 1))  # shots 1..k, numbered as in the survey
         with GradientEngine(ps, max_batch=1, use_graphs=False) as pe:
             pe.set_observed(cr0_r[:, : args.plain_shots], cr0_l[:, : args.plain_shots])
             pe.gradient(ps.vp, ps.vs)
@@ -318,7 +418,7 @@ def main():
         line["plain_gpu"] = {"value": args.plain_shots / tp, "unit": UNIT, "shots": args.plain_shots,
                              "how": "same kernels, one shot per launch, no CUDA graphs, host in/out per call"}
         line["batched_over_plain"] = line["e2e"]["value"] / line["plain_gpu"]["value"]
-    eng.close()
+    sg.close()
     if world == 1 and rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(s, args.cpu_shots)
     if rank == 0:

@@ -25,7 +25,8 @@ enum {
   SWD_ERR_CUDA = 3,         /* CUDA runtime error */
   SWD_ERR_OOM = 4,          /* device allocation failed or over the HBM budget */
   SWD_ERR_CANCELLED = 5,    /* a served request was cancelled */
-  SWD_ERR_NUMERIC = 6       /* NaN spectrum column, or interp1 with fewer than two picks */
+  SWD_ERR_NUMERIC = 6,      /* NaN spectrum column, or interp1 with fewer than two picks */
+  SWD_ERR_TIMEOUT = 7       /* swd_server_wait: the request has not finished yet */
 };
 
 /* Precision of the Radon transform (DFT + contraction). */
@@ -179,6 +180,12 @@ typedef struct {
   int offset, m, M, w, ini, pick_method;
   double soft_arg_norm;  /* SoftArgNorm, 1e4 in SWD.m:114 */
   int smooth_z, smooth_x;
+  /* Shots of a larger survey (one rank's share of the parfor of SWD.m:171): shot_no holds the
+   * 1-based shot numbers `is` of these ns shots in that survey and ns_total its shot count; both
+   * set the Radon windows and the side rules (RTrAD.m:4-9, ADWDgrad_1.m:15,47).
+   * shot_no NULL: 1..ns.  ns_total 0: ns. */
+  const int* shot_no;
+  int ns_total;
 } swd_survey;
 
 typedef struct {
@@ -216,6 +223,9 @@ typedef struct {
 
 int swd_engine_create(const swd_survey* survey, const swd_engine_opts* opts, swd_engine** out);
 int swd_engine_destroy(swd_engine* e);
+/* The plan swd_engine_create would make for (s, o): batch, mode and device bytes, without
+ * allocating anything (o->hbm_budget 0 plans against the device's free memory). */
+int swd_engine_plan(const swd_survey* s, const swd_engine_opts* o, swd_engine_info_t* info);
 int swd_engine_info(const swd_engine* e, swd_engine_info_t* info);
 /* Source wavelet s (nt samples), rounded to float as SWD_single.m:92 does. */
 int swd_engine_set_source(swd_engine* e, const double* s);
@@ -245,6 +255,69 @@ int swd_engine_assemble_device(swd_engine* e, const double* d_gsum, double* d_dk
  * sources, adjoint+imaging), summed over batches, in milliseconds. */
 int swd_engine_set_timing(swd_engine* e, int on);
 int swd_engine_phase_times(const swd_engine* e, double* fwd_ms, double* spec_ms, double* adj_ms);
+
+/* ------------------------------------------------------------------------
+ * Served request loop (one GPU): misfit and gradient requests of any survey size
+ * are admitted in arrival order by the HBM footprint of their engines and run
+ * concurrently, each on its own stream.  Engines stay resident between requests
+ * with the same nonzero survey_key (device memory, Radon tables, checkpoint
+ * buffers and captured time loops are reused).  No counterpart in the reference,
+ * whose SWD.m runs one inversion at a time.
+ * ------------------------------------------------------------------------ */
+
+typedef struct swd_server swd_server;
+
+enum { SWD_REQ_GRADIENT = 0, SWD_REQ_MISFIT = 1 };
+
+typedef struct {
+  size_t hbm_budget; /* bytes all engines together may hold (0: 85% of free memory) */
+  int max_inflight;  /* requests on the GPU at once (0: 4); each may plan up to budget/max_inflight */
+  int device;
+  int keep_engines;  /* keep finished engines resident for their survey_key */
+} swd_server_opts;
+
+typedef struct {
+  const swd_survey* survey; /* copied at submit */
+  uint64_t survey_key;      /* nonzero: reuse a resident engine of the same key and survey */
+  int kind;                 /* SWD_REQ_GRADIENT or SWD_REQ_MISFIT */
+  int npair;                /* kept frequency bins (rows of cr0_r / cr0_l) */
+  const double* wavelet;    /* nt samples */
+  const double* vp;         /* nz x nx, column-major */
+  const double* vs;
+  const double* cr0_r;      /* npair x ns observed curves */
+  const double* cr0_l;
+} swd_request;
+
+typedef struct {
+  int status;               /* the request's own SWD_* status */
+  double residual;          /* mean right-side misfit (SWD.m:196) */
+  double queue_ms, run_ms, total_ms; /* submit -> start -> done */
+  int reused_engine;        /* 1 when a resident engine served it */
+  size_t engine_bytes;
+  double* dk_vs;            /* outputs, caller buffers (NULL skipped): nz x nx (gradient only) */
+  double* res_r;            /* ns */
+  double* res_l;            /* ns */
+  double* cr_pre_r;         /* npair x ns */
+  double* cr_pre_l;         /* npair x ns */
+} swd_request_result;
+
+typedef struct {
+  uint64_t submitted, admitted, completed, cancelled, waits_for_memory;
+  int peak_inflight, idle_engines;
+  size_t peak_bytes, bytes_in_use, budget;
+} swd_server_stats_t;
+
+int swd_server_create(const swd_server_opts* opts, swd_server** out);
+/* Queue a request (inputs are copied); *id names it for swd_server_wait / _cancel. */
+int swd_server_submit(swd_server* s, const swd_request* req, uint64_t* id);
+/* Wait up to timeout_ms (< 0: forever) for request id; copies its outputs into out's buffers
+ * and releases it.  SWD_ERR_TIMEOUT leaves it pending; otherwise returns its status. */
+int swd_server_wait(swd_server* s, uint64_t id, int timeout_ms, swd_request_result* out);
+/* Cancel a request that has not started (its wait returns SWD_ERR_CANCELLED). */
+int swd_server_cancel(swd_server* s, uint64_t id);
+int swd_server_stats(swd_server* s, swd_server_stats_t* out);
+/* Cancel queued requests, wait for running ones, free every engine. */
+int swd_server_destroy(swd_server* s);
 
 #ifdef __cplusplus
 }

@@ -86,7 +86,8 @@ def lib():
 def declared_symbols():
     """Every C entry point the Python package binds (here and in engine.py)."""
     from .engine import ENGINE_SYMBOLS
-    return list(_SIGS) + ENGINE_SYMBOLS
+    from .serve import SERVER_SYMBOLS
+    return list(_SIGS) + ENGINE_SYMBOLS + SERVER_SYMBOLS
 
 
 def call(name, *args):

@@ -29,6 +29,7 @@ SOURCES = {
     "radon.cu": [],
     "engine.cu": ["-fmad=false"],
     "pick_noalloc.cu": [],
+    "server.cu": [],
 }
 
 

@@ -47,6 +47,9 @@ class Survey:
     vs: np.ndarray = field(default=None, repr=False)        # current model
     vs_true: np.ndarray = field(default=None, repr=False)   # model generating the observed data
     vp_ratio: float = 1.73
+    # shots of a larger survey (a rank's share): 1-based shot numbers and that survey's shot count
+    shot_no: np.ndarray = field(default=None, repr=False)
+    ns_total: int = 0
 
     @property
     def ns(self):
@@ -157,3 +160,47 @@ def tiny(nz=8, nx=24, nbc=6, nt=400, ns=3, seed=3) -> Survey:
                vs=vs, vs_true=vs * 1.05, offset=12, fmin=40.0, fmax=200.0, df=25.0, vmin=100.0, vmax=800.0,
                dv=5.0, ini=3)
     return s
+
+
+def served_surveys(n=16, seed=4):
+    """Surveys of the served request stream: grids log-uniform from 60 x 200 to 300 x 1200
+    (dx 0.5 m), 8-64 shots spread along the line with an integer spacing, nt 3000-10000 in
+    steps of 50, seeded random layered Vs (150-600 m/s) with a +/-5% checkerboard."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nz = int(round(math.exp(rng.uniform(math.log(60), math.log(300)))))
+        nx = int(round(math.exp(rng.uniform(math.log(200), math.log(1200)))))
+        ns = int(rng.integers(8, 65))
+        M = max(1, (nx - 1) // ns)
+        nt = int(round(rng.uniform(3000, 10000) / 50)) * 50
+        nl = int(rng.integers(3, 7))
+        cuts = np.sort(rng.choice(np.arange(1, nz), nl - 1, replace=False))
+        vel = np.sort(rng.uniform(150.0, 600.0, nl))
+        vs = np.repeat(vel[np.searchsorted(cuts, np.arange(nz), side="right")][:, None], nx, 1)
+        vs = vs * _checker(nz, nx, 10, 0.05, rng)
+        sx = 1 + M * np.arange(ns)
+        out.append(Survey(f"served-{k}-{nz}x{nx}", nz, nx, 0.5, 30, 5e-5, nt, 25.0, sx, np.arange(1, nx + 1), M,
+                          vs=vs, vs_true=vs * 1.02))
+    return out
+
+
+def served_stream(n_requests=64, n_surveys=16, rate=2.0, seed=4):
+    """(arrival time s, survey index, kind, model scale) of a Poisson request stream over the
+    served surveys: half gradients, half line-search misfits, each on a slightly scaled model."""
+    rng = np.random.default_rng(seed + 1)
+    t = np.cumsum(rng.exponential(1.0 / rate, n_requests))
+    idx = rng.integers(0, n_surveys, n_requests)
+    kind = np.where(rng.random(n_requests) < 0.5, "gradient", "misfit")
+    scale = 1.0 + rng.uniform(-0.02, 0.02, n_requests)
+    return list(zip(t.tolist(), idx.tolist(), kind.tolist(), scale.tolist()))
+
+
+def smooth_curve(s, seed=0):
+    """A synthetic observed dispersion curve per shot (npair x ns): a decreasing phase velocity
+    inside the Radon axis, standing in for picks of observed data."""
+    rng = np.random.default_rng(seed)
+    f = np.arange(s.npair)[:, None]
+    span = s.vmax - s.vmin
+    base = s.vmin + span * (0.15 + 0.35 * np.exp(-f / max(1.0, s.npair / 3)))
+    return np.round(base + rng.normal(0, 2.0, (1, s.ns)))

@@ -76,6 +76,8 @@ struct swd_engine {
   swd_survey sv{};
   swd_engine_opts opt{};
   std::vector<int> sx, sz;
+  std::vector<int> shot_no;  // 1-based shot number `is` of each shot in the whole survey
+  int ns_total = 0;          // shots in the whole survey
   FdGeom g{};          // store mode geometry (nrec = nt/nt_wf)
   FdGeom gseg{};       // checkpoint mode segment geometry (nrec = ckpt/nt_wf)
   PrepParams pp{};
@@ -378,7 +380,7 @@ static int check_status(swd_engine* e) {
   SWD_CUDA(cudaStreamSynchronize(e->st));
   for (size_t i = 0; i < stv.size(); ++i)
     if (stv[i]) {
-      set_error("shot %zu %s side: %s", i / 2 + 1, (i & 1) ? "left" : "right",
+      set_error("shot %d %s side: %s", e->shot_no[i / 2], (i & 1) ? "left" : "right",
                 stv[i] == 1 ? "NaN in the dispersion spectrum" : "interp1 needs at least two retained picks");
       return SWD_ERR_NUMERIC;
     }
@@ -448,8 +450,8 @@ static int copy_picks(swd_engine* e, double* res_r, double* res_l, double* crp_r
   double sum = 0.0;
   int cnt = 0;
   for (int s = 0; s < e->ns; ++s) {
-    const bool r_on = side_active(s + 1, 0, e->ns, e->sv.m, e->sv.M, e->sv.w);
-    const bool l_on = side_active(s + 1, 1, e->ns, e->sv.m, e->sv.M, e->sv.w);
+    const bool r_on = side_active(e->shot_no[s], 0, e->ns_total, e->sv.m, e->sv.M, e->sv.w);
+    const bool l_on = side_active(e->shot_no[s], 1, e->ns_total, e->sv.m, e->sv.M, e->sv.w);
     if (res_r) res_r[s] = r_on ? e->h_gres[2 * s] : NAN;
     if (res_l) res_l[s] = l_on ? e->h_gres[2 * s + 1] : NAN;
     for (int f = 0; f < np2; ++f) {  // cr_pre defaults to 1 where a side is skipped (SWD.m:164-165)
@@ -471,22 +473,27 @@ static int copy_plane(swd_engine* e, const double* d_rowmajor, double* h_colmajo
   return SWD_OK;
 }
 
-static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engine** out) {
-  clear_error();
-  SWD_CHECK(s && out, "null argument");
-  *out = nullptr;
+// Validation, geometry and the memory plan of an engine (no device allocation).
+static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engine* e) {
   SWD_CHECK(s->ns >= 1 && s->sx && s->sz, "need ns >= 1 shots with sx/sz");
   SWD_CHECK(s->ng >= 2 && s->dgx >= 1, "need ng >= 2 receivers with spacing dgx >= 1");
   SWD_CHECK(s->source_type >= 1 && s->source_type <= 5, "source_type must be 1..5");
-  auto e = new swd_engine();
-  std::unique_ptr<swd_engine> guard(e);
   e->sv = *s;
   if (o) e->opt = *o; else e->opt.use_graphs = 1;
   e->ns = s->ns;
   e->sx.assign(s->sx, s->sx + s->ns);
   e->sz.assign(s->sz, s->sz + s->ns);
+  e->ns_total = s->ns_total > 0 ? s->ns_total : s->ns;
+  SWD_CHECK(e->ns_total >= e->ns, "ns_total (%d) below ns (%d)", e->ns_total, e->ns);
+  e->shot_no.resize(e->ns);
+  for (int i = 0; i < e->ns; ++i) {
+    e->shot_no[i] = s->shot_no ? s->shot_no[i] : i + 1;
+    SWD_CHECK(e->shot_no[i] >= 1 && e->shot_no[i] <= e->ns_total, "shot_no[%d] = %d outside 1..%d", i,
+              e->shot_no[i], e->ns_total);
+  }
   e->sv.sx = nullptr;
   e->sv.sz = nullptr;
+  e->sv.shot_no = nullptr;
   e->device = e->opt.device;
   SWD_CUDA(cudaSetDevice(e->device));
   // model prep / FD geometry
@@ -505,13 +512,11 @@ static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engi
   g.field = (size_t)g.NZ * g.pitch;
   SWD_CHECK(g.gz >= 1 && g.gz <= g.NZ - 2 && g.gx >= 1 && g.gx + (long)(g.ng - 1) * g.dg <= g.NX - 2,
             "receivers must lie inside the padded grid's rows/cols 1..n-2");
-  std::vector<int2> hsrc(e->ns);
   for (int i = 0; i < e->ns; ++i) {
     const int z = e->sz[i] + pp.pad_top - 1, x = e->sx[i] + s->nbc - 1;
     const int zlo = s->source_type == 2 ? 2 : 1, xhi = s->source_type == 2 ? g.NX - 3 : g.NX - 2;
     SWD_CHECK(z >= zlo && z <= g.NZ - 2 && x >= 1 && x <= xhi, "shot %d source (%d,%d) outside the grid interior",
               i + 1, e->sz[i], e->sx[i]);
-    hsrc[i] = make_int2(z, x);
   }
   e->plane = (size_t)g.nz * g.nx;
   g.warps = e->opt.warps;
@@ -530,9 +535,21 @@ static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engi
   SWD_CHECK(s->ini >= 1 && s->ini <= e->rg.npair, "ini (%d) must lie in 1..npair (%d)", s->ini, e->rg.npair);
   SWD_TRY(plan(e));
   plan_decomposition(g, e->B, e->opt.chunk_rows);
-
   e->gseg = g;
   e->gseg.nrec = e->ckpt / g.nt_wf;
+  return SWD_OK;
+}
+
+static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engine** out) {
+  clear_error();
+  SWD_CHECK(s && out, "null argument");
+  *out = nullptr;
+  auto e = new swd_engine();
+  std::unique_ptr<swd_engine> guard(e);
+  SWD_TRY(engine_setup(s, o, e));
+  std::vector<int2> hsrc(e->ns);
+  for (int i = 0; i < e->ns; ++i)
+    hsrc[i] = make_int2(e->sz[i] + e->pp.pad_top - 1, e->sx[i] + s->nbc - 1);
   SWD_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
   SWD_TRY(alloc_all(e));
   SWD_CUDA(cudaMemcpyAsync(e->src.p, hsrc.data(), e->ns * sizeof(int2), cudaMemcpyHostToDevice, e->st));
@@ -544,9 +561,9 @@ static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engi
       for (int side = 0; side < 2; ++side) {
         Gather gg{};
         if (sidx < e->ns) {
-          gg = make_gather(e->rg, sidx + 1, side, b, e->ns, s->w);
-          SWD_CHECK(gg.valid >= 0, "shot %d: the %s window is empty or leaves the receiver line", sidx + 1,
-                    side ? "left" : "right");
+          gg = make_gather(e->rg, e->shot_no[sidx], side, b, e->ns_total, s->w);
+          SWD_CHECK(gg.valid >= 0, "shot %d: the %s window is empty or leaves the receiver line",
+                    e->shot_no[sidx], side ? "left" : "right");
         }
         hg[((size_t)bi * e->B + b) * 2 + side] = gg;
       }
@@ -574,9 +591,7 @@ int swd_engine_destroy(swd_engine* e) {
   return SWD_OK;
 }
 
-int swd_engine_info(const swd_engine* e, swd_engine_info_t* info) {
-  clear_error();
-  SWD_CHECK(e && info, "null argument");
+static void fill_info(const swd_engine* e, swd_engine_info_t* info) {
   info->batch = e->B;
   info->nbatch = e->nbatch;
   info->mode = e->mode;
@@ -592,6 +607,21 @@ int swd_engine_info(const swd_engine* e, swd_engine_info_t* info) {
   info->cells = e->g.cells;
   info->ring_fwd = e->g.ring_fwd;
   info->ring_adj = e->g.ring_adj;
+}
+
+int swd_engine_info(const swd_engine* e, swd_engine_info_t* info) {
+  clear_error();
+  SWD_CHECK(e && info, "null argument");
+  fill_info(e, info);
+  return SWD_OK;
+}
+
+int swd_engine_plan(const swd_survey* s, const swd_engine_opts* o, swd_engine_info_t* info) {
+  clear_error();
+  SWD_CHECK(s && info, "null argument");
+  swd_engine e;
+  SWD_TRY(engine_setup(s, o, &e));
+  fill_info(&e, info);
   return SWD_OK;
 }
 
@@ -679,7 +709,8 @@ int swd_engine_shot_sums_device(swd_engine* e, const double* d_vp, const double*
   double r = 0;
   SWD_TRY(copy_picks(e, nullptr, nullptr, nullptr, nullptr, &r));
   int cnt = 0;
-  for (int s = 0; s < e->ns; ++s) cnt += side_active(s + 1, 0, e->ns, e->sv.m, e->sv.M, e->sv.w) ? 1 : 0;
+  for (int s = 0; s < e->ns; ++s)
+    cnt += side_active(e->shot_no[s], 0, e->ns_total, e->sv.m, e->sv.M, e->sv.w) ? 1 : 0;
   if (res_sum) *res_sum = cnt ? r * cnt : 0.0;
   if (res_count) *res_count = cnt;
   return SWD_OK;

@@ -29,7 +29,8 @@ class SurveyC(ctypes.Structure):
                 ("source_type", _i), ("dx", _d), ("dt", _d), ("ns", _i), ("sx", _ip), ("sz", _ip), ("ng", _i),
                 ("gx0", _i), ("dgx", _i), ("gz", _i), ("df", _d), ("fmin", _d), ("fmax", _d), ("vmin", _d),
                 ("vmax", _d), ("dv", _d), ("offset", _i), ("m", _i), ("M", _i), ("w", _i), ("ini", _i),
-                ("pick_method", _i), ("soft_arg_norm", _d), ("smooth_z", _i), ("smooth_x", _i)]
+                ("pick_method", _i), ("soft_arg_norm", _d), ("smooth_z", _i), ("smooth_x", _i),
+                ("shot_no", _ip), ("ns_total", _i)]
 
 
 class EngineOpts(ctypes.Structure):
@@ -93,12 +94,14 @@ def survey_struct(s):
     sx = np.ascontiguousarray(np.asarray(s.sx, np.int32))
     sz = np.ascontiguousarray(np.ones(s.ns, np.int32))
     gx = np.asarray(s.gx)
+    shot_no = None if s.shot_no is None else np.ascontiguousarray(np.asarray(s.shot_no, np.int32))
     c = SurveyC(nz=s.nz, nx=s.nx, nbc=s.nbc, nt=s.nt, nt_wf=s.nt_wf, fd_order=s.fd_order, isfs=s.isfs,
                 source_type=_SRC[s.source_type], dx=s.dx, dt=s.dt, ns=s.ns, sx=sx.ctypes.data_as(_ip),
                 sz=sz.ctypes.data_as(_ip), ng=s.ng, gx0=int(gx[0]), dgx=int(gx[1] - gx[0]), gz=1, df=s.df,
                 fmin=s.fmin, fmax=s.fmax, vmin=s.vmin, vmax=s.vmax, dv=s.dv, offset=s.offset, m=s.m, M=s.M, w=s.w,
-                ini=s.ini, pick_method=1, soft_arg_norm=s.soft_arg_norm, smooth_z=s.smooth_z, smooth_x=s.smooth_x)
-    c._keep = (sx, sz)
+                ini=s.ini, pick_method=1, soft_arg_norm=s.soft_arg_norm, smooth_z=s.smooth_z, smooth_x=s.smooth_x,
+                shot_no=shot_no.ctypes.data_as(_ip) if shot_no is not None else None, ns_total=int(s.ns_total))
+    c._keep = (sx, sz, shot_no)
     return c
 
 

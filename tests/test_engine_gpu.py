@@ -87,3 +87,38 @@ def test_plain_30x120_gradient(O):
     for k in ("g_cl", "g_cm", "g_illum", "dk_vs"):
         assert _rel(out[k], ref[k]) < TOL, (k, _rel(out[k], ref[k]))
     assert out["residual"] == pytest.approx(ref["residual"], rel=1e-12)
+
+
+def test_sharded_engines_sum_to_the_full_survey(tiny_case):
+    """Shots split over two engines (two ranks' shares, run one after the other on one GPU):
+    picks and misfits per shot are identical and the FP64 shot sums add up to the full ones."""
+    import torch
+
+    from swd_b200 import shots
+    s, cr0_r, cr0_l, _ = tiny_case
+    with GradientEngine(s) as e:
+        e.set_observed(cr0_r, cr0_l)
+        full = e.gradient(s.vp, s.vs)
+    n = s.nz * s.nx
+    d_vp = torch.from_numpy(np.ascontiguousarray(s.vp.T)).cuda()
+    d_vs = torch.from_numpy(np.ascontiguousarray(s.vs.T)).cuda()
+    total = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    rsum, rcnt = 0.0, 0
+    for rank in range(2):
+        mine = shots.shard(s.ns, 2, rank)
+        local = shots.subset(s, mine)
+        with GradientEngine(local) as e:
+            e.set_observed(cr0_r[:, mine - 1], cr0_l[:, mine - 1])
+            part = e.gradient(s.vp, s.vs)
+            assert np.array_equal(part["cr_pre_r"], full["cr_pre_r"][:, mine - 1])
+            assert np.array_equal(part["cr_pre_l"], full["cr_pre_l"][:, mine - 1])
+            np.testing.assert_array_equal(part["res_r"], full["res_r"][mine - 1])
+            g = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+            a, c = e.shot_sums_device(d_vp, d_vs, g)
+            torch.cuda.synchronize()
+            total += g
+            rsum, rcnt = rsum + a, rcnt + c
+    t = total.cpu().numpy().reshape(3, s.nz, s.nx)
+    for k, key in enumerate(("g_cl", "g_cm", "g_illum")):
+        np.testing.assert_allclose(t[k], full[key], rtol=1e-12, atol=1e-300 + 1e-14 * np.abs(full[key]).max())
+    assert rsum / rcnt == pytest.approx(full["residual"], rel=1e-12)
