@@ -63,6 +63,8 @@ def parse():
     p.add_argument("--rate", type=float, default=2.0, help="served stream: Poisson arrival rate, requests/s")
     p.add_argument("--inflight", type=int, default=4, help="served stream: requests on the GPU at once")
     p.add_argument("--surveys", type=int, default=16, help="served stream: distinct surveys (engine keys)")
+    p.add_argument("--radon", action="store_true",
+                   help="Radon contraction precision study (200 f x 400 v x 600 offsets x 96 shots)")
     p.add_argument("--plain-sample", type=int, default=8,
                    help="served stream: requests re-run serially on the plain path for the comparison")
     return p.parse_args()
@@ -258,12 +260,94 @@ def run_serve(args):
     return 0
 
 
+def radon_inputs(nf=200, npv=400, nx=600, ns=96, nt=1000, dt=1e-3, seed=11):
+    """Axes of the precision study and complex64 spectra of seeded band-limited Gaussian traces:
+    white noise band-passed to 3-80 Hz in the FFT domain, then a direct DFT at the nf frequencies."""
+    rng = np.random.default_rng(seed)
+    freq = np.linspace(3.0, 80.0, nf)
+    vel = np.linspace(80.0, 1200.0, npv)
+    off = np.arange(nx) * 0.5
+    u = rng.standard_normal((ns * nx, nt)).astype(np.float32)
+    fu = np.fft.rfft(u, axis=1)
+    fr = np.fft.rfftfreq(nt, dt)
+    fu[:, (fr < 3.0) | (fr > 80.0)] = 0
+    u = np.fft.irfft(fu, nt, axis=1).astype(np.float32)
+    e = np.exp(-2j * np.pi * np.outer(np.arange(nt) * dt, freq)).astype(np.complex64)  # [t, f]
+    spec = (u @ e).reshape(ns, nx, nf).transpose(0, 2, 1)  # [s, f, x]
+    return freq, vel, off, np.ascontiguousarray(spec.astype(np.complex64).astype(np.complex128))
+
+
+def run_radon(args):
+    """Radon contraction in FP64, FP32 (CUDA cores) and split-BF16 (tcgen05): time per launch,
+    GFLOP/s, tensor-pipe FLOP/s against the measured bf16 peak, and the error of the spectrum,
+    its column-normalised amplitude and its argmax picks against the FP64 path."""
+    import torch
+
+    from swd_b200 import kernel_launches
+    from swd_b200.contract import Contraction
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    freq, vel, off, spec = radon_inputs()
+    ns = spec.shape[0]
+    d_spec = torch.from_numpy(spec).cuda()
+    peaks_j = {}
+    pf = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(pf):
+        peaks_j = json.load(open(pf))
+    out, ref = {}, None
+    for prec in ("fp64", "fp32", "bf16x2", "bf16x3"):
+        with Contraction(freq, vel, off, ns, prec) as c:
+            d_mm = torch.zeros(c.shape_out, dtype=torch.complex128, device="cuda")
+            st = torch.cuda.current_stream()
+            for _ in range(max(3, args.warmup)):
+                c.run(d_spec, d_mm, st)
+            torch.cuda.synchronize()
+            reps = max(5, args.steps)
+            l0 = kernel_launches()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(reps):
+                c.run(d_spec, d_mm, st)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / reps
+            useful, issued = c.flops()
+            timed_out = c.timed_out()
+            mm = d_mm.cpu().numpy()
+        r = {"ms": ms, "gflops": useful / ms / 1e6, "launches_per_run": (kernel_launches() - l0) / reps,
+             "timed_out": timed_out}
+        if prec.startswith("bf16"):
+            tf = issued / ms / 1e9
+            pk = peaks_j.get("bf16_tflops", 1590.0)
+            r["tensor"] = {"achieved": tf, "peak": pk, "unit": "TFLOP/s", "frac": tf / pk,
+                           "peak_source": "measured bf16_tflops" if peaks_j else "fallback 1590"}
+        if ref is None:
+            ref = mm
+        else:
+            amp, aref = np.abs(mm), np.abs(ref)
+            nmax, rmax = amp / amp.max(axis=2, keepdims=True), aref / aref.max(axis=2, keepdims=True)
+            r["rel_l2_mm"] = float(np.linalg.norm(mm - ref) / np.linalg.norm(ref))
+            r["rel_l2_spectrum"] = float(np.linalg.norm(nmax - rmax) / np.linalg.norm(rmax))
+            r["pick_agreement"] = float(np.mean(amp.argmax(axis=2) == aref.argmax(axis=2)))
+        out[prec] = r
+    line = {"metric": "Radon contraction GFLOP/s (split-BF16 tcgen05)", "value": out["bf16x2"]["gflops"],
+            "unit": "GFLOP/s", "n_gpus": 1, "higher_is_better": True, "dtype": "bf16x2 (FP32 accumulate)",
+            "data": "synthetic: complex64 spectra of seeded band-limited Gaussian traces",
+            "config": {"workload": "200 frequencies 3-80 Hz x 400 velocities 80-1200 m/s x 600 offsets 0.5 m x "
+                                   "96 shots", "useful_gflop": 8 * 200 * 400 * 600 * 96 / 1e9},
+            "precisions": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.serve:
         return run_serve(args)
+    if args.radon:
+        return run_radon(args)
     import torch
     import torch.distributed as dist
 

@@ -257,6 +257,28 @@ int swd_engine_set_timing(swd_engine* e, int on);
 int swd_engine_phase_times(const swd_engine* e, double* fwd_ms, double* spec_ms, double* adj_ms);
 
 /* ------------------------------------------------------------------------
+ * Batched Radon contraction with general axes (the slant stack of RTrAD.m:20-26
+ * for many shots at once): mm[s][f][p] = sum_x exp(i*2*pi*freq[f]*offset[x]/vel[p])
+ * * spec[s][f][x].  spec and mm are DEVICE arrays of interleaved complex doubles,
+ * [ns][nf][nx] and [ns][nf][np].  precision: SWD_PREC_FP64 / _FP32 (CUDA cores)
+ * or _BF16X2 / _BF16X3 (tcgen05 tensor cores, split-BF16 operands, FP32 accumulate).
+ * The kernel table is built once at create time.
+ * ------------------------------------------------------------------------ */
+
+typedef struct swd_contract swd_contract;
+
+int swd_contract_create(int nf, const double* freq, int np, const double* vel, int nx, const double* offset,
+                        int ns, int precision, int device, swd_contract** out);
+/* Enqueue one contraction on `stream` (a cudaStream_t; NULL: legacy default stream). */
+int swd_contract_run(swd_contract* c, const double* d_spec, double* d_mm, void* stream);
+/* 1 in *timed_out when a tensor-core launch gave up waiting on its MMAs (results invalid). */
+int swd_contract_status(swd_contract* c, int* timed_out);
+/* Useful FLOPs (8 per complex multiply-add) and the FLOPs the tensor cores execute
+ * (padded tiles x split products; equal to useful on CUDA cores). */
+int swd_contract_flops(const swd_contract* c, double* useful, double* issued);
+int swd_contract_destroy(swd_contract* c);
+
+/* ------------------------------------------------------------------------
  * Served request loop (one GPU): misfit and gradient requests of any survey size
  * are admitted in arrival order by the HBM footprint of their engines and run
  * concurrently, each on its own stream.  Engines stay resident between requests

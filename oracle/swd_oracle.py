@@ -712,3 +712,11 @@ def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=True):
            "cr_pre_r": np.stack([p["crp_r"] for p in per], 1), "cr_pre_l": np.stack([p["crp_l"] for p in per], 1),
            "residual": float(np.nanmean(res_r)), "per_shot": per}
     return out
+
+
+def contract(freq, vel, off, spec):
+    """Slant stack of RTrAD.m:20-26 with general axes, for a batch of shots:
+    mm[s,f,p] = sum_x exp(1i*2*pi*freq[f]*off[x]/vel[p]) * spec[s,f,x]   (FP64)."""
+    freq, vel, off = (np.asarray(a, np.float64) for a in (freq, vel, off))
+    th = 2 * np.pi * freq[:, None, None] * off[None, None, :] / vel[None, :, None]  # [f,p,x]
+    return np.einsum("fpx,sfx->sfp", np.exp(1j * th), np.asarray(spec, np.complex128))

@@ -86,8 +86,9 @@ def lib():
 def declared_symbols():
     """Every C entry point the Python package binds (here and in engine.py)."""
     from .engine import ENGINE_SYMBOLS
+    from .contract import CONTRACT_SYMBOLS
     from .serve import SERVER_SYMBOLS
-    return list(_SIGS) + ENGINE_SYMBOLS + SERVER_SYMBOLS
+    return list(_SIGS) + ENGINE_SYMBOLS + SERVER_SYMBOLS + CONTRACT_SYMBOLS
 
 
 def call(name, *args):

@@ -30,6 +30,7 @@ SOURCES = {
     "engine.cu": ["-fmad=false"],
     "pick_noalloc.cu": [],
     "server.cu": [],
+    "radon_tc.cu": [],
 }
 
 
