@@ -65,6 +65,8 @@ def parse():
     p.add_argument("--surveys", type=int, default=16, help="served stream: distinct surveys (engine keys)")
     p.add_argument("--radon", action="store_true",
                    help="Radon contraction precision study (200 f x 400 v x 600 offsets x 96 shots)")
+    p.add_argument("--precision", action="store_true",
+                   help="FP32 engine vs the full-FP64 per-shot path: seismograms, spectra, picks, gradient, misfit")
     p.add_argument("--plain-sample", type=int, default=8,
                    help="served stream: requests re-run serially on the plain path for the comparison")
     return p.parse_args()
@@ -340,8 +342,63 @@ def run_radon(args):
     return 0
 
 
+def run_precision(args):
+    """Relative errors of the FP32 path against the full-FP64 path on the same inputs.
+
+    FP32 path: the batched engine (FP32 FD with FP64 image accumulation, FP64 spectra, picks
+    and SoftMax) and, for seismograms and spectra, the FP32 MEX-convention calls per shot.
+    FP64 path: SWD.m's shot loop on the double MEX pair (swd_b200.swd_loop, single=False).
+    Both use the same observed curves (the FP32 engine's picks of the true model)."""
+    from swd_b200 import configs, shots, swd_loop
+    from swd_b200.engine import GradientEngine
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+
+    def rel(a, b):
+        a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+        return float(np.linalg.norm((a - b).ravel()) / np.linalg.norm(b.ravel()))
+
+    cases = (("plain-30x120, 12 shots, nt 6000", configs.plain_c1()),
+             ("batched-100x600, shots 1/25/49/73 of 96, nt 8000",
+              shots.subset(configs.batched_c2(), [1, 25, 49, 73])))
+    out = {}
+    for name, s in cases:
+        with GradientEngine(s) as e:
+            cr0_r, cr0_l = e.observed_curves(s.vp_true, s.vs_true)
+            e.set_observed(cr0_r, cr0_l)
+            g32 = e.gradient(s.vp, s.vs)
+        g64 = swd_loop.gradient(s, s.vs, cr0_r, cr0_l, single=False, keep_shots=True)
+        seis, spec = [], []
+        for is_ in range(1, s.ns + 1):
+            sw32, _ = swd_loop._seismogram(s, is_, s.vs, True)
+            p64 = g64["per_shot"][is_ - 1]
+            seis.append(rel(sw32, p64["seismo_w"]))
+            sp32 = swd_loop.spectra(s, sw32, is_)
+            for side in ("r", "l"):
+                if side in sp32:
+                    spec.append(rel(sp32[side][0], p64["ml_" + side]))
+        picks32 = np.concatenate([g32["cr_pre_r"].ravel(), g32["cr_pre_l"].ravel()])
+        picks64 = np.concatenate([g64["cr_pre_r"].ravel(), g64["cr_pre_l"].ravel()])
+        out[name] = {
+            "seismogram_rel_l2": {"max": max(seis), "median": float(np.median(seis))},
+            "spectrum_rel_l2": {"max": max(spec), "median": float(np.median(spec))},
+            "picks": {"identical_fraction": float(np.mean(picks32 == picks64)),
+                      "max_abs_diff_m_s": float(np.max(np.abs(picks32 - picks64)))},
+            "gradient_rel_l2": {k: rel(g32[k], g64[k]) for k in ("dk_vs", "g_cl", "g_cm", "g_illum")},
+            "misfit_rel": abs(g32["residual"] - g64["residual"]) / abs(g64["residual"]),
+        }
+    line = {"metric": "FP32 path relative error vs full FP64", "value": max(v["gradient_rel_l2"]["dk_vs"]
+                                                                           for v in out.values()),
+            "unit": "relative L2 of the Vs gradient (worst case)", "higher_is_better": False, "n_gpus": 1,
+            "dtype": "f32 FD, f64 accumulation / spectra / SoftMax", "data": "synthetic", "cases": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.precision:
+        return run_precision(args)
     if args.impl == "reference":
         return run_reference(args)
     if args.serve:

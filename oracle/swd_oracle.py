@@ -671,9 +671,10 @@ def observed_curves(s, vs, single=True):
     return cr, cl
 
 
-def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True):
-    """SWD_single.m:172-193 for one shot: forward (FP32), spectra, picks, ADWDgrad_1, adjoint."""
-    inp = _survey_fd(s, is_, vs)
+def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True, single=True):
+    """SWD_single.m:172-193 for one shot: forward (FP32), spectra, picks, ADWDgrad_1, adjoint.
+    single=False: SWD.m's double path (FP64 FD, adjoint source kept in double)."""
+    inp = _survey_fd(s, is_, vs, single)
     _, sw, wf = mex_staggerfd(inp, s.source())
     sp = _spectra(s, sw.astype(np.float64), is_)
     npair = s.npair
@@ -686,21 +687,21 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True):
     gl = out["crp_l"] - cr0_l[:, is_ - 1]
     a = ADWDgrad_1(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl,
                    sp.get("r", (0, 0, None))[2], sp.get("l", (0, 0, None))[2])
-    out["adj_src"] = a.astype(np.float32)
-    ainp = _survey_fd(s, is_, vs, adjoint=True)
+    out["adj_src"] = a.astype(np.float32) if single else a
+    ainp = _survey_fd(s, is_, vs, single, adjoint=True)
     out["cl"], out["cm"], out["il"] = mex_e2drtm(ainp, out["adj_src"], wf, accum_fp64)
     return out
 
 
-def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=True):
-    """SWD_single.m:171-201 with the shot sum in FP64 in shot order."""
+def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=True, single=True):
+    """SWD_single.m:171-201 (SWD.m with single=False) with the shot sum in FP64 in shot order."""
     from concurrent.futures import ThreadPoolExecutor
     shots = list(range(1, s.ns + 1))
     if threads > 1:
         with ThreadPoolExecutor(threads) as ex:
-            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64), shots))
+            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single), shots))
     else:
-        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64) for i in shots]
+        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single) for i in shots]
     g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
     for p in per:
         for k in g:

@@ -1,0 +1,131 @@
+"""The shot loops of SWD.m / SWD_single.m on the MEX-convention entry points.
+
+This is what the reference's driver runs once the MEX shims stand in for its MEX files:
+one shot per call, as the body of its parfor (SWD.m:171-201), with the spectra, picks and
+SoftMax adjoint sources of the .m functions (RTrAD/RTlAD, LHDispPick, ADWDgrad_1).
+
+    single=True   SWD_single.m: FP32 FD (eigen_staggerfd_single / eigen_e2drtm_single), the
+                  adjoint source cast to single (SWD_single.m:193)
+    single=False  SWD.m: FP64 FD (the _double MEX pair), all in double
+
+The batched engine (swd_b200.engine) computes the same gradient in one pipeline; this loop
+is the per-shot path and the full-FP64 path the engine's precision is measured against.
+Images are accumulated in FP64 in both modes.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from .fd import e2drtm_eigen, e2drtm_eigend, staggerfd_eigen, staggerfd_eigend
+from .spectrum import ADWDgrad_1, LHDispPick, RTlAD, RTrAD
+
+
+def _mround(x):
+    return int(math.floor(x + 0.5)) if x >= 0 else -int(math.floor(-x + 0.5))
+
+
+def has_right(is_, ns, m, M, w):
+    """ADWDgrad_1.m:13 / SWD.m:175."""
+    return is_ <= ns - math.floor(m / M) - _mround(w / M)
+
+
+def has_left(is_, m, M, w):
+    """ADWDgrad_1.m:46 / SWD.m:181."""
+    return is_ >= _mround(w / M) + math.floor(m / M) + 1
+
+
+def smooth2a(a, nr, nc):
+    """smooth2a(A, Nr, Nc) (core/smooth2a.m:52-76): mean over the (2Nr+1) x (2Nc+1) window
+    clipped to the grid; NaNs are left out of sums and counts and stay NaN."""
+    a = np.asarray(a, np.float64)
+    nz, nx = a.shape
+    ok = ~np.isnan(a)
+    v = np.where(ok, a, 0.0)
+    s = np.zeros_like(v)
+    n = np.zeros_like(v)
+    for dz in range(-nr, nr + 1):
+        for dx in range(-nc, nc + 1):
+            z0, z1 = max(0, -dz), min(nz, nz - dz)
+            x0, x1 = max(0, -dx), min(nx, nx - dx)
+            s[z0:z1, x0:x1] += v[z0 + dz:z1 + dz, x0 + dx:x1 + dx]
+            n[z0:z1, x0:x1] += ok[z0 + dz:z1 + dz, x0 + dx:x1 + dx]
+    out = s / n
+    out[~ok] = np.nan
+    return out
+
+
+def _seismogram(s, is_, vs, single, want_wf=True):
+    fd = staggerfd_eigen if single else staggerfd_eigend
+    su, sw, www = fd(is_, s.nbc, s.nt, s.dtx, s.dx, s.dt, int(s.sx[is_ - 1]), 1, s.gx, np.ones(s.ng), s.source(),
+                     s.vp_ratio * vs, vs, s.isfs, s.fd_order, s.source_type, 0, s.nt_wf)
+    return sw, www
+
+
+def spectra(s, seismo, is_):
+    """RTrAD / RTlAD of one shot's vertical-component record for the sides it has (SWD.m:174-185)."""
+    shot_no = int(s.shot_no[is_ - 1]) if s.shot_no is not None else is_
+    ns = s.ns_total or s.ns
+    args = (shot_no, s.df, s.dt, s.np_vel, s.vmin, s.vmax, s.fmin, s.fmax, s.nt, s.ng, s.ds, s.offset, s.m, s.M,
+            s.dv)
+    out = {}
+    if has_right(shot_no, ns, s.m, s.M, s.w):
+        out["r"] = RTrAD(np.asarray(seismo, np.float64), *args)
+    if has_left(shot_no, s.m, s.M, s.w):
+        out["l"] = RTlAD(np.asarray(seismo, np.float64), *args)
+    return out
+
+
+def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True):
+    """SWD.m:172-193 for shot is_ (1-based in s): images cl, cm, illum plus picks and misfits."""
+    sw, www = _seismogram(s, is_, vs, single)
+    sp = spectra(s, sw, is_)
+    npair = s.npair
+    shot_no = int(s.shot_no[is_ - 1]) if s.shot_no is not None else is_
+    ns = s.ns_total or s.ns
+    out = {"seismo_w": sw, "res_r": np.nan, "res_l": np.nan, "crp_r": np.ones(npair), "crp_l": np.ones(npair)}
+    if "r" in sp:
+        out["ml_r"] = sp["r"][0]
+        out["res_r"], out["crp_r"] = LHDispPick(sp["r"][0], s.vmin, cr0_r[:, is_ - 1], 1, s.ini)
+    if "l" in sp:
+        out["ml_l"] = sp["l"][0]
+        out["res_l"], out["crp_l"] = LHDispPick(sp["l"][0], s.vmin, cr0_l[:, is_ - 1], 1, s.ini)
+    gr = out["crp_r"] - cr0_r[:, is_ - 1]  # SWD.m:186-187
+    gl = out["crp_l"] - cr0_l[:, is_ - 1]
+    space = np.repeat(np.arange(1.0, s.np_vel + 1)[:, None], npair, 1)  # SWD.m:133-136
+    a = ADWDgrad_1(s.nt, s.ng, ns, npair, shot_no, s.w, s.m, s.M, s.soft_arg_norm, gr, gl, space,
+                   sp["r"][2] if "r" in sp else None, sp["l"][2] if "l" in sp else None)
+    if single:
+        a = a.astype(np.float32)  # SWD_single.m:193
+        cl, cm, il = e2drtm_eigen(www, a, is_, s.nbc, s.nt, s.dtx, s.dx, s.dt, s.gx, np.ones(s.ng), s.source(),
+                                  s.vp_ratio * vs, vs, s.isfs, s.fd_order, 0, s.nt_wf, fp64_out=True)
+    else:
+        cl, cm, il = e2drtm_eigend(www, a, is_, s.nbc, s.nt, s.dtx, s.dx, s.dt, s.gx, np.ones(s.ng), s.source(),
+                                   s.vp_ratio * vs, vs, s.isfs, s.fd_order, 0, s.nt_wf)
+    out.update(cl=np.asarray(cl, np.float64), cm=np.asarray(cm, np.float64), il=np.asarray(il, np.float64))
+    return out
+
+
+def gradient(s, vs, cr0_r, cr0_l, single=True, keep_shots=False):
+    """SWD.m:171-201: shot sums in shot order (FP64), Vs gradient, smoothing, misfit."""
+    g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
+    res_r, res_l, crp_r, crp_l, per = [], [], [], [], []
+    for is_ in range(1, s.ns + 1):
+        p = shot_gradient(s, is_, vs, cr0_r, cr0_l, single)
+        for k in g:
+            g[k] = g[k] + p[k]
+        res_r.append(p["res_r"])
+        res_l.append(p["res_l"])
+        crp_r.append(p["crp_r"])
+        crp_l.append(p["crp_l"])
+        if keep_shots:
+            per.append(p)
+    dk = -4 * vs * (g["cl"] / g["il"]) + 2 * vs * (g["cm"] / g["il"])  # SWD.m:199-200
+    res_r = np.array(res_r)
+    out = {"g_cl": g["cl"], "g_cm": g["cm"], "g_illum": g["il"], "dk_vs": smooth2a(dk, s.smooth_z, s.smooth_x),
+           "res_r": res_r, "res_l": np.array(res_l), "cr_pre_r": np.stack(crp_r, 1), "cr_pre_l": np.stack(crp_l, 1),
+           "residual": float(np.nanmean(res_r)) if np.any(~np.isnan(res_r)) else float("nan")}
+    if keep_shots:
+        out["per_shot"] = per
+    return out
