@@ -367,6 +367,9 @@ def run_precision(args):
             cr0_r, cr0_l = e.observed_curves(s.vp_true, s.vs_true)
             e.set_observed(cr0_r, cr0_l)
             g32 = e.gradient(s.vp, s.vs)
+        with GradientEngine(s, radon_precision="bf16x2") as e:  # FP32 FD + split-BF16 Radon
+            e.set_observed(cr0_r, cr0_l)
+            gbf = e.gradient(s.vp, s.vs)
         g64 = swd_loop.gradient(s, s.vs, cr0_r, cr0_l, single=False, keep_shots=True)
         seis, spec = [], []
         for is_ in range(1, s.ns + 1):
@@ -387,6 +390,12 @@ def run_precision(args):
             "gradient_rel_l2": {k: rel(g32[k], g64[k]) for k in ("dk_vs", "g_cl", "g_cm", "g_illum")},
             "misfit_rel": abs(g32["residual"] - g64["residual"]) / abs(g64["residual"]),
         }
+        pbf = np.concatenate([gbf["cr_pre_r"].ravel(), gbf["cr_pre_l"].ravel()])
+        out[name]["with_split_bf16_radon"] = {
+            "picks_identical_fraction": float(np.mean(pbf == picks64)),
+            "picks_max_abs_diff_m_s": float(np.max(np.abs(pbf - picks64))),
+            "gradient_rel_l2": rel(gbf["dk_vs"], g64["dk_vs"]),
+            "misfit_rel": abs(gbf["residual"] - g64["residual"]) / abs(g64["residual"])}
     line = {"metric": "FP32 path relative error vs full FP64", "value": max(v["gradient_rel_l2"]["dk_vs"]
                                                                            for v in out.values()),
             "unit": "relative L2 of the Vs gradient (worst case)", "higher_is_better": False, "n_gpus": 1,
@@ -421,9 +430,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     s = survey(args)
     # this rank's share of the survey's shots (all of them at N=1)
+    # the engine times its FD kernel variants on this survey unless a shape is given
+    tune = not (args.warps or args.cells or args.ring or args.chunk)
     sg = ShardedGradient(s, world, rank, device=local, snapshot_mode=args.snapshot_mode,
                          ckpt_interval=args.ckpt, warps=args.warps, cells=args.cells, ring_fwd=args.ring,
-                         ring_adj=args.ring, chunk_rows=args.chunk)
+                         ring_adj=args.ring, chunk_rows=args.chunk, autotune=tune)
     eng = sg.engine
     info = eng.info
     # observed curves of the "true" model (setup, SWD.m:155-162), then resident inputs
@@ -536,6 +547,8 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model + Gaussian anomaly)",
             "config": workload_config(s, {"adjoint": {1: "stored strain snapshots", 2: "checkpoint+recompute"}[
                 info["mode"]], "batch": info["batch"], "engine_bytes": info["bytes"],
+                "fd_variant": {k: info[k] for k in ("warps", "cells", "ring_fwd", "ring_adj", "chunk_rows")} |
+                {"autotuned": tune},
                 "parallelism": f"{s.ns} shots split round-robin over {world} GPU(s), one FP64 all-reduce of "
                                f"the shot sums per step", "shots_this_rank": nloc}),
             "e2e": {"value": s.ns / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,

@@ -10,6 +10,7 @@
 // then illumination normalisation, Vs gradient and smoothing (SWD.m:196-201).
 // Time loops are captured once into CUDA graphs and replayed on later calls.
 // Compiled with -fmad=false like the FD kernels.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <map>
@@ -100,6 +101,8 @@ struct swd_engine {
   DevBuf cr0, crp, dc, gres, status;
   DevBuf outbuf;       // staging for host outputs
   bool have_source = false, have_observed = false;
+  double tuned_fwd_us = 0, tuned_adj_us = 0;  // autotune: chosen variants' step times
+  swd_contract* tc = nullptr;                  // split-BF16 forward contraction (radon_precision)
   std::map<long, cudaGraphExec_t> graphs;
   std::vector<double> h_gres, h_crp;
   // optional per-phase timing of the last call (events on the engine stream)
@@ -107,6 +110,7 @@ struct swd_engine {
   std::vector<cudaEvent_t> ev;  // 4 per batch: before forward, after forward, after spectra, after adjoint
   double phase_ms[3] = {0, 0, 0};
   ~swd_engine() {
+    if (tc) swd_contract_destroy(tc);
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     for (auto x : ev) cudaEventDestroy(x);
     if (st) cudaStreamDestroy(st);
@@ -341,15 +345,103 @@ static int adjoint_batch(swd_engine* e, int bi, int s0, int nb) {
   return SWD_OK;
 }
 
+// Autotuner: times the forward and adjoint step kernels of every built CTA shape, ring depth
+// and chunk height (the planner's, 2/3 and 3/2 of it) on this engine's own buffers, a batch of
+// B shots, and keeps the fastest forward + adjoint pair.  Runs once at create, before any
+// graph is captured; the buffers it touches are all overwritten by the first real call.
+static int autotune(swd_engine* e) {
+  static const int shapes[][2] = {{3, 1}, {2, 1}, {4, 1}, {1, 2}};
+  static const int rings[] = {4, 6};
+  const FdGeom base = e->g;
+  FdGeom h = base;
+  h.warps = 3; h.cells = 1; h.ring_fwd = h.ring_adj = 4;
+  plan_decomposition(h, e->B, 0);
+  const int rows = base.NZ - 2;
+  std::vector<int> chunks = {h.chunk, std::max(8, h.chunk * 2 / 3), std::min(rows, h.chunk * 3 / 2)};
+  std::sort(chunks.begin(), chunks.end());
+  chunks.erase(std::unique(chunks.begin(), chunks.end()), chunks.end());
+  const int span = (e->mode == 2 ? e->ckpt : base.nt) - 1;  // adjoint steps must index stored snapshots
+  const int n = std::max(1, std::min(16, span));
+  const int snap_nrec = e->mode == 2 ? e->gseg.nrec : base.nrec;
+  const size_t fieldB = (size_t)e->B * 5 * base.field;
+  float* S[2] = {e->fstate.as<float>(), e->fstate.as<float>() + fieldB};
+  cudaEvent_t t0, t1;
+  SWD_CUDA(cudaEventCreate(&t0));
+  SWD_CUDA(cudaEventCreate(&t1));
+  auto time_steps = [&](const FdGeom& gc, bool fwd, float* ms) -> int {
+    FwdArgs<float> f = fwd_args(e, gc, 0, e->B);
+    f.seis_w = e->seis.as<float>();
+    AdjArgs<float> a = adj_args(e, gc, e->B);
+    a.snap = e->snap.as<float>();
+    for (int i = -2; i < n; ++i) {  // two untimed warm-up launches
+      if (i == 0) SWD_CUDA(cudaEventRecord(t0, e->st));
+      const int it = std::max(i, 0);
+      if (fwd) { f.in = S[i & 1]; f.out = S[(i + 1) & 1]; SWD_TRY(launch_fwd_step<float, 3>(f, it, e->st)); }
+      else { a.in = S[i & 1]; a.out = S[(i + 1) & 1]; SWD_TRY(launch_adj_step<float, 3>(a, it, e->st)); }
+    }
+    SWD_CUDA(cudaEventRecord(t1, e->st));
+    SWD_CUDA(cudaEventSynchronize(t1));
+    SWD_CUDA(cudaEventElapsedTime(ms, t0, t1));
+    return SWD_OK;
+  };
+  double best = 1e30;
+  FdGeom pick = base;
+  int rc = SWD_OK;
+  for (const auto& sh : shapes) {
+    for (int ch : chunks) {
+      double bf = 1e30, ba = 1e30;
+      int rf = 4, ra = 4;
+      for (int d : rings) {
+        if (!fd_variant_built(sh[0], sh[1], d)) continue;
+        FdGeom gc = base;
+        gc.nrec = snap_nrec;  // records per shot in the snapshot buffer (one segment in checkpoint mode)
+        gc.warps = sh[0]; gc.cells = sh[1]; gc.ring_fwd = gc.ring_adj = d;
+        plan_decomposition(gc, e->B, ch);
+        float mf = 0, ma = 0;
+        if ((rc = time_steps(gc, true, &mf)) != SWD_OK) break;
+        if ((rc = time_steps(gc, false, &ma)) != SWD_OK) break;
+        if (mf < bf) { bf = mf; rf = d; }
+        if (ma < ba) { ba = ma; ra = d; }
+      }
+      if (rc != SWD_OK) break;
+      if (bf + ba < best) {
+        best = bf + ba;
+        pick = base;
+        pick.warps = sh[0]; pick.cells = sh[1]; pick.ring_fwd = rf; pick.ring_adj = ra;
+        plan_decomposition(pick, e->B, ch);
+        e->tuned_fwd_us = bf * 1e3 / n;
+        e->tuned_adj_us = ba * 1e3 / n;
+      }
+    }
+    if (rc != SWD_OK) break;
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (rc != SWD_OK) return rc;
+  e->g = pick;
+  const int nrec = e->gseg.nrec;
+  e->gseg = pick;
+  e->gseg.nrec = nrec;
+  return SWD_OK;
+}
+
 // Spectra, picks, misfits (+ adjoint sources when `grad`) for the gathers of one batch.
 static int spectrum_batch(swd_engine* e, int bi, int s0, int nb, bool grad) {
   const RadonGeom& rg = e->rg;
   const int G = 2 * e->B;
   const Gather* gs = e->gath.as<Gather>() + (size_t)bi * G;
   const size_t sstride = (size_t)e->g.nt * e->g.ng;
+  if (e->tc) {  // offsets beyond a gather's window must be zero for the padded tensor-core tiles
+    SWD_CUDA(cudaMemsetAsync(e->D.p, 0, (size_t)G * rg.npair * rg.offset * sizeof(double2), e->st));
+  }
   SWD_TRY(radon_dft<float>(rg, gs, G, e->seis.as<float>(), sstride, e->W.as<double2>(), e->D.as<double2>(), e->st));
-  SWD_TRY(radon_contract(rg, gs, G, e->K.as<double2>(), e->D.as<double2>(), e->MM.as<double2>(),
-                         e->mlraw.as<double>(), e->ml.as<double>(), e->st));
+  if (e->tc) {
+    SWD_TRY(swd_contract_run(e->tc, e->D.as<double>(), e->MM.as<double>(), e->st));
+    SWD_TRY(radon_amplitudes(rg, gs, G, e->MM.as<double2>(), e->mlraw.as<double>(), e->ml.as<double>(), e->st));
+  } else {
+    SWD_TRY(radon_contract(rg, gs, G, e->K.as<double2>(), e->D.as<double2>(), e->MM.as<double2>(),
+                           e->mlraw.as<double>(), e->ml.as<double>(), e->st));
+  }
   const size_t go = (size_t)2 * s0;
   SWD_TRY(pick_batch(rg.np, rg.npair, G, e->sv.ini, e->sv.pick_method, e->sv.vmin, gs, e->ml.as<double>(),
                      e->cr0.as<double>() + go * rg.npair, e->crp.as<double>() + go * rg.npair,
@@ -570,6 +662,19 @@ static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engi
     }
   SWD_CUDA(cudaMemcpyAsync(e->gath.p, hg.data(), hg.size() * sizeof(Gather), cudaMemcpyHostToDevice, e->st));
   SWD_TRY(radon_tables(e->rg, e->W.as<double2>(), e->K.as<double2>(), e->st));
+  if (e->opt.autotune) SWD_TRY(autotune(e));
+  if (e->opt.radon_precision == SWD_PREC_BF16X2 || e->opt.radon_precision == SWD_PREC_BF16X3) {
+    // the engine's axes: kept bins lf..nf, velocities vmin + dv*p, offsets (m + x)*ds (RTrAD.m:11,18-21)
+    const RadonGeom& rg = e->rg;
+    std::vector<double> fr(rg.npair), vel(rg.np), off(rg.offset);
+    for (int f = 0; f < rg.npair; ++f) fr[f] = rg.df * (rg.lf - 1 + f);
+    for (int p = 0; p < rg.np; ++p) vel[p] = rg.vmin + rg.dv * p;
+    for (int x = 0; x < rg.offset; ++x) off[x] = (rg.m + x) * rg.ds;
+    SWD_TRY(swd_contract_create(rg.npair, fr.data(), rg.np, vel.data(), rg.offset, off.data(), 2 * e->B,
+                                e->opt.radon_precision, e->device, &e->tc));
+  } else {
+    SWD_CHECK(e->opt.radon_precision == SWD_PREC_FP64, "radon_precision must be SWD_PREC_FP64, _BF16X2 or _BF16X3");
+  }
   // default observed curves: ones (SWD.m:153-154)
   std::vector<double> ones((size_t)e->nbatch * 2 * e->B * e->rg.npair, 1.0);
   SWD_CUDA(cudaMemcpyAsync(e->cr0.p, ones.data(), ones.size() * sizeof(double), cudaMemcpyHostToDevice, e->st));
@@ -607,6 +712,8 @@ static void fill_info(const swd_engine* e, swd_engine_info_t* info) {
   info->cells = e->g.cells;
   info->ring_fwd = e->g.ring_fwd;
   info->ring_adj = e->g.ring_adj;
+  info->tuned_fwd_us = e->tuned_fwd_us;
+  info->tuned_adj_us = e->tuned_adj_us;
 }
 
 int swd_engine_info(const swd_engine* e, swd_engine_info_t* info) {

@@ -102,7 +102,7 @@ template int pack_materials<double>(const double*, const double*, const double*,
   X(1, 2, 4) X(1, 2, 6) X(1, 2, 8) X(1, 3, 4) X(1, 3, 6) X(2, 1, 4) X(2, 1, 6) X(2, 1, 8) X(3, 1, 4) X(3, 1, 6) \
   X(3, 1, 8) X(4, 1, 4) X(4, 1, 6) X(4, 1, 8)
 
-static bool variant_built(int w, int c, int d) {
+bool fd_variant_built(int w, int c, int d) {
 #define X(W, C, D) if (w == W && c == C && d == D) return true;
   SWD_SHAPES(X)
 #undef X
@@ -111,9 +111,9 @@ static bool variant_built(int w, int c, int d) {
 
 void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
   const int rows = g.NZ - 2;
-  if (!variant_built(g.warps, g.cells, 4)) { g.warps = 3; g.cells = 1; }
-  if (!variant_built(g.warps, g.cells, g.ring_fwd)) g.ring_fwd = 4;
-  if (!variant_built(g.warps, g.cells, g.ring_adj)) g.ring_adj = 4;
+  if (!fd_variant_built(g.warps, g.cells, 4)) { g.warps = 3; g.cells = 1; }
+  if (!fd_variant_built(g.warps, g.cells, g.ring_fwd)) g.ring_fwd = 4;
+  if (!fd_variant_built(g.warps, g.cells, g.ring_adj)) g.ring_adj = 4;
   const int cols = 32 * g.warps * g.cells;
   g.n_strips = (g.NX - 2 + cols - 1) / cols;
   if (chunk_rows <= 0) {

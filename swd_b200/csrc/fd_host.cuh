@@ -22,6 +22,8 @@ int pack_materials(const T* temp, const T* b, const T* b1, const T* ca, const T*
 
 // Choose strips/chunks for a launch over n_shots shots (chunk_rows <= 0: heuristic).
 void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows);
+// true when the engine-path FD kernels are built for (warps, cells, ring depth)
+bool fd_variant_built(int w, int c, int d);
 
 template <typename T, int NF>
 int launch_fwd_step(const FwdArgs<T>& a, int it, cudaStream_t st);

@@ -231,6 +231,33 @@ __global__ void __launch_bounds__(256) contract_kernel(RadonGeom g, const Gather
   for (int p = threadIdx.x; p < g.np; p += blockDim.x) ml[col * g.np + p] = mlraw[col * g.np + p] / mx;
 }
 
+// mlraw = |MM| and ml = mlraw / max_p mlraw per (gather, bin), for an MM computed elsewhere
+// (the tensor-core contraction); the same amplitude and normalisation as contract_kernel.
+__global__ void __launch_bounds__(256) amplitude_kernel(RadonGeom g, const Gather* gs, const double2* __restrict__ MM,
+                                                        double* mlraw, double* ml) {
+  __shared__ double red[33];
+  const int f = blockIdx.x, gi = blockIdx.y;
+  if (gs[gi].valid <= 0) return;
+  const size_t col = ((size_t)gi * g.npair + f) * g.np;
+  double mx = -1.0 / 0.0;
+  for (int p = threadIdx.x; p < g.np; p += blockDim.x) {
+    const double2 v = MM[col + p];
+    const double a = hypot(v.x, v.y);
+    mlraw[col + p] = a;
+    mx = fmax(mx, a);
+  }
+  mx = block_max(mx, red);
+  for (int p = threadIdx.x; p < g.np; p += blockDim.x) ml[col + p] = mlraw[col + p] / mx;
+}
+
+int radon_amplitudes(const RadonGeom& g, const Gather* d_gath, int G, const double2* MM, double* mlraw, double* ml,
+                     cudaStream_t st) {
+  amplitude_kernel<<<dim3(g.npair, G), 256, 0, st>>>(g, d_gath, MM, mlraw, ml);
+  count_launch(1);
+  SWD_CUDA(cudaGetLastError());
+  return SWD_OK;
+}
+
 int radon_contract(const RadonGeom& g, const Gather* d_gath, int G, const double2* K, const double2* D, double2* MM,
                    double* mlraw, double* ml, cudaStream_t st) {
   dim3 grid(g.npair, G);

@@ -41,6 +41,9 @@ int radon_dft(const RadonGeom& g, const Gather* d_gath, int G, const S* seis, si
 // MM[g][f][p] = sum_x K[f][x][p] D[g][f][x]; mlraw = |MM|; ml = mlraw / max_p mlraw
 int radon_contract(const RadonGeom& g, const Gather* d_gath, int G, const double2* K, const double2* D, double2* MM,
                    double* mlraw, double* ml, cudaStream_t st);
+// mlraw = |MM|, ml = mlraw / max_p mlraw for an MM computed elsewhere (valid gathers only)
+int radon_amplitudes(const RadonGeom& g, const Gather* d_gath, int G, const double2* MM, double* mlraw, double* ml,
+                     cudaStream_t st);
 // pickFDC1 + LHDispPick per gather: cr_pre = picks + vmin, res = mean((cr_pre-cr0)^2), dc = cr_pre - cr0.
 // Gathers with valid <= 0 are skipped (res = NaN); d_gath may be null (all gathers picked).
 int pick_batch(int np, int npair, int G, int ini, int method, double vmin, const Gather* d_gath, const double* ml,

@@ -122,3 +122,35 @@ def test_sharded_engines_sum_to_the_full_survey(tiny_case):
     for k, key in enumerate(("g_cl", "g_cm", "g_illum")):
         np.testing.assert_allclose(t[k], full[key], rtol=1e-12, atol=1e-300 + 1e-14 * np.abs(full[key]).max())
     assert rsum / rcnt == pytest.approx(full["residual"], rel=1e-12)
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_autotuned_engine_is_bit_identical(tiny_case, mode):
+    """The autotuner only picks among variants that give the same bits; it reports what it timed."""
+    s, cr0_r, cr0_l, _ = tiny_case
+    outs = []
+    for tune in (False, True):
+        with GradientEngine(s, snapshot_mode=mode, ckpt_interval=35, autotune=tune) as e:
+            e.set_observed(cr0_r, cr0_l)
+            outs.append(e.gradient(s.vp, s.vs))
+            if tune:
+                assert e.info["tuned_fwd_us"] > 0 and e.info["tuned_adj_us"] > 0
+                assert (e.info["warps"], e.info["cells"]) in [(3, 1), (2, 1), (4, 1), (1, 2)]
+    for k in ("g_cl", "g_cm", "g_illum", "dk_vs", "cr_pre_r", "cr_pre_l"):
+        assert np.array_equal(outs[0][k], outs[1][k]), k
+
+
+def test_split_bf16_radon_in_the_engine(tiny_case):
+    """radon_precision='bf16x2': the forward contraction on the tensor cores.  Spectra move by
+    ~1e-5 relative, so picks may change only at near-ties; the gradient stays close."""
+    s, cr0_r, cr0_l, _ = tiny_case
+    outs = []
+    for prec in ("fp64", "bf16x2"):
+        with GradientEngine(s, radon_precision=prec) as e:
+            e.set_observed(cr0_r, cr0_l)
+            outs.append(e.gradient(s.vp, s.vs))
+    a, b = outs
+    same = np.mean(np.concatenate([(a["cr_pre_r"] == b["cr_pre_r"]).ravel(), (a["cr_pre_l"] == b["cr_pre_l"]).ravel()]))
+    err = _rel(b["dk_vs"], a["dk_vs"])
+    print("identical picks", same, "dk rel L2", err)
+    assert same >= 0.95 and err < 1e-2
