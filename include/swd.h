@@ -200,11 +200,13 @@ typedef struct {
                          (1,2), (1,3), (2,1), (3,1), (4,1); others: (3,1) */
   int ring_fwd, ring_adj; /* rows in the forward / adjoint shared-memory ring: 4, 6 or 8 (6 at most
                              for (1,3)); anything else: 4 */
-  int autotune;       /* 1: at create, time the FD step kernels of each CTA shape, ring depth and
-                         chunk height on this survey's buffers and keep the fastest (overrides
-                         warps, cells, ring_*, chunk_rows) */
+  int autotune;       /* 1: at create, time the FD step kernels of each schedule, CTA shape, ring
+                         depth and chunk height on this survey's buffers and keep the fastest
+                         (overrides warps, cells, ring_*, chunk_rows, fd_schedule) */
   int radon_precision; /* forward Radon contraction: SWD_PREC_FP64 (0, default, as the reference)
                           or SWD_PREC_BF16X2 / _BF16X3 (tcgen05 split-BF16, see swd_contract_*) */
+  int fd_schedule;    /* FD kernels: 0 two CTA barriers per row, 1 one barrier with the velocities
+                         a row ahead (shapes (2,1), (3,1), (4,1) ring 4, (3,1) ring 6); same bits */
 } swd_engine_opts;
 
 typedef struct {
@@ -212,6 +214,7 @@ typedef struct {
   size_t bytes;
   int npair, np, ccn, nzbc, nxbc, chunk_rows, warps, cells, ring_fwd, ring_adj;
   double tuned_fwd_us, tuned_adj_us; /* autotune: the chosen variants' step times (0 if not tuned) */
+  int fd_schedule;
 } swd_engine_info_t;
 
 /* Gradient outputs (host pointers, nz x nx column-major; NULL entries skipped). */

@@ -352,6 +352,7 @@ static int adjoint_batch(swd_engine* e, int bi, int s0, int nb) {
 static int autotune(swd_engine* e) {
   static const int shapes[][2] = {{3, 1}, {2, 1}, {4, 1}, {1, 2}};
   static const int rings[] = {4, 6};
+  static const int scheds[] = {0, 1};
   const FdGeom base = e->g;
   FdGeom h = base;
   h.warps = 3; h.cells = 1; h.ring_fwd = h.ring_adj = 4;
@@ -387,15 +388,17 @@ static int autotune(swd_engine* e) {
   double best = 1e30;
   FdGeom pick = base;
   int rc = SWD_OK;
+  for (int sc : scheds)
+  if (rc == SWD_OK)
   for (const auto& sh : shapes) {
     for (int ch : chunks) {
       double bf = 1e30, ba = 1e30;
       int rf = 4, ra = 4;
       for (int d : rings) {
-        if (!fd_variant_built(sh[0], sh[1], d)) continue;
+        if (!fd_variant_built(sh[0], sh[1], d) || (sc == 1 && !fd_lead_built(sh[0], sh[1], d))) continue;
         FdGeom gc = base;
         gc.nrec = snap_nrec;  // records per shot in the snapshot buffer (one segment in checkpoint mode)
-        gc.warps = sh[0]; gc.cells = sh[1]; gc.ring_fwd = gc.ring_adj = d;
+        gc.warps = sh[0]; gc.cells = sh[1]; gc.ring_fwd = gc.ring_adj = d; gc.sched = sc;
         plan_decomposition(gc, e->B, ch);
         float mf = 0, ma = 0;
         if ((rc = time_steps(gc, true, &mf)) != SWD_OK) break;
@@ -407,7 +410,7 @@ static int autotune(swd_engine* e) {
       if (bf + ba < best) {
         best = bf + ba;
         pick = base;
-        pick.warps = sh[0]; pick.cells = sh[1]; pick.ring_fwd = rf; pick.ring_adj = ra;
+        pick.warps = sh[0]; pick.cells = sh[1]; pick.ring_fwd = rf; pick.ring_adj = ra; pick.sched = sc;
         plan_decomposition(pick, e->B, ch);
         e->tuned_fwd_us = bf * 1e3 / n;
         e->tuned_adj_us = ba * 1e3 / n;
@@ -615,6 +618,7 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   g.cells = e->opt.cells;
   g.ring_fwd = e->opt.ring_fwd;
   g.ring_adj = e->opt.ring_adj;
+  g.sched = e->opt.fd_schedule == 1 ? 1 : 0;
   plan_decomposition(g, std::max(1, std::min(e->opt.max_batch > 0 ? e->opt.max_batch : e->ns, e->ns)),
                      e->opt.chunk_rows);
   // Radon geometry
@@ -714,6 +718,7 @@ static void fill_info(const swd_engine* e, swd_engine_info_t* info) {
   info->ring_adj = e->g.ring_adj;
   info->tuned_fwd_us = e->tuned_fwd_us;
   info->tuned_adj_us = e->tuned_adj_us;
+  info->fd_schedule = e->g.sched;
 }
 
 int swd_engine_info(const swd_engine* e, swd_engine_info_t* info) {

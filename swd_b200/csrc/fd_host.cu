@@ -8,7 +8,7 @@
 
 #include "fd_host.cuh"
 #include "fd_kernels.cuh"
-#include "fd_smem.cuh"
+#include "fd_lead.cuh"
 
 namespace swd {
 
@@ -102,9 +102,19 @@ template int pack_materials<double>(const double*, const double*, const double*,
   X(1, 2, 4) X(1, 2, 6) X(1, 2, 8) X(1, 3, 4) X(1, 3, 6) X(2, 1, 4) X(2, 1, 6) X(2, 1, 8) X(3, 1, 4) X(3, 1, 6) \
   X(3, 1, 8) X(4, 1, 4) X(4, 1, 6) X(4, 1, 8)
 
+// Variants of the one-barrier-per-row schedule (fd_lead.cuh).
+#define SWD_LEAD_SHAPES(X) X(2, 1, 4) X(3, 1, 4) X(3, 1, 6) X(4, 1, 4)
+
 bool fd_variant_built(int w, int c, int d) {
 #define X(W, C, D) if (w == W && c == C && d == D) return true;
   SWD_SHAPES(X)
+#undef X
+  return false;
+}
+
+bool fd_lead_built(int w, int c, int d) {
+#define X(W, C, D) if (w == W && c == C && d == D) return true;
+  SWD_LEAD_SHAPES(X)
 #undef X
   return false;
 }
@@ -114,6 +124,8 @@ void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
   if (!fd_variant_built(g.warps, g.cells, 4)) { g.warps = 3; g.cells = 1; }
   if (!fd_variant_built(g.warps, g.cells, g.ring_fwd)) g.ring_fwd = 4;
   if (!fd_variant_built(g.warps, g.cells, g.ring_adj)) g.ring_adj = 4;
+  if (g.sched == 1 && !(fd_lead_built(g.warps, g.cells, g.ring_fwd) && fd_lead_built(g.warps, g.cells, g.ring_adj)))
+    g.sched = 0;
   const int cols = 32 * g.warps * g.cells;
   g.n_strips = (g.NX - 2 + cols - 1) / cols;
   if (chunk_rows <= 0) {
@@ -152,6 +164,32 @@ static int fwd_impl(const FwdArgs<T>& a, int it, cudaStream_t st) {
   return fwd_launch<T, NF, W, C, D, GB, false>(a, it, st);
 }
 
+template <typename T, int NF, int W, int C, int D, bool GB, bool SNAP>
+static int fwd_lead_launch(const FwdArgs<T>& a, int it, cudaStream_t st) {
+  constexpr size_t smem = lead_smem_bytes<T, W, C, D, GB>();
+  static int ready = set_smem(fd_fwd_lead<T, NF, W, C, D, GB, SNAP>, smem);
+  if (ready != SWD_OK) return ready;
+  const long blocks = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
+  fd_fwd_lead<T, NF, W, C, D, GB, SNAP><<<(unsigned)blocks, 32 * W, smem, st>>>(a, it);
+  count_launch(1);
+  return SWD_OK;
+}
+template <typename T, int NF, int W, int C, int D, bool GB>
+static int fwd_lead_impl(const FwdArgs<T>& a, int it, cudaStream_t st) {
+  if (a.snap && it % a.g.nt_wf == 0) return fwd_lead_launch<T, NF, W, C, D, GB, true>(a, it, st);
+  return fwd_lead_launch<T, NF, W, C, D, GB, false>(a, it, st);
+}
+template <typename T, int NF, int W, int C, int D, bool GB, bool IMG>
+static int adj_lead_impl(const AdjArgs<T>& a, int it, cudaStream_t st) {
+  constexpr size_t smem = lead_smem_bytes<T, W, C, D, GB>();
+  static int ready = set_smem(fd_adj_lead<T, NF, W, C, D, GB, IMG>, smem);
+  if (ready != SWD_OK) return ready;
+  const long blocks = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
+  fd_adj_lead<T, NF, W, C, D, GB, IMG><<<(unsigned)blocks, 32 * W, smem, st>>>(a, it);
+  count_launch(1);
+  return SWD_OK;
+}
+
 template <typename T, int NF, int W, int C, int D, bool GB, bool IMG>
 static int adj_impl(const AdjArgs<T>& a, int it, cudaStream_t st) {
   constexpr size_t smem = smem_bytes<T, W, C, D, GB>();
@@ -170,6 +208,16 @@ int launch_fwd_step(const FwdArgs<T>& a, int it, cudaStream_t st) {
   if (a.mb) return fwd_impl<T, NF, 4, 1, 4, true>(a, it, st);
   if constexpr (NF == 3 && sizeof(T) == 4) {
     const int key = a.g.warps * 100 + a.g.cells * 10 + a.g.ring_fwd;
+    if (a.g.sched == 1) {
+      switch (key) {
+#define X(w, c, d) case w * 100 + c * 10 + d: return fwd_lead_impl<T, NF, w, c, d, false>(a, it, st);
+        SWD_LEAD_SHAPES(X)
+#undef X
+        default: break;
+      }
+      set_error("internal: unsupported FD kernel variant");
+      return SWD_ERR_INVALID;
+    }
     switch (key) {
 #define X(w, c, d) case w * 100 + c * 10 + d: return fwd_impl<T, NF, w, c, d, false>(a, it, st);
       SWD_SHAPES(X)
@@ -186,6 +234,16 @@ static int adj_dispatch(const AdjArgs<T>& a, int it, cudaStream_t st) {
   if (a.mb) return adj_impl<T, NF, 4, 1, 4, true, IMG>(a, it, st);
   if constexpr (NF == 3 && sizeof(T) == 4) {
     const int key = a.g.warps * 100 + a.g.cells * 10 + a.g.ring_adj;
+    if (a.g.sched == 1) {
+      switch (key) {
+#define X(w, c, d) case w * 100 + c * 10 + d: return adj_lead_impl<T, NF, w, c, d, false, IMG>(a, it, st);
+        SWD_LEAD_SHAPES(X)
+#undef X
+        default: break;
+      }
+      set_error("internal: unsupported FD kernel variant");
+      return SWD_ERR_INVALID;
+    }
     switch (key) {
 #define X(w, c, d) case w * 100 + c * 10 + d: return adj_impl<T, NF, w, c, d, false, IMG>(a, it, st);
       SWD_SHAPES(X)

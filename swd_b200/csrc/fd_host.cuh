@@ -24,6 +24,8 @@ int pack_materials(const T* temp, const T* b, const T* b1, const T* ca, const T*
 void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows);
 // true when the engine-path FD kernels are built for (warps, cells, ring depth)
 bool fd_variant_built(int w, int c, int d);
+// true when the one-barrier-per-row (lead) schedule is built for (warps, cells, ring depth)
+bool fd_lead_built(int w, int c, int d);
 
 template <typename T, int NF>
 int launch_fwd_step(const FwdArgs<T>& a, int it, cudaStream_t st);

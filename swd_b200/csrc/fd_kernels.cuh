@@ -33,6 +33,7 @@ struct FdGeom {
   int warps;                 // warps per CTA
   int cells;                 // output columns per thread; a CTA owns 32*warps*cells columns
   int ring_fwd, ring_adj;    // rows in the shared-memory ring of the forward / adjoint kernels (4, 6, 8)
+  int sched;                 // 0: two barriers per row (fd_smem.cuh); 1: one, velocities a row ahead (fd_lead.cuh)
   size_t field;              // NZ * pitch
 };
 

@@ -56,13 +56,34 @@ def test_modes_are_bit_identical(tiny_case):
     s, cr0_r, cr0_l, _ = tiny_case
     outs = []
     for kw in ({"snapshot_mode": 1}, {"snapshot_mode": 2, "ckpt_interval": 20}, {"snapshot_mode": 1, "max_batch": 1},
-               {"snapshot_mode": 1, "use_graphs": False, "chunk_rows": 3}):
+               {"snapshot_mode": 1, "use_graphs": False, "chunk_rows": 3},
+               # one barrier per row (velocities a row ahead): same bits in every mode and chunking
+               {"snapshot_mode": 1, "fd_schedule": 1}, {"snapshot_mode": 2, "ckpt_interval": 20, "fd_schedule": 1},
+               {"snapshot_mode": 1, "fd_schedule": 1, "chunk_rows": 3},
+               {"snapshot_mode": 1, "fd_schedule": 1, "chunk_rows": 5, "ring_fwd": 6, "ring_adj": 6},
+               {"snapshot_mode": 1, "fd_schedule": 1, "warps": 2, "cells": 1, "chunk_rows": 1},
+               {"snapshot_mode": 1, "fd_schedule": 1, "warps": 4, "cells": 1, "chunk_rows": 2}):
         with GradientEngine(s, **kw) as e:
             e.set_observed(cr0_r, cr0_l)
             outs.append(e.gradient(s.vp, s.vs))
     for o in outs[1:]:
         for k in ("g_cl", "g_cm", "g_illum", "dk_vs", "cr_pre_r"):
             assert np.array_equal(o[k], outs[0][k]), k
+
+
+def test_lead_schedule_on_the_plain_survey_matches_the_oracle(O):
+    """The one-barrier schedule against the oracle on the 30 x 120 survey (source near the
+    top, receivers on the free-surface row, several chunks)."""
+    s = configs.plain_c1(ns=3, nt=1000)
+    cr0_r, cr0_l = O.observed_curves(s, s.vs_true)
+    ref = O.gradient(s, s.vs, cr0_r, cr0_l)
+    with GradientEngine(s, fd_schedule=1, chunk_rows=7) as e:
+        assert e.info["fd_schedule"] == 1
+        e.set_observed(cr0_r, cr0_l)
+        out = e.gradient(s.vp, s.vs)
+    assert np.array_equal(out["cr_pre_r"], ref["cr_pre_r"])
+    for k in ("g_cl", "g_cm", "g_illum", "dk_vs"):
+        assert _rel(out[k], ref[k]) < TOL, k
 
 
 def test_misfit_pass_matches_gradient_picks(tiny_case):
