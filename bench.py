@@ -67,6 +67,8 @@ def parse():
                    help="Radon contraction precision study (200 f x 400 v x 600 offsets x 96 shots)")
     p.add_argument("--precision", action="store_true",
                    help="FP32 engine vs the full-FP64 per-shot path: seismograms, spectra, picks, gradient, misfit")
+    p.add_argument("--invert", type=int, default=0,
+                   help="SWD inversion iterations (gradient + line search) on the batched 100x600 survey")
     p.add_argument("--plain-sample", type=int, default=8,
                    help="served stream: requests re-run serially on the plain path for the comparison")
     return p.parse_args()
@@ -404,8 +406,43 @@ def run_precision(args):
     return 0
 
 
+def run_invert(args):
+    """SWD.m's inversion loop on the engine: iterations/hour, misfit per iteration and the
+    forward/gradient passes each iteration took (the starting model is linear in depth
+    between the true model's extremes, SWD.m:27-30)."""
+    import torch
+
+    from swd_b200 import configs
+    from swd_b200.invert import Inversion
+    if int(os.environ.get("RANK", "0")) != 0:
+        return 0
+    s = survey(args)
+    vs0 = np.repeat(np.linspace(np.min(s.vs_true), np.max(s.vs_true), s.nz)[:, None], s.nx, 1)
+    inv = Inversion(s, vs0, s.vs_true, autotune=True)
+    inv.run(1)  # warm-up: engine, graphs, observed curves
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    hist = inv.run(args.invert)
+    dt = time.perf_counter() - t0
+    err0 = float(np.sqrt(np.mean((vs0 - s.vs_true) ** 2)))
+    err1 = float(np.sqrt(np.mean((inv.vs - s.vs_true) ** 2)))
+    inv.close()
+    line = {"metric": "SWD iterations/hour", "value": len(hist[1:]) / dt * 3600 if len(hist) > 1 else None,
+            "unit": "iterations/hour", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic (seeded layered model + Gaussian anomaly)",
+            "config": workload_config(s, {"iterations_timed": len(hist) - 1}),
+            "seconds_per_iteration": dt / max(1, len(hist) - 1),
+            "residual": [h.residual for h in hist], "accepted_misfit": [h.res0 for h in hist],
+            "misfit_passes": [h.misfit_passes for h in hist], "offset": [h.offset for h in hist],
+            "vs_rms_error_m_s": {"start": err0, "end": err1}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.invert:
+        return run_invert(args)
     if args.precision:
         return run_precision(args)
     if args.impl == "reference":

@@ -637,9 +637,10 @@ def assemble(vs, g_cl, g_cm, g_illum, smoothZ=1, smoothX=2):
 # Whole shot loops of SWD.m / SWD_single.m
 # --------------------------------------------------------------------------------------
 
-def _survey_fd(s, is_, vs, single=True, adjoint=False):
+def _survey_fd(s, is_, vs, single=True, adjoint=False, vp=None):
+    vp = s.vp_ratio * vs if vp is None else vp
     return fd_inputs(s.nbc, s.nt, s.dtx, s.dx, s.dt, int(s.sx[is_ - 1]), 1, s.gx, np.ones(s.ng),
-                     s.vp_ratio * vs, vs, s.isfs, s.fd_order, s.source_type, s.nt_wf, single, adjoint)
+                     vp, vs, s.isfs, s.fd_order, s.source_type, s.nt_wf, single, adjoint)
 
 
 def _sides(s, is_):
@@ -656,13 +657,13 @@ def _spectra(s, seis, is_):
     return out
 
 
-def observed_curves(s, vs, single=True):
+def observed_curves(s, vs, single=True, vp=None):
     """SWD.m:150-162 (SWD_single.m in single precision): picks of the data of model vs."""
     npair = s.npair
     cr = np.ones((npair, s.ns))
     cl = np.ones((npair, s.ns))
     for is_ in range(1, s.ns + 1):
-        _, sw, _ = mex_staggerfd(_survey_fd(s, is_, vs, single), s.source(), want_wf=False)
+        _, sw, _ = mex_staggerfd(_survey_fd(s, is_, vs, single, vp=vp), s.source(), want_wf=False)
         sp = _spectra(s, sw.astype(np.float64), is_)
         if "r" in sp:
             cr[:, is_ - 1] = LHDispPick(sp["r"][0], s.vmin, cr[:, is_ - 1], 1, s.ini)[1]
@@ -671,10 +672,10 @@ def observed_curves(s, vs, single=True):
     return cr, cl
 
 
-def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True, single=True):
+def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True, single=True, vp=None):
     """SWD_single.m:172-193 for one shot: forward (FP32), spectra, picks, ADWDgrad_1, adjoint.
     single=False: SWD.m's double path (FP64 FD, adjoint source kept in double)."""
-    inp = _survey_fd(s, is_, vs, single)
+    inp = _survey_fd(s, is_, vs, single, vp=vp)
     _, sw, wf = mex_staggerfd(inp, s.source())
     sp = _spectra(s, sw.astype(np.float64), is_)
     npair = s.npair
@@ -688,20 +689,20 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True, single=True):
     a = ADWDgrad_1(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl,
                    sp.get("r", (0, 0, None))[2], sp.get("l", (0, 0, None))[2])
     out["adj_src"] = a.astype(np.float32) if single else a
-    ainp = _survey_fd(s, is_, vs, single, adjoint=True)
+    ainp = _survey_fd(s, is_, vs, single, adjoint=True, vp=vp)
     out["cl"], out["cm"], out["il"] = mex_e2drtm(ainp, out["adj_src"], wf, accum_fp64)
     return out
 
 
-def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=True, single=True):
+def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=True, single=True, vp=None):
     """SWD_single.m:171-201 (SWD.m with single=False) with the shot sum in FP64 in shot order."""
     from concurrent.futures import ThreadPoolExecutor
     shots = list(range(1, s.ns + 1))
     if threads > 1:
         with ThreadPoolExecutor(threads) as ex:
-            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single), shots))
+            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp), shots))
     else:
-        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single) for i in shots]
+        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp) for i in shots]
     g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
     for p in per:
         for k in g:
@@ -721,3 +722,17 @@ def contract(freq, vel, off, spec):
     freq, vel, off = (np.asarray(a, np.float64) for a in (freq, vel, off))
     th = 2 * np.pi * freq[:, None, None] * off[None, None, :] / vel[None, :, None]  # [f,p,x]
     return np.einsum("fpx,sfx->sfp", np.exp(1j * th), np.asarray(spec, np.complex128))
+
+
+def misfit(s, vs, cr0_r, cr0_l, single=True, vp=None):
+    """SWD.m:215-228: forward-only misfit of a trial model, the mean of res_r over the shots
+    that have a right side (res_r is only assigned for them, and they come first)."""
+    res = []
+    for is_ in range(1, s.ns + 1):
+        if not has_right(is_, s.ns, s.m, s.M, s.w):
+            continue
+        _, sw, _ = mex_staggerfd(_survey_fd(s, is_, vs, single, vp=vp), s.source(), want_wf=False)
+        ml = radon(sw.astype(np.float64), is_, s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.ng, s.ds, s.offset,
+                   s.m, s.M, "r", s.dv)[0]
+        res.append(LHDispPick(ml, s.vmin, cr0_r[:, is_ - 1], 1, s.ini)[0])
+    return float(np.mean(res))

@@ -64,3 +64,28 @@ def test_two_gloo_ranks_reduce_to_the_single_process_gradient(O, tmp_path):
     g = r["gsum"].reshape(3, s.nz, s.nx)
     dk = O.assemble(s.vs, g[0], g[1], g[2], s.smooth_z, s.smooth_x)
     np.testing.assert_allclose(dk, ref["dk_vs"], rtol=1e-10, atol=1e-300)
+
+
+@pytest.mark.gpu
+def test_two_ranks_of_sharded_engines_reduce_to_the_one_engine_gradient(tmp_path):
+    """The GPU path of the shard/reduce logic: two ranks with their own engines and shot shares
+    on one GPU, the shot sums all-reduced over gloo, against one engine over all shots."""
+    out = str(tmp_path / "g0.npz")
+    env = dict(os.environ, MASTER_ADDR="127.0.0.1", MASTER_PORT=str(_free_port()), WORLD_SIZE="2")
+    procs = [subprocess.Popen([sys.executable, os.path.join(HERE, "shots_worker_gpu.py"), out],
+                              env=dict(env, RANK=str(r), LOCAL_RANK=str(r)), stdout=subprocess.PIPE,
+                              stderr=subprocess.STDOUT) for r in range(2)]
+    try:
+        logs = [p.communicate(timeout=300)[0].decode() for p in procs]
+    finally:
+        for p in procs:
+            if p.poll() is None:
+                p.kill()
+    assert all(p.returncode == 0 for p in procs), logs
+    r = np.load(out)
+    assert r["shots"].tolist() == [1, 3, 5]
+    a, b = r["dk"], r["ref_dk"]
+    assert np.array_equal(np.isnan(a), np.isnan(b))
+    m = ~np.isnan(b)
+    assert np.linalg.norm(a[m] - b[m]) / np.linalg.norm(b[m]) < 1e-12
+    assert float(r["mis"]) == pytest.approx(float(r["ref_mis"]), rel=1e-12)
