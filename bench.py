@@ -47,13 +47,16 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    p.add_argument("--shots", type=int, default=96, help="shots in the survey (split over the GPUs)")
-    p.add_argument("--nt", type=int, default=8000)
+    p.add_argument("--workload", choices=["batched-100x600", "large-400x3000"], default="batched-100x600",
+                   help="batched-100x600 (96 shots, nt 8000) or large-400x3000 (240 shots, nt 20000)")
+    p.add_argument("--shots", type=int, default=0, help="shots in the survey (0: the workload's; split over GPUs)")
+    p.add_argument("--nt", type=int, default=0, help="time steps (0: the workload's)")
     p.add_argument("--plain-shots", type=int, default=8, help="shots timed on the one-shot-per-launch path")
     p.add_argument("--cpu-shots", type=int, default=0, help="CPU baseline sample size (0: one per host thread)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     p.add_argument("--snapshot-mode", type=int, default=0, help="0 auto, 1 store snapshots, 2 checkpoint")
-    p.add_argument("--ckpt", type=int, default=50, help="steps between checkpoints (snapshot mode 2)")
+    p.add_argument("--ckpt", type=int, default=0,
+                   help="steps between checkpoints (snapshot mode 2; 0: memory-optimal)")
     p.add_argument("--warps", type=int, default=0, help="FD kernel CTA shape (0: planner default)")
     p.add_argument("--cells", type=int, default=0)
     p.add_argument("--ring", type=int, default=0)
@@ -130,11 +133,13 @@ class ClockSampler:
 
 def survey(args):
     from swd_b200 import configs
+    if args.workload == "large-400x3000":
+        return configs.large_c5(ns=args.shots, nt=args.nt)
     return configs.batched_c2(ns=args.shots, nt=args.nt)
 
 
 def workload_config(s, extra=None):
-    c = {"workload": f"batched-{s.nz}x{s.nx}: nz={s.nz} nx={s.nx} dx={s.dx} nbc={s.nbc} nt={s.nt} dt={s.dt} "
+    c = {"workload": f"{s.name}: nz={s.nz} nx={s.nx} dx={s.dx} nbc={s.nbc} nt={s.nt} dt={s.dt} "
                      f"{s.ns} shots x {s.ng} receivers, Ricker f0={s.f0}, Radon {s.fmin:g}-{s.fmax:g} Hz "
                      f"df={s.df:g}, {s.vmin:g}-{s.vmax:g} m/s step {s.dv:g}, offset {s.offset}",
          "shots": s.ns, "grid_padded": [s.nzbc, s.nxbc], "nt": s.nt, "nt_wf": s.nt_wf,
@@ -441,6 +446,10 @@ def run_invert(args):
 
 def main():
     args = parse()
+    if not args.shots:
+        args.shots = 240 if args.workload == "large-400x3000" else 96
+    if not args.nt:
+        args.nt = 20000 if args.workload == "large-400x3000" else 8000
     if args.invert:
         return run_invert(args)
     if args.precision:
@@ -530,7 +539,8 @@ def main():
         sg.gradient_device(d_vp, d_vs, d_dk)
         dk_h.copy_(d_dk)
 
-    e2e_step()  # warm
+    if args.steps < 1:
+        e2e_step()  # warm (the timed steps already captured the engine's graphs otherwise)
     if world > 1:
         dist.barrier()
     t0 = time.perf_counter()

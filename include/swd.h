@@ -159,6 +159,27 @@ int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_a
                  const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
                  double* a_data_res);
 
+/* Replaces ADWDgrad_norm(...) (core/ADWDgrad_norm.m:1-102, same arguments as ADWDgrad_1):
+ * the SoftMax weights are replaced by normpdf(1:np, cr, 16) around the picks
+ * (core/paddingMl_norm.m:1-9).  cr_r / cr_l: npair, saveForBackward.cr_r / cr_l = cr_pre - vmin
+ * (SWD.m:178, 184). */
+int swd_adwdgrad_norm(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
+                      const double* grad_output_r, const double* grad_output_l, const double* space_m,
+                      const double* mm_r, const double* ml_raw_r, const double* cr_r, const double* mm_l,
+                      const double* ml_raw_l, const double* cr_l, double* a_data_res);
+
+/* Replaces weight_data_muti3(seismo_v_d,seismo_v,is,dt,df,offset,dg,F1,w,M,m,ns,refsx,win,
+ * fmin,fmax,cr_0,cr_0l,cr_pre_r,cr_pre_l,ind) (core/weight_data_muti3.m:1-122), the WD adjoint
+ * source of SWD.m:188.  seismo_v_d / seismo_v: nt x ng (F1 = 1 reads seismo_v_d, F1 = 0
+ * seismo_v; the other may be NULL); refsx: ns receiver indices floor(sx/dg)+1 (SWD.m:96);
+ * dg: receiver spacing in metres; cr_*: npair = floor((fmax-fmin)/df+1) picks (a side the
+ * reference skips may pass NULL).  Needs nt <= floor(1/dt/df), 2*win < floor(1/dt/df) and
+ * ind+npair-1 <= win (SWD.m:124-127 gives win = npair+2*ind).  seismo_v_d1: nt x ng (out). */
+int swd_wd_residual(int nt, int ng, const double* seismo_v_d, const double* seismo_v, int is, double dt, double df,
+                    int offset, double dg, int F1, int w, double M, int m, int ns, const double* refsx, int win,
+                    double fmin, double fmax, const double* cr_0, const double* cr_0l, const double* cr_pre_r,
+                    const double* cr_pre_l, int ind, double* seismo_v_d1);
+
 /* ------------------------------------------------------------------------
  * Batched gradient engine: the per-iteration shot loops of SWD.m run as one
  * batched GPU pipeline (replaces the parfor loops SWD.m:155-162 observed curves,
@@ -192,7 +213,8 @@ typedef struct {
   size_t hbm_budget;  /* bytes the engine may allocate (0: 92% of free memory) */
   int max_batch;      /* shots per batch (0: as many as fit) */
   int snapshot_mode;  /* 0 auto, 1 keep every strain snapshot, 2 checkpoint + recompute */
-  int ckpt_interval;  /* steps between forward checkpoints (mode 2; rounded to nt_wf) */
+  int ckpt_interval;  /* steps between forward checkpoints (mode 2; rounded to nt_wf; 0: the
+                         interval that minimises checkpoint + snapshot memory per shot) */
   int use_graphs;     /* capture the time loops in CUDA graphs */
   int chunk_rows;     /* rows per CTA in the FD kernels (0: heuristic) */
   int device;
@@ -207,6 +229,10 @@ typedef struct {
                           or SWD_PREC_BF16X2 / _BF16X3 (tcgen05 split-BF16, see swd_contract_*) */
   int fd_schedule;    /* FD kernels: 0 two CTA barriers per row, 1 one barrier with the velocities
                          a row ahead (shapes (2,1), (3,1), (4,1) ring 4, (3,1) ring 6); same bits */
+  int adjoint_weight; /* adjoint source: 0 ADWDgrad_1 (SoftMax weights, SWD.m:190), 1 ADWDgrad_norm
+                         (Gaussian weights around the picks, core/ADWDgrad_norm.m), 2 the WD residual
+                         weight_data_muti3 with F1 = 0 (SWD.m:188; ind = fmin/df+1, win = npair+2*ind,
+                         refsx = floor(sx/dgx)+1, dg = dgx*dx as SWD.m:96-97,124-127 set them) */
 } swd_engine_opts;
 
 typedef struct {

@@ -556,13 +556,21 @@ def softmax_cols(z):
     return e / e.sum(axis=0, keepdims=True)
 
 
-def adwd_side(nt, ng, npair, soft_arg_norm, grad_output, save, side, a_data_res):
-    """One side of core/ADWDgrad_1.m:15-44 (right) / :47-77 (left), written into a_data_res."""
+def normpdf_cols(npv, cr):
+    """core/paddingMl_norm.m:1-9: column i is normpdf(1:np, cr(i), 16)."""
+    x = np.arange(1, npv + 1, dtype=np.float64)[:, None]
+    z = (x - np.asarray(cr, np.float64)[None, :]) / 16.0
+    return np.exp(-0.5 * z * z) / (np.sqrt(2 * np.pi) * 16.0)
+
+
+def adwd_side(nt, ng, npair, soft_arg_norm, grad_output, save, side, a_data_res, cr=None):
+    """One side of core/ADWDgrad_1.m:15-44 (right) / :47-77 (left), written into a_data_res.
+    cr given: ADWDgrad_norm.m:22-23, the weights are normpdf around cr = cr_pre - vmin."""
     lf, nf, ccn = save["lf"], save["nf"], save["ccn"]
     pos = save["uxtpos"]
     noff = len(pos)
     mlr = save["ml_raw"] ** (1.0 / 40.0)
-    E = softmax_cols(mlr * soft_arg_norm)
+    E = softmax_cols(mlr * soft_arg_norm) if cr is None else normpdf_cols(mlr.shape[0], cr)
     npv = E.shape[0]
     space = np.arange(1, npv + 1, dtype=np.float64)[:, None]
     go = np.array(grad_output, np.float64).copy()
@@ -587,6 +595,94 @@ def adwd_side(nt, ng, npair, soft_arg_norm, grad_output, save, side, a_data_res)
         # uxtposl ascending; row 1 of g is the source trace (fliplr); ADWDgrad_1.m:76
         a_data_res[:, [p - 1 for p in pos[:-1]]] = g[:0:-1, :].T
     return a_data_res
+
+
+def ADWDgrad_norm(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, saver, savel, cr_r,
+                  cr_l):
+    """core/ADWDgrad_norm.m:1-102 (saveForBackward.cr_r / cr_l passed as cr_r / cr_l)."""
+    a = np.zeros((nt, ng))
+    if has_right(is_, ns, m, M, w):
+        adwd_side(nt, ng, npair, SoftArgNorm, grad_outputr, saver, "r", a, cr_r)
+    if has_left(is_, m, M, w):
+        adwd_side(nt, ng, npair, SoftArgNorm, grad_outputl, savel, "l", a, cr_l)
+    return a
+
+
+def mlinspace(d1, d2, n):
+    """MATLAB linspace(d1, d2, n): floor(n) points d1 + i*(d2-d1)/(n-1), the last one d2."""
+    n = int(math.floor(n))
+    if n < 1:
+        return np.zeros(0)
+    if n == 1:
+        return np.array([float(d2)])
+    y = d1 + np.arange(n, dtype=np.float64) * (d2 - d1) / (n - 1)
+    y[-1] = d2
+    return y
+
+
+def weight_data_muti3(seismo_v_d, seismo_v, is_, dt, df, offset, dg, F1, w, M, m, ns, refsx, win, fmin, fmax,
+                      cr_0, cr_0l, cr_pre_r, cr_pre_l, ind):
+    """core/weight_data_muti3.m:1-122, the WD adjoint source (SWD.m:188, commented out there).
+
+    Each side's traces are zero-padded to ntpad = floor(1/dt/df) samples and Fourier
+    transformed; bins 2..win+1 are multiplied by -1i*dk*y/(2 pi) (F1=0, the predicted data
+    seismo_v) or -1i*dk*y*exp(-1i*dk*y)/(2 pi) (F1=1, the observed data seismo_v_d), with
+    dk = 2 pi f (cr_0 - cr_pre)/(cr_0 cr_pre) at bins ind..ind+npair-1 and 0 at the other
+    bins up to win, and y the trace's offset in metres; bins ntpad-win+1..ntpad are set to the
+    conjugates; the other bins keep the data's spectrum.  The inverse transform's first nt
+    samples are the adjoint source.  The left side runs for is > round(w/M)+floor(m/M)+1
+    (strictly greater, unlike ADWDgrad_1) and is written after the right side."""
+    nt, b = np.shape(seismo_v_d)[:2]
+    fre = 2 * np.pi * mlinspace(fmin, fmax, (fmax - fmin) / df + 1)  # :4
+    npair = fre.size
+    ntpad = int(math.floor(1 / dt / df))                               # :10
+    ind, win = int(ind), int(win)
+    if nt > ntpad or 2 * win >= ntpad or ind < 1 or ind + npair - 1 > win:
+        raise ValueError("weight_data_muti3 needs nt <= ntpad, 2*win < ntpad and ind+npair-1 <= win")
+    src = np.asarray(seismo_v_d if F1 == 1 else seismo_v, np.float64)
+    out = np.zeros((nt, b))
+    rs = int(refsx[is_ - 1])
+
+    def filtered(c_first, c_last, y, cr0, crp):
+        if c_last < c_first:
+            raise ValueError(f"shot {is_}: empty WD window")
+        dk = np.zeros(win)
+        dk[ind - 1:ind - 1 + npair] = fre * (np.asarray(cr0, np.float64) - crp) / (cr0 * np.asarray(crp))
+        temp = np.zeros((ntpad, c_last - c_first + 1))
+        temp[:nt] = src[:, c_first - 1:c_last]
+        spec = np.fft.fft(temp, axis=0)
+        th = (-1j * dk[:, None]) * y[None, :]
+        fac = (th * np.exp(th)) / np.pi / 2 if F1 == 1 else th / np.pi / 2   # :37-41
+        for om in range(1, win + 1):                                         # :48-56
+            spec[om] = spec[om] * fac[om - 1]
+            spec[ntpad - om] = np.conj(spec[om])
+        return np.real(np.fft.ifft(spec, axis=0))[:nt]
+
+    if is_ <= ns - math.floor(m / M) - mround(w / M):                       # :21-68
+        nend = min(m + offset - 1 + rs, b)
+        newoffset = nend - (rs + m) + 1
+        c0 = mround(m + rs)
+        y = (m + mlinspace(0, newoffset - 1, newoffset)) * dg
+        out[:, c0 - 1:nend] = filtered(c0, nend, y, cr_0, cr_pre_r)
+    if is_ > mround(w / M) + math.floor(m / M) + 1:                         # :74-121
+        nend = max(rs - offset - m, 0)
+        newoffset = rs - m - nend
+        y = (m + mlinspace(newoffset - 1, 0, newoffset)) * dg
+        out[:, nend:rs - m] = filtered(nend + 1, rs - m, y, cr_0l, cr_pre_l)
+    return out
+
+
+def wd_direct(x, k_lo, fac, ntpad):
+    """The same filter as weight_data_muti3 on one zero-padded trace, without FFTs: x plus
+    (2/ntpad) Re sum_k (fac_k - 1) X_k exp(2 pi i k t / ntpad) over bins k = 1..len(fac).
+    A cross-check of the restatement's bin bookkeeping."""
+    x = np.asarray(x, np.float64)
+    t = np.arange(x.size)
+    k = np.arange(k_lo, k_lo + len(fac))
+    E = np.exp(-2j * np.pi * np.outer(k, t) / ntpad)
+    X = E @ x
+    d = (np.asarray(fac) - 1) * X
+    return x + 2.0 / ntpad * np.real(d @ E.conj())
 
 
 def has_right(is_, ns, m, M, w):
@@ -672,7 +768,7 @@ def observed_curves(s, vs, single=True, vp=None):
     return cr, cl
 
 
-def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True, single=True, vp=None):
+def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True, single=True, vp=None, weight="softmax"):
     """SWD_single.m:172-193 for one shot: forward (FP32), spectra, picks, ADWDgrad_1, adjoint.
     single=False: SWD.m's double path (FP64 FD, adjoint source kept in double)."""
     inp = _survey_fd(s, is_, vs, single, vp=vp)
@@ -686,23 +782,35 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True, single=True, vp=Non
         out["res_l"], out["crp_l"] = LHDispPick(sp["l"][0], s.vmin, cr0_l[:, is_ - 1], 1, s.ini)
     gr = out["crp_r"] - cr0_r[:, is_ - 1]
     gl = out["crp_l"] - cr0_l[:, is_ - 1]
-    a = ADWDgrad_1(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl,
-                   sp.get("r", (0, 0, None))[2], sp.get("l", (0, 0, None))[2])
+    if weight == "wd":  # SWD.m:188 (F1 = 0), ind/win of SWD.m:124-127, refsx of SWD.m:96
+        dgc = int(s.gx[1] - s.gx[0])
+        ind = s.fmin / s.df + 1
+        a = weight_data_muti3(sw, sw.astype(np.float64), is_, s.dt, s.df, s.offset, s.ds, 0, s.w, s.M, s.m, s.ns,
+                              np.floor(np.asarray(s.sx) / dgc) + 1, npair + 2 * ind, s.fmin, s.fmax,
+                              cr0_r[:, is_ - 1], cr0_l[:, is_ - 1], out["crp_r"], out["crp_l"], ind)
+    elif weight == "gauss":  # SWD.m:178,184 keep cr_pre - vmin in saveForBackward
+        a = ADWDgrad_norm(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl,
+                          sp.get("r", (0, 0, None))[2], sp.get("l", (0, 0, None))[2], out["crp_r"] - s.vmin,
+                          out["crp_l"] - s.vmin)
+    else:
+        a = ADWDgrad_1(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl,
+                       sp.get("r", (0, 0, None))[2], sp.get("l", (0, 0, None))[2])
     out["adj_src"] = a.astype(np.float32) if single else a
     ainp = _survey_fd(s, is_, vs, single, adjoint=True, vp=vp)
     out["cl"], out["cm"], out["il"] = mex_e2drtm(ainp, out["adj_src"], wf, accum_fp64)
     return out
 
 
-def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=True, single=True, vp=None):
+def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=True, single=True, vp=None, weight="softmax"):
     """SWD_single.m:171-201 (SWD.m with single=False) with the shot sum in FP64 in shot order."""
     from concurrent.futures import ThreadPoolExecutor
     shots = list(range(1, s.ns + 1))
     if threads > 1:
         with ThreadPoolExecutor(threads) as ex:
-            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp), shots))
+            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight),
+                              shots))
     else:
-        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp) for i in shots]
+        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight) for i in shots]
     g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
     for p in per:
         for k in g:

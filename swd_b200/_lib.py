@@ -49,6 +49,9 @@ _SIGS = {
     "swd_pick_noalloc": [ctypes.c_void_p, _c_int, _c_int, _c_dbl, ctypes.c_void_p, _c_int, _c_int,
                          ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
     "swd_adwdgrad": [_rpp, _c_int, _c_int, _c_int, _c_dbl] + [_f64p] * 8,
+    "swd_adwdgrad_norm": [_rpp, _c_int, _c_int, _c_int, _c_dbl] + [_f64p] * 10,
+    "swd_wd_residual": [_c_int, _c_int, _f64p, _f64p, _c_int, _c_dbl, _c_dbl, _c_int, _c_dbl, _c_int, _c_int,
+                        _c_dbl, _c_int, _c_int, _f64p, _c_int, _c_dbl, _c_dbl] + [_f64p] * 4 + [_c_int, _f64p],
 }
 _RESTYPE = {"swd_last_error": ctypes.c_char_p, "swd_kernel_launches": ctypes.c_uint64}
 

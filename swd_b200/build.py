@@ -31,6 +31,7 @@ SOURCES = {
     "pick_noalloc.cu": [],
     "server.cu": [],
     "radon_tc.cu": [],
+    "wd.cu": [],
 }
 
 

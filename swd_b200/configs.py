@@ -204,3 +204,40 @@ def smooth_curve(s, seed=0):
     span = s.vmax - s.vmin
     base = s.vmin + span * (0.15 + 0.35 * np.exp(-f / max(1.0, s.npair / 3)))
     return np.round(base + rng.normal(0, 2.0, (1, s.ns)))
+
+
+def _grf(shape, corr, rng):
+    """Zero-mean, unit-variance Gaussian random field with a Gaussian correlation of `corr` cells."""
+    nz, nx = shape
+    w = rng.standard_normal(shape)
+    kz = np.fft.fftfreq(nz)[:, None]
+    kx = np.fft.rfftfreq(nx)[None, :]
+    f = np.fft.irfft2(np.fft.rfft2(w) * np.exp(-2 * (np.pi * corr) ** 2 * (kz ** 2 + kx ** 2)), s=shape)
+    return (f - f.mean()) / f.std()
+
+
+def large_c5(ns=240, nt=20000) -> Survey:
+    """400 x 3000 grid, dx 0.25 m, 240 shots (every 10th column) x 1200 receivers (every 2nd), nt 20000,
+    dt 2.5e-5 s, Ricker f0 40 Hz.  Vs: seeded layers from 150 to 800 m/s whose interfaces drop
+    3 m across a vertical fault, times a Gaussian random field (correlation 5 m, +/-8% at two
+    standard deviations); Vp = 1.8 Vs."""
+    nz, nx, dx = 400, 3000, 0.25
+    rng = np.random.default_rng(5)
+    nl = 6
+    vel = np.linspace(150.0, 800.0, nl)
+    cuts = np.sort(rng.choice(np.arange(30, nz - 30), nl - 1, replace=False))
+    throw = int(round(3.0 / dx))
+    xf = int(rng.integers(nx // 3, 2 * nx // 3))
+    z = np.arange(nz)[:, None]
+    left = np.searchsorted(cuts, z, side="right")
+    right = np.searchsorted(cuts + throw, z, side="right")
+    layer = np.where(np.arange(nx)[None, :] < xf, left, right)
+    vs = vel[layer] * (1.0 + 0.04 * _grf((nz, nx), 5.0 / dx, rng))
+    vs_true = vs.copy()
+    zz, xx = np.mgrid[0:nz, 0:nx]
+    vs_true *= 1.0 - 0.10 * np.exp(-(((zz - nz // 3) / 40.0) ** 2 + ((xx - nx // 2) / 200.0) ** 2))
+    # shots every 10 columns (5 receivers): 240 shots then span the 2400 columns the receivers
+    # cover (a 12-column spacing would put the last 40 shots' windows past the receiver line)
+    sx = 1 + 10 * np.arange(ns)
+    return Survey("large-400x3000", nz, nx, dx, 40, 2.5e-5, nt, 40.0, sx, np.arange(1, 2400, 2), 5,
+                  vs=vs, vs_true=vs_true, vp_ratio=1.8)

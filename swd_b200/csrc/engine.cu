@@ -20,6 +20,7 @@
 #include "fd_host.cuh"
 #include "model_prep.cuh"
 #include "radon.cuh"
+#include "wd.cuh"
 
 namespace swd {
 
@@ -100,6 +101,9 @@ struct swd_engine {
   DevBuf W, K, gath, D, MM, mlraw, ml, Gx;
   DevBuf cr0, crp, dc, gres, status;
   DevBuf outbuf;       // staging for host outputs
+  // WD adjoint source (adjoint_weight 2): geometry, gathers, bin table, pick frequencies, DFT scratch
+  WdGeom wg{};
+  DevBuf wgath, Ww, wfre, Xw;
   bool have_source = false, have_observed = false;
   double tuned_fwd_us = 0, tuned_adj_us = 0;  // autotune: chosen variants' step times
   swd_contract* tc = nullptr;                  // split-BF16 forward contraction (radon_precision)
@@ -125,10 +129,14 @@ static int plan(swd_engine* e) {
   const size_t plane = e->plane;
   const RadonGeom& rg = e->rg;
   const size_t tables = (size_t)rg.npair * rg.ntd * 16 + (size_t)rg.npair * rg.offset * rg.np * 16;
-  const size_t fixed = 2 * e->g.field * sizeof(float4) + 2 * (size_t)e->sv.nz * e->sv.nx * 8 + tables +
+  size_t fixed = 2 * e->g.field * sizeof(float4) + 2 * (size_t)e->sv.nz * e->sv.nx * 8 + tables +
                        5 * plane * 8 + (size_t)2 * e->ns * rg.npair * 8 * 3 + (64 << 20);
   const size_t gather = (size_t)rg.npair * rg.offset * 16 * 2 + (size_t)rg.npair * rg.np * (16 + 8 + 8);
-  const size_t per_common = 2 * 5 * field + 2 * (size_t)g.nt * g.ng * 4 + 3 * plane * 8 + 2 * gather;
+  const bool wd = e->opt.adjoint_weight == 2;
+  const size_t wd_fixed = wd ? (size_t)e->wg.win * g.nt * 16 + (size_t)e->wg.nfre * 8 + (size_t)2 * e->ns * 32 : 0;
+  fixed += wd_fixed;
+  const size_t per_common = 2 * 5 * field + 2 * (size_t)g.nt * g.ng * 4 + 3 * plane * 8 + 2 * gather +
+                            (wd ? (size_t)2 * e->wg.win * rg.offset * 16 : 0);
   const size_t per_store = per_common + (size_t)g.nrec * 3 * plane * 4;
   size_t budget = e->opt.hbm_budget;
   if (budget == 0) {
@@ -138,7 +146,13 @@ static int plan(swd_engine* e) {
   }
   SWD_CHECK(budget > fixed, "HBM budget %zu bytes below the fixed tables (%zu)", budget, fixed);
   const size_t avail = budget - fixed;
-  int ck = e->opt.ckpt_interval > 0 ? e->opt.ckpt_interval : 50;
+  int ck = e->opt.ckpt_interval;
+  if (ck <= 0) {
+    // memory-optimal interval: a shot holds nt/ck checkpoints of 5 fields and ck/nt_wf
+    // snapshot records of 3 planes; their sum is smallest at ck = sqrt(nt * 5 field * nt_wf / (3 plane))
+    const double c = std::sqrt((double)g.nt * 5.0 * (double)field * g.nt_wf / (3.0 * (double)plane * 4.0));
+    ck = std::max(g.nt_wf, std::min(g.nt, (int)std::lround(c / g.nt_wf) * g.nt_wf));
+  }
   ck = std::max(g.nt_wf, ck / g.nt_wf * g.nt_wf);
   const int nseg = (g.nt + ck - 1) / ck;
   const size_t per_ckpt = per_common + 2 * 5 * field + (size_t)nseg * 5 * field + (size_t)(ck / g.nt_wf) * 3 * plane * 4;
@@ -206,6 +220,12 @@ static int alloc_all(swd_engine* e) {
   SWD_TRY(e->dc.alloc(GA * rg.npair * sizeof(double)));
   SWD_TRY(e->gres.alloc(GA * sizeof(double)));
   SWD_TRY(e->status.alloc(GA * sizeof(int)));
+  if (e->opt.adjoint_weight == 2) {
+    SWD_TRY(e->wgath.alloc((size_t)e->nbatch * G2 * sizeof(Gather)));
+    SWD_TRY(e->Ww.alloc((size_t)e->wg.win * g.nt * sizeof(double2)));
+    SWD_TRY(e->wfre.alloc((size_t)e->wg.nfre * sizeof(double)));
+    SWD_TRY(e->Xw.alloc(G2 * e->wg.win * rg.offset * sizeof(double2)));
+  }
   return SWD_OK;
 }
 
@@ -450,8 +470,18 @@ static int spectrum_batch(swd_engine* e, int bi, int s0, int nb, bool grad) {
                      e->cr0.as<double>() + go * rg.npair, e->crp.as<double>() + go * rg.npair,
                      e->dc.as<double>() + go * rg.npair, e->gres.as<double>() + go, e->status.as<int>() + go, e->st));
   if (!grad) return SWD_OK;
+  if (e->opt.adjoint_weight == 2) {  // WD residual of the predicted data (SWD.m:188, F1 = 0)
+    SWD_CUDA(cudaMemsetAsync(e->res.p, 0, (size_t)e->B * sstride * sizeof(float), e->st));
+    const Gather* wgs = e->wgath.as<Gather>() + (size_t)bi * G;
+    return wd_adjoint<float, float>(e->wg, wgs, G, e->seis.as<float>(), sstride, e->Ww.as<double2>(),
+                                    e->wfre.as<double>(), e->cr0.as<double>() + go * rg.npair,
+                                    e->crp.as<double>() + go * rg.npair, e->Xw.as<double2>(), e->res.as<float>(),
+                                    sstride, e->st);
+  }
+  const bool gauss = e->opt.adjoint_weight == 1;  // ADWDgrad_norm: Gaussian around the picks
   SWD_TRY(softmax_adjoint(rg, gs, G, e->mlraw.as<double>(), e->MM.as<double2>(), e->dc.as<double>() + go * rg.npair,
-                          nullptr, e->sv.soft_arg_norm, e->K.as<double2>(), e->Gx.as<double2>(), e->st));
+                          nullptr, e->sv.soft_arg_norm, e->K.as<double2>(), e->Gx.as<double2>(), e->st,
+                          gauss ? e->crp.as<double>() + go * rg.npair : nullptr, e->sv.vmin));
   SWD_CUDA(cudaMemsetAsync(e->res.p, 0, (size_t)e->B * sstride * sizeof(float), e->st));
   SWD_TRY(radon_idft_scatter<float>(rg, gs, G, e->Gx.as<double2>(), e->W.as<double2>(), e->res.as<float>(), sstride,
                                     e->st));
@@ -629,6 +659,20 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   SWD_TRY(radon_geom(&rp, e->rg));
   SWD_CHECK(e->rg.ccn >= s->nt, "ADWDgrad_1 needs ccn = fix(1/df/dt) (%d) >= nt (%d)", e->rg.ccn, s->nt);
   SWD_CHECK(s->ini >= 1 && s->ini <= e->rg.npair, "ini (%d) must lie in 1..npair (%d)", s->ini, e->rg.npair);
+  SWD_CHECK(e->opt.adjoint_weight >= 0 && e->opt.adjoint_weight <= 2,
+            "adjoint_weight must be 0 (ADWDgrad_1), 1 (ADWDgrad_norm) or 2 (weight_data_muti3)");
+  if (e->opt.adjoint_weight == 2) {
+    // SWD.m:124-127: ind = fmin/df+1, npair = length(fmin:df:fmax), win = npair+2*ind
+    const double ind = s->fmin / s->df + 1;
+    SWD_CHECK(ind == std::floor(ind) && ind >= 1 && ind < 1e7, "the WD residual needs fmin/df+1 (%g) to be an integer",
+              ind);
+    const int win = e->rg.npair + 2 * (int)ind;
+    SWD_TRY(wd_geom(s->nt, s->ng, s->dt, s->df, s->offset, s->m, win, (int)ind, s->fmin, s->fmax, s->dgx * s->dx, 0,
+                    e->wg));
+    SWD_CHECK(e->wg.nfre == e->rg.npair, "linspace(fmin,fmax,(fmax-fmin)/df+1) has %d points, the picks %d",
+              e->wg.nfre, e->rg.npair);
+    e->wg.npair = e->rg.npair;
+  }
   SWD_TRY(plan(e));
   plan_decomposition(g, e->B, e->opt.chunk_rows);
   e->gseg = g;
@@ -666,6 +710,30 @@ static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engi
     }
   SWD_CUDA(cudaMemcpyAsync(e->gath.p, hg.data(), hg.size() * sizeof(Gather), cudaMemcpyHostToDevice, e->st));
   SWD_TRY(radon_tables(e->rg, e->W.as<double2>(), e->K.as<double2>(), e->st));
+  std::vector<Gather> hw;
+  std::vector<double> hfre;
+  if (e->opt.adjoint_weight == 2) {  // WD gathers: refsx = floor(sx/dg)+1 (SWD.m:96)
+    hw.resize(hg.size());
+    for (int bi = 0; bi < e->nbatch; ++bi)
+      for (int b = 0; b < e->B; ++b) {
+        const int sidx = bi * e->B + b;
+        for (int side = 0; side < 2; ++side) {
+          Gather gg{};
+          if (sidx < e->ns) {
+            const int refsx = (int)std::floor((double)e->sx[sidx] / s->dgx) + 1;
+            gg = make_wd_gather(e->wg, e->shot_no[sidx], side, b, e->ns_total, s->w, (double)s->M, refsx);
+            SWD_CHECK(gg.valid >= 0, "shot %d: the %s WD window is empty or leaves the receiver line",
+                      e->shot_no[sidx], side ? "left" : "right");
+          }
+          hw[((size_t)bi * e->B + b) * 2 + side] = gg;
+        }
+      }
+    hfre.resize(e->wg.nfre);
+    wd_fre(s->fmin, s->fmax, e->wg.nfre, hfre.data());
+    SWD_CUDA(cudaMemcpyAsync(e->wgath.p, hw.data(), hw.size() * sizeof(Gather), cudaMemcpyHostToDevice, e->st));
+    SWD_CUDA(cudaMemcpyAsync(e->wfre.p, hfre.data(), hfre.size() * sizeof(double), cudaMemcpyHostToDevice, e->st));
+    SWD_TRY(radon_tables(e->wg.dft, e->Ww.as<double2>(), nullptr, e->st));
+  }
   if (e->opt.autotune) SWD_TRY(autotune(e));
   if (e->opt.radon_precision == SWD_PREC_BF16X2 || e->opt.radon_precision == SWD_PREC_BF16X3) {
     // the engine's axes: kept bins lf..nf, velocities vmin + dv*p, offsets (m + x)*ds (RTrAD.m:11,18-21)

@@ -474,7 +474,8 @@ __global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const
                                                               const double2* __restrict__ MM,
                                                               const double* __restrict__ dc,
                                                               const double* __restrict__ space_m, double beta,
-                                                              const double2* __restrict__ K, double2* Gx) {
+                                                              const double2* __restrict__ K, double2* Gx,
+                                                              const double* __restrict__ pick, double pick_off) {
   extern __shared__ double2 sgm[];
   __shared__ double red[33];
   const int f = blockIdx.x, gi = blockIdx.y;
@@ -482,16 +483,30 @@ __global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const
   if (gg.valid <= 0) return;
   const size_t col = (size_t)gi * g.npair + f;
   const double* mr = mlraw + col * g.np;
-  // E = softmax(beta * mlr.^(1/40)) over p (ADWDgrad_1.m:22-23), max-shifted in FP64
-  double zmax = -1.0 / 0.0;
-  for (int p = threadIdx.x; p < g.np; p += blockDim.x) zmax = fmax(zmax, pow(mr[p], 1.0 / 40.0) * beta);
-  zmax = block_max(zmax, red);
-  double se = 0.0;
-  for (int p = threadIdx.x; p < g.np; p += blockDim.x) se += exp(pow(mr[p], 1.0 / 40.0) * beta - zmax);
-  se = block_sum(se, red);
+  // Weights over p.  ADWDgrad_1.m:22-23: E = softmax(beta * mlr.^(1/40)), max-shifted in FP64.
+  // ADWDgrad_norm.m:22-23 (pick != null): E = normpdf(1:np, cr, 16) around the pick cr =
+  // cr_pre - vmin (paddingMl_norm.m:5-7), not normalised.
+  double zmax = 0.0, se = 1.0, mu = 0.0;
+  if (pick) {
+    mu = pick[(size_t)gi * g.npair + f] - pick_off;
+  } else {
+    zmax = -1.0 / 0.0;
+    for (int p = threadIdx.x; p < g.np; p += blockDim.x) zmax = fmax(zmax, pow(mr[p], 1.0 / 40.0) * beta);
+    zmax = block_max(zmax, red);
+    se = 0.0;
+    for (int p = threadIdx.x; p < g.np; p += blockDim.x) se += exp(pow(mr[p], 1.0 / 40.0) * beta - zmax);
+    se = block_sum(se, red);
+  }
+  auto weight = [&](int p) -> double {
+    if (pick) {
+      const double z = ((double)(p + 1) - mu) / 16.0;
+      return exp(-0.5 * (z * z)) / (2.5066282746310002 * 16.0);  // sqrt(2*pi) * sigma
+    }
+    return exp(pow(mr[p], 1.0 / 40.0) * beta - zmax) / se;
+  };
   double sm = 0.0;
   for (int p = threadIdx.x; p < g.np; p += blockDim.x) {
-    const double E = exp(pow(mr[p], 1.0 / 40.0) * beta - zmax) / se;
+    const double E = weight(p);
     const double s = space_m ? space_m[(size_t)f * g.np + p] : (double)(p + 1);
     sm += s * E;
   }
@@ -499,7 +514,7 @@ __global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const
   double d = dc[(size_t)gi * g.npair + f];
   if (d == 0.0) d = 1.0;  // grad_output(grad_output==0)=1 (ADWDgrad_1.m:26)
   for (int p = threadIdx.x; p < g.np; p += blockDim.x) {
-    const double E = exp(pow(mr[p], 1.0 / 40.0) * beta - zmax) / se;
+    const double E = weight(p);
     const double s = space_m ? space_m[(size_t)f * g.np + p] : (double)(p + 1);
     const double gml = (((E * s - sm * E) * 2.0) * d) * beta;   // :28-31
     const double2 m = MM[col * g.np + p];
@@ -530,12 +545,12 @@ __global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const
 
 int softmax_adjoint(const RadonGeom& g, const Gather* d_gath, int G, const double* mlraw, const double2* MM,
                     const double* dc, const double* space_m, double beta, const double2* K, double2* Gx,
-                    cudaStream_t st) {
+                    cudaStream_t st, const double* pick, double pick_off) {
   dim3 grid(g.npair, G);
   const size_t smem = (size_t)g.np * sizeof(double2);
   if (smem > 48 * 1024)
     SWD_CUDA(cudaFuncSetAttribute(softmax_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  softmax_adjoint_kernel<<<grid, 256, smem, st>>>(g, d_gath, mlraw, MM, dc, space_m, beta, K, Gx);
+  softmax_adjoint_kernel<<<grid, 256, smem, st>>>(g, d_gath, mlraw, MM, dc, space_m, beta, K, Gx, pick, pick_off);
   count_launch(1);
   SWD_CUDA(cudaGetLastError());
   return SWD_OK;
@@ -693,10 +708,13 @@ int swd_pick(const double* ml, int np_, int npair, double vmin, const double* cr
   return SWD_OK;
 }
 
-int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm, const double* grad_output_r,
-                 const double* grad_output_l, const double* space_m, const double* mm_r, const double* ml_raw_r,
-                 const double* mm_l, const double* ml_raw_l, double* a_data_res) {
-  clear_error();
+}  // extern "C"
+
+// ADWDgrad_1 (picks null) or ADWDgrad_norm (picks cr_r / cr_l) of one shot.
+static int adwdgrad_impl(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
+                         const double* grad_output_r, const double* grad_output_l, const double* space_m,
+                         const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
+                         const double* cr_r, const double* cr_l, bool gauss, double* a_data_res) {
   RadonGeom g{};
   SWD_TRY(radon_geom(p, g));
   SWD_CHECK(a_data_res, "null a_data_res");
@@ -705,15 +723,18 @@ int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_a
   const double* mm[2] = {mm_r, mm_l};
   const double* raw[2] = {ml_raw_r, ml_raw_l};
   const double* go[2] = {grad_output_r, grad_output_l};
+  const double* cr[2] = {cr_r, cr_l};
   for (int s = 0; s < 2; ++s) {
     gg[s] = make_gather(g, is, s, 0, ns, w);
     if (gg[s].valid) {
       SWD_CHECK(gg[s].valid == 1, "shot %d: %s window is empty", is, s ? "left" : "right");
       SWD_CHECK(mm[s] && raw[s] && go[s], "missing saved state for the %s side", s ? "left" : "right");
+      SWD_CHECK(!gauss || cr[s], "missing picks cr_%s for the %s side", s ? "l" : "r", s ? "left" : "right");
     }
   }
   const size_t spec = (size_t)g.npair * g.np, nsz = (size_t)g.nt * g.ng;
-  DevBuf b_W, b_K, b_MM, b_raw, b_dc, b_sm, b_Gx, b_out, b_out_t, b_g;
+  DevBuf b_W, b_K, b_MM, b_raw, b_dc, b_sm, b_Gx, b_out, b_out_t, b_g, b_cr;
+  if (gauss) SWD_TRY(b_cr.alloc(2 * (size_t)g.npair * sizeof(double)));
   SWD_TRY(b_W.alloc((size_t)g.npair * g.ntd * sizeof(double2)));
   SWD_TRY(b_K.alloc((size_t)g.npair * g.offset * g.np * sizeof(double2)));
   SWD_TRY(b_MM.alloc(2 * spec * sizeof(double2)));
@@ -732,6 +753,9 @@ int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_a
     SWD_CUDA(cudaMemcpyAsync(b_raw.as<double>() + s * spec, raw[s], spec * sizeof(double), cudaMemcpyHostToDevice, st));
     SWD_CUDA(cudaMemcpyAsync(b_dc.as<double>() + s * g.npair, go[s], g.npair * sizeof(double),
                              cudaMemcpyHostToDevice, st));
+    if (gauss)
+      SWD_CUDA(cudaMemcpyAsync(b_cr.as<double>() + s * g.npair, cr[s], g.npair * sizeof(double),
+                               cudaMemcpyHostToDevice, st));
   }
   if (space_m) SWD_CUDA(cudaMemcpyAsync(b_sm.p, space_m, spec * sizeof(double), cudaMemcpyHostToDevice, st));
   gg[0].shot = 0;
@@ -741,7 +765,7 @@ int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_a
   SWD_TRY(radon_tables(g, b_W.as<double2>(), b_K.as<double2>(), st));
   SWD_TRY(softmax_adjoint(g, b_g.as<Gather>(), 2, b_raw.as<double>(), b_MM.as<double2>(), b_dc.as<double>(),
                           space_m ? b_sm.as<double>() : nullptr, soft_arg_norm, b_K.as<double2>(),
-                          b_Gx.as<double2>(), st));
+                          b_Gx.as<double2>(), st, gauss ? b_cr.as<double>() : nullptr));
   SWD_TRY(radon_idft_scatter<double>(g, b_g.as<Gather>(), 2, b_Gx.as<double2>(), b_W.as<double2>(),
                                      b_out.as<double>(), 0, st));
   // [nt][ng] -> MATLAB nt x ng
@@ -749,6 +773,25 @@ int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_a
   SWD_CUDA(cudaMemcpyAsync(a_data_res, b_out_t.p, nsz * sizeof(double), cudaMemcpyDeviceToHost, st));
   SWD_CUDA(cudaStreamSynchronize(st));
   return SWD_OK;
+}
+
+extern "C" {
+
+int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm, const double* grad_output_r,
+                 const double* grad_output_l, const double* space_m, const double* mm_r, const double* ml_raw_r,
+                 const double* mm_l, const double* ml_raw_l, double* a_data_res) {
+  clear_error();
+  return adwdgrad_impl(p, ns, is, w, soft_arg_norm, grad_output_r, grad_output_l, space_m, mm_r, ml_raw_r, mm_l,
+                       ml_raw_l, nullptr, nullptr, false, a_data_res);
+}
+
+int swd_adwdgrad_norm(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
+                      const double* grad_output_r, const double* grad_output_l, const double* space_m,
+                      const double* mm_r, const double* ml_raw_r, const double* cr_r, const double* mm_l,
+                      const double* ml_raw_l, const double* cr_l, double* a_data_res) {
+  clear_error();
+  return adwdgrad_impl(p, ns, is, w, soft_arg_norm, grad_output_r, grad_output_l, space_m, mm_r, ml_raw_r, mm_l,
+                       ml_raw_l, cr_r, cr_l, true, a_data_res);
 }
 
 }  // extern "C"

@@ -3,6 +3,8 @@
     RTr / RTl / RTrAD / RTlAD   core/RTr.m:2, core/RTl.m:2, core/RTrAD.m:2, core/RTlAD.m:2
     LHDispPick                  core/LHDispPick.m:2 (pickFDC1, core/pickFDC1.m:1)
     ADWDgrad_1                  core/ADWDgrad_1.m:1
+    ADWDgrad_norm               core/ADWDgrad_norm.m:1
+    weight_data_muti3           core/weight_data_muti3.m:1 (the WD adjoint source)
 
 Each call runs on the GPU through libswd.so (FP64, like the reference's MATLAB
 code).  Arrays use MATLAB's layout; saveForBackward is a dict with the
@@ -84,9 +86,23 @@ def LHDispPick(ml, vmin, cr_0, method=1, ini=10):
     return res.value, cr
 
 
+def ADWDgrad_norm(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
+                  saveForBackwardr, saveForBackwardl):
+    """[a_data_res]=ADWDgrad_norm(...) (core/ADWDgrad_norm.m:1): ADWDgrad_1 with normpdf weights
+    around the picks; the saveForBackward dicts carry cr_r / cr_l = cr_pre - vmin (SWD.m:178,184)."""
+    return _adwdgrad(True, nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
+                     saveForBackwardr, saveForBackwardl)
+
+
 def ADWDgrad_1(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
                saveForBackwardr, saveForBackwardl):
     """[a_data_res]=ADWDgrad_1(...) (core/ADWDgrad_1.m:1)."""
+    return _adwdgrad(False, nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
+                     saveForBackwardr, saveForBackwardl)
+
+
+def _adwdgrad(gauss, nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
+              saveForBackwardr, saveForBackwardl):
     sr = saveForBackwardr if isinstance(saveForBackwardr, dict) else None
     sl = saveForBackwardl if isinstance(saveForBackwardl, dict) else None
     p = (sr or sl)["params"]
@@ -107,6 +123,50 @@ def ADWDgrad_1(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_
     mml, rawl, gl = side(sl, grad_outputl, "mll")
     spm = None if space_M is None else np.asfortranarray(np.asarray(space_M, np.float64))
     cp = lambda x: None if x is None else x.ctypes.data_as(dp)
-    call("swd_adwdgrad", ctypes.byref(p), int(ns), int(is_), int(w), float(SoftArgNorm), cp(gr), cp(gl), cp(spm),
-         cp(mmr), cp(rawr), cp(mml), cp(rawl), ptr(a))
+    if gauss:
+        def picks(sv, key):
+            return None if sv is None else np.ascontiguousarray(np.asarray(sv[key], np.float64).reshape(-1))
+        crr, crl = picks(sr, "cr_r"), picks(sl, "cr_l")
+        call("swd_adwdgrad_norm", ctypes.byref(p), int(ns), int(is_), int(w), float(SoftArgNorm), cp(gr), cp(gl),
+             cp(spm), cp(mmr), cp(rawr), cp(crr), cp(mml), cp(rawl), cp(crl), ptr(a))
+    else:
+        call("swd_adwdgrad", ctypes.byref(p), int(ns), int(is_), int(w), float(SoftArgNorm), cp(gr), cp(gl),
+             cp(spm), cp(mmr), cp(rawr), cp(mml), cp(rawl), ptr(a))
     return a
+
+
+def weight_data_muti3(seismo_v_d, seismo_v, is_, dt, df, offset, dg, F1, w, M, m, ns, refsx, win, fmin, fmax,
+                      cr_0, cr_0l, cr_pre_r, cr_pre_l, ind):
+    """[seismo_v_d1]=weight_data_muti3(...) (core/weight_data_muti3.m:1), the WD adjoint source
+    that SWD.m:188 offers: F1=0 filters the predicted data seismo_v, F1=1 the observed data
+    seismo_v_d (the other may be None).  Returns seismo_v_d1 (nt x ng)."""
+    src = seismo_v_d if int(F1) == 1 else seismo_v
+    if src is None:
+        raise ValueError("F1=1 needs seismo_v_d, F1=0 needs seismo_v")
+    src = np.asfortranarray(np.asarray(src, np.float64))
+    if src.ndim != 2:
+        raise ValueError("seismograms must be nt x ng")
+    nt, ng = src.shape
+    other = seismo_v if int(F1) == 1 else seismo_v_d
+    if other is not None and np.shape(other)[:2] != (nt, ng):
+        raise ValueError("seismo_v_d and seismo_v differ in size")
+    refsx = np.ascontiguousarray(np.asarray(refsx, np.float64).reshape(-1))
+    if refsx.size < int(ns):
+        raise ValueError(f"refsx has {refsx.size} entries, ns is {ns}")
+    npair = int(np.floor((fmax - fmin) / df + 1))
+    dp = ctypes.POINTER(ctypes.c_double)
+
+    def picks(a):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1))
+        if a.size != npair:
+            raise ValueError(f"picks have {a.size} entries, linspace(fmin, fmax, ...) has {npair}")
+        return a
+    crs = [picks(a) for a in (cr_0, cr_0l, cr_pre_r, cr_pre_l)]
+    out = np.zeros((nt, ng), order="F")
+    cp = lambda x: None if x is None else x.ctypes.data_as(dp)
+    call("swd_wd_residual", nt, ng, cp(src) if int(F1) == 1 else None, cp(src) if int(F1) == 0 else None, int(is_),
+         float(dt), float(df), int(offset), float(dg), int(F1), int(w), float(M), int(m), int(ns),
+         refsx.ctypes.data_as(dp), int(win), float(fmin), float(fmax), *[cp(c) for c in crs], int(ind), ptr(out))
+    return out

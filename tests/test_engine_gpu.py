@@ -56,6 +56,7 @@ def test_modes_are_bit_identical(tiny_case):
     s, cr0_r, cr0_l, _ = tiny_case
     outs = []
     for kw in ({"snapshot_mode": 1}, {"snapshot_mode": 2, "ckpt_interval": 20}, {"snapshot_mode": 1, "max_batch": 1},
+               {"snapshot_mode": 2},  # memory-optimal checkpoint interval
                {"snapshot_mode": 1, "use_graphs": False, "chunk_rows": 3},
                # one barrier per row (velocities a row ahead): same bits in every mode and chunking
                {"snapshot_mode": 1, "fd_schedule": 1}, {"snapshot_mode": 2, "ckpt_interval": 20, "fd_schedule": 1},
@@ -175,3 +176,29 @@ def test_split_bf16_radon_in_the_engine(tiny_case):
     err = _rel(b["dk_vs"], a["dk_vs"])
     print("identical picks", same, "dk rel L2", err)
     assert same >= 0.95 and err < 1e-2
+
+
+def test_gaussian_adjoint_weight_matches_oracle(tiny_case):
+    """adjoint_weight='gauss' (ADWDgrad_norm) in the engine against the oracle's shot loop."""
+    from oracle import swd_oracle as O
+    s, cr0_r, cr0_l, _ = tiny_case
+    ref = O.gradient(s, s.vs, cr0_r, cr0_l, weight="gauss")
+    with GradientEngine(s, adjoint_weight="gauss") as e:
+        e.set_observed(cr0_r, cr0_l)
+        out = e.gradient(s.vp, s.vs)
+    assert np.array_equal(out["cr_pre_r"], ref["cr_pre_r"])
+    for k in ("g_cl", "g_cm", "g_illum", "dk_vs"):
+        assert _rel(out[k], ref[k]) < TOL, k
+
+
+def test_wd_adjoint_source_matches_oracle(tiny_case):
+    """adjoint_weight='wd' (weight_data_muti3, SWD.m:188) in the engine against the oracle's shot loop."""
+    from oracle import swd_oracle as O
+    s, cr0_r, cr0_l, _ = tiny_case
+    ref = O.gradient(s, s.vs, cr0_r, cr0_l, weight="wd")
+    with GradientEngine(s, adjoint_weight="wd") as e:
+        e.set_observed(cr0_r, cr0_l)
+        out = e.gradient(s.vp, s.vs)
+    assert np.array_equal(out["cr_pre_r"], ref["cr_pre_r"])
+    for k in ("g_cl", "g_cm", "g_illum", "dk_vs"):
+        assert _rel(out[k], ref[k]) < TOL, k

@@ -17,7 +17,8 @@ import mexsim  # noqa: E402
 from swd_b200 import configs  # noqa: E402
 
 SHIMS = ["eigen_staggerfd_single", "eigen_staggerfd_double", "eigen_e2drtm_single", "eigen_e2drtm_double",
-         "RTrAD", "RTlAD", "RTr", "RTl", "LHDispPick", "ADWDgrad_1"]
+         "RTrAD", "RTlAD", "RTr", "RTl", "LHDispPick", "ADWDgrad_1", "ADWDgrad_norm",
+         "weight_data_muti3"]
 
 
 @pytest.fixture(scope="module")
@@ -146,3 +147,32 @@ def test_spectrum_shims_match_the_c_abi(O, shim):
     ra = SP.ADWDgrad_1(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl, space, out[0][2],
                        out[1][2])
     assert np.abs(ra).max() > 0 and np.array_equal(a, ra)
+    # ADWDgrad_norm: the structs also carry the picks minus vmin (SWD.m:178, :184)
+    cr_r, cr_l = rcr - s.vmin, np.linspace(2.0, npv - 2.0, npair)
+    sr, sl = dict(out[0][1], cr_r=cr_r), dict(out[1][1], cr_l=cr_l)
+    an = shim("ADWDgrad_norm")(1, s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl, space,
+                               sr, sl)[0]
+    ran = SP.ADWDgrad_norm(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl, space,
+                           dict(out[0][2], cr_r=cr_r), dict(out[1][2], cr_l=cr_l))
+    assert np.abs(ran).max() > 0 and np.array_equal(an, ran)
+    with pytest.raises(mexsim.MexError, match="cr_r"):
+        shim("ADWDgrad_norm")(1, s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl, space,
+                              out[0][1], sl)
+
+
+@pytest.mark.gpu
+def test_wd_shim_matches_the_c_abi(O, shim):
+    from swd_b200 import spectrum as SP
+    rng = np.random.default_rng(4)
+    nt, ng, dt, df, fmin, fmax = 300, 40, 1e-3, 2.0, 10.0, 40.0
+    ind, npair = 6, 16
+    refsx = np.floor(1 + 3 * np.arange(12)) + 1
+    pred = rng.standard_normal((nt, ng)).astype(np.float32)  # SWD_single.m's single seismo_v
+    cr0, crp = 300 + 50 * rng.random(npair), 300 + 50 * rng.random(npair)
+    args = (5, dt, df, 12, 0.5, 0, 3, 3.0, 0, 12, refsx, npair + 2 * ind, fmin, fmax, cr0, cr0[::-1].copy(), crp,
+            crp[::-1].copy(), float(ind))
+    got = shim("weight_data_muti3")(1, np.zeros((nt, ng)), pred, *args)[0]
+    want = SP.weight_data_muti3(None, pred.astype(np.float64), *args)
+    assert np.abs(want).max() > 0 and np.array_equal(got, want)
+    with pytest.raises(mexsim.MexError, match="picks"):
+        shim("weight_data_muti3")(1, np.zeros((nt, ng)), pred, *args[:14], cr0[:5], *args[15:])

@@ -200,3 +200,57 @@ def test_adwdgrad_sides_disjoint(O):
     src_col = s.M * is_ - s.M + 1
     nz_cols = np.nonzero(np.abs(a).sum(0))[0] + 1
     assert nz_cols.min() >= max(1, src_col - s.offset) and nz_cols.max() <= min(s.ng, src_col + s.offset - 1)
+
+
+def test_normpdf_weights_match_scipy(O):
+    """paddingMl_norm.m's normpdf(1:np, cr, 16) against scipy's normal density."""
+    from scipy.stats import norm
+    cr = np.array([1.0, 17.5, 80.0, 140.0])
+    w = O.normpdf_cols(141, cr)
+    ref = norm.pdf(np.arange(1, 142)[:, None], loc=cr[None, :], scale=16.0)
+    np.testing.assert_allclose(w, ref, rtol=1e-13, atol=0)
+
+
+@pytest.mark.parametrize("F1", [0, 1])
+def test_wd_restatement_matches_direct_low_bin_filter(O, F1):
+    """weight_data_muti3 (FFT, bin loop, conjugate mirror) against the same filter written as
+    x + (2/ntpad) Re sum_k (fac_k - 1) X_k e^{2 pi i k t/ntpad}: bin bookkeeping, window
+    columns, offsets and the strict left-side rule."""
+    rng = np.random.default_rng(11)
+    nt, ng, dt, df, fmin, fmax = 300, 40, 1e-3, 2.0, 10.0, 40.0
+    ntpad = int(1 / dt / df)
+    ind = int(fmin / df + 1)
+    npair = int((fmax - fmin) / df + 1)
+    win = npair + 2 * ind
+    offset, m, M, w, ns, dg = 12, 0, 3, 3, 12, 0.5
+    refsx = np.floor((1 + 3 * np.arange(ns)) / 1) + 1
+    obs, pred = rng.standard_normal((nt, ng)), rng.standard_normal((nt, ng))
+    cr0, cr0l = 300 + 50 * rng.random(npair), 300 + 50 * rng.random(npair)
+    crp, crpl = cr0 + rng.integers(-20, 21, npair), cr0l + rng.integers(-20, 21, npair)
+    fre = 2 * np.pi * O.mlinspace(fmin, fmax, npair)
+    for is_ in (1, 2, 5, 12):
+        got = O.weight_data_muti3(obs, pred, is_, dt, df, offset, dg, F1, w, M, m, ns, refsx, win, fmin, fmax, cr0,
+                                  cr0l, crp, crpl, ind)
+        want = np.zeros((nt, ng))
+        src = obs if F1 else pred
+        rs = int(refsx[is_ - 1])
+        sides = []
+        if is_ <= ns - m // M - round(w / M):
+            cols = np.arange(rs + m, min(m + offset - 1 + rs, ng) + 1)
+            sides.append((cols, (m + np.arange(cols.size)) * dg, cr0, crp))
+        if is_ > round(w / M) + m // M + 1:
+            cols = np.arange(max(rs - offset - m, 0) + 1, rs - m + 1)
+            sides.append((cols, (m + np.arange(cols.size)[::-1]) * dg, cr0l, crpl))
+        for cols, y, c0, cp in sides:
+            dk = np.zeros(win)
+            dk[ind - 1:ind - 1 + npair] = fre * (c0 - cp) / (c0 * cp)
+            for j, c in enumerate(cols):
+                th = dk * y[j]
+                fac = -1j * th / (2 * np.pi) * (np.exp(-1j * th) if F1 else 1)
+                xp = np.zeros(ntpad)
+                xp[:nt] = src[:, c - 1]
+                want[:, c - 1] = O.wd_direct(xp, 1, fac, ntpad)[:nt]
+        assert np.abs(want).max() > 0
+        np.testing.assert_allclose(got, want, rtol=0, atol=1e-12 * np.abs(want).max())
+        if is_ == 1:  # no left side for the first shots
+            assert not np.any(got[:, :rs - 1])

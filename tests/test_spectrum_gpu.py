@@ -129,3 +129,31 @@ def test_adwdgrad_matches_oracle(O, survey, shots):
         assert np.abs(ref).max() > 0
         assert _rel(got, ref) < 1e-9, is_
         assert np.array_equal(np.abs(got).sum(0) > 0, np.abs(ref).sum(0) > 0)
+
+
+@pytest.mark.parametrize("survey,shots", [("tiny", [1, 2, 3]), ("plain", [1, 6, 12])])
+def test_adwdgrad_norm_matches_oracle(O, survey, shots):
+    """ADWDgrad_norm: the SoftMax weights replaced by normpdf around the picks."""
+    s = configs.tiny(nt=400) if survey == "tiny" else configs.plain_c1()
+    rng = np.random.default_rng(8)
+    for is_ in shots:
+        seis = _seis(O, s, is_)
+        saves = {}
+        for side in ("r", "l"):
+            saves[side] = O.radon(seis, is_, s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.ng, s.ds, s.offset, s.m,
+                                  s.M, side, s.dv)[2]
+        npair = saves["r"]["nf"] - saves["r"]["lf"] + 1
+        npv = saves["r"]["ml_raw"].shape[0]
+        gr = rng.integers(-3, 4, npair).astype(float)
+        gl = rng.integers(-3, 4, npair).astype(float)
+        cr_r = rng.integers(1, npv, npair).astype(float)
+        cr_l = rng.integers(1, npv, npair).astype(float) + 0.5  # interpolated picks are not integers
+        ref = O.ADWDgrad_norm(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl, saves["r"],
+                              saves["l"], cr_r, cr_l)
+        p = SP.radon_params(s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.nt, s.ng, s.ds, s.offset, s.m, s.M, s.dv)
+        gs = {"r": {"mm": saves["r"]["mm"], "mlr": saves["r"]["ml_raw"], "params": p, "cr_r": cr_r},
+              "l": {"mm": saves["l"]["mm"], "mll": saves["l"]["ml_raw"], "params": p, "cr_l": cr_l}}
+        got = SP.ADWDgrad_norm(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl, None, gs["r"],
+                               gs["l"])
+        assert np.abs(ref).max() > 0
+        assert _rel(got, ref) < 1e-9, is_
