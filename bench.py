@@ -61,6 +61,8 @@ def parse():
     p.add_argument("--cells", type=int, default=0)
     p.add_argument("--ring", type=int, default=0)
     p.add_argument("--chunk", type=int, default=0)
+    p.add_argument("--sched", type=int, default=-1,
+                   help="FD schedule: 0 two barriers per row, 1 one barrier, 2 warp streaming (-1: autotuned)")
     p.add_argument("--serve", type=int, default=0,
                    help="served request stream: number of requests (0: run the gradient bench instead)")
     p.add_argument("--rate", type=float, default=2.0, help="served stream: Poisson arrival rate, requests/s")
@@ -477,10 +479,11 @@ def main():
     s = survey(args)
     # this rank's share of the survey's shots (all of them at N=1)
     # the engine times its FD kernel variants on this survey unless a shape is given
-    tune = not (args.warps or args.cells or args.ring or args.chunk)
+    tune = not (args.warps or args.cells or args.ring or args.chunk or args.sched >= 0)
     sg = ShardedGradient(s, world, rank, device=local, snapshot_mode=args.snapshot_mode,
                          ckpt_interval=args.ckpt, warps=args.warps, cells=args.cells, ring_fwd=args.ring,
-                         ring_adj=args.ring, chunk_rows=args.chunk, autotune=tune)
+                         ring_adj=args.ring, chunk_rows=args.chunk, autotune=tune,
+                         fd_schedule=max(args.sched, 0))
     eng = sg.engine
     info = eng.info
     # observed curves of the "true" model (setup, SWD.m:155-162), then resident inputs
@@ -594,7 +597,8 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model + Gaussian anomaly)",
             "config": workload_config(s, {"adjoint": {1: "stored strain snapshots", 2: "checkpoint+recompute"}[
                 info["mode"]], "batch": info["batch"], "engine_bytes": info["bytes"],
-                "fd_variant": {k: info[k] for k in ("warps", "cells", "ring_fwd", "ring_adj", "chunk_rows")} |
+                "fd_variant": {k: info[k] for k in ("fd_schedule", "warps", "cells", "ring_fwd", "ring_adj",
+                                                    "chunk_rows")} |
                 {"autotuned": tune},
                 "parallelism": f"{s.ns} shots split round-robin over {world} GPU(s), one FP64 all-reduce of "
                                f"the shot sums per step", "shots_this_rank": nloc}),

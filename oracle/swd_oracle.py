@@ -636,6 +636,8 @@ def weight_data_muti3(seismo_v_d, seismo_v, is_, dt, df, offset, dg, F1, w, M, m
     fre = 2 * np.pi * mlinspace(fmin, fmax, (fmax - fmin) / df + 1)  # :4
     npair = fre.size
     ntpad = int(math.floor(1 / dt / df))                               # :10
+    if ind != math.floor(ind) or win != math.floor(win):
+        raise ValueError("ind and win must be integers (they index deta_cc2)")
     ind, win = int(ind), int(win)
     if nt > ntpad or 2 * win >= ntpad or ind < 1 or ind + npair - 1 > win:
         raise ValueError("weight_data_muti3 needs nt <= ntpad, 2*win < ntpad and ind+npair-1 <= win")

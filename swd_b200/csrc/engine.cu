@@ -438,6 +438,49 @@ static int autotune(swd_engine* e) {
     }
     if (rc != SWD_OK) break;
   }
+  // warp-streaming schedule (no shared memory): warps per CTA and chunk height
+  if (rc == SWD_OK) {
+    FdGeom hw = base;
+    hw.sched = 2;
+    hw.warps = 4;
+    plan_decomposition(hw, e->B, 0);
+    std::vector<int> wch = {hw.chunk, std::max(8, hw.chunk * 2 / 3), std::min(rows, hw.chunk * 3 / 2)};
+    std::sort(wch.begin(), wch.end());
+    wch.erase(std::unique(wch.begin(), wch.end()), wch.end());
+    for (int nw : {4, 2, 8}) {
+      for (int ch : wch) {
+        double bf = 1e30, ba = 1e30;
+        int rf = 4, ra = 4;
+        for (int slots : {4, 6, 8}) {
+          if (slots == 8 && nw == 8) continue;
+          FdGeom gc = base;
+          gc.nrec = snap_nrec;
+          gc.sched = 2;
+          gc.warps = nw;
+          gc.ring_fwd = gc.ring_adj = slots;
+          plan_decomposition(gc, e->B, ch);
+          float mf = 0, ma = 0;
+          if ((rc = time_steps(gc, true, &mf)) != SWD_OK) break;
+          if ((rc = time_steps(gc, false, &ma)) != SWD_OK) break;
+          if (mf < bf) { bf = mf; rf = slots; }
+          if (ma < ba) { ba = ma; ra = slots; }
+        }
+        if (rc != SWD_OK) break;
+        if (bf + ba < best) {
+          best = bf + ba;
+          pick = base;
+          pick.sched = 2;
+          pick.warps = nw;
+          pick.ring_fwd = rf;
+          pick.ring_adj = ra;
+          plan_decomposition(pick, e->B, ch);
+          e->tuned_fwd_us = bf * 1e3 / n;
+          e->tuned_adj_us = ba * 1e3 / n;
+        }
+      }
+      if (rc != SWD_OK) break;
+    }
+  }
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   if (rc != SWD_OK) return rc;
@@ -648,7 +691,7 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   g.cells = e->opt.cells;
   g.ring_fwd = e->opt.ring_fwd;
   g.ring_adj = e->opt.ring_adj;
-  g.sched = e->opt.fd_schedule == 1 ? 1 : 0;
+  g.sched = (e->opt.fd_schedule == 1 || e->opt.fd_schedule == 2) ? e->opt.fd_schedule : 0;
   plan_decomposition(g, std::max(1, std::min(e->opt.max_batch > 0 ? e->opt.max_batch : e->ns, e->ns)),
                      e->opt.chunk_rows);
   // Radon geometry

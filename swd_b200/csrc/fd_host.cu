@@ -9,6 +9,7 @@
 #include "fd_host.cuh"
 #include "fd_kernels.cuh"
 #include "fd_lead.cuh"
+#include "fd_warp.cuh"
 
 namespace swd {
 
@@ -121,6 +122,26 @@ bool fd_lead_built(int w, int c, int d) {
 
 void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
   const int rows = g.NZ - 2;
+  if (g.sched == 2) {  // warp streaming (fd_warp.cuh): 30 output columns per warp, warps per CTA 2, 4 or 8,
+                       // 4, 6 or 8 register row slots (ring_fwd / ring_adj)
+    if (g.warps != 2 && g.warps != 8) g.warps = 4;
+    g.cells = 1;
+    if (g.ring_fwd != 6 && !(g.ring_fwd == 8 && g.warps != 8)) g.ring_fwd = 4;
+    if (g.ring_adj != 6 && !(g.ring_adj == 8 && g.warps != 8)) g.ring_adj = 4;
+    g.n_strips = (g.NX - 2 + kWarpOut - 1) / kWarpOut;
+    if (chunk_rows <= 0) {
+      // about 5 waves of warps (148 SMs x 28 resident warps): short chunks keep more rows in
+      // flight and every SM busy through the tail of a step; 96 shots of 132 x 660 -> 11 rows
+      const long target = 148L * 28 * 5;
+      const long per = (long)g.n_strips * n_shots;
+      int nch = (int)((target + per - 1) / per);
+      nch = std::max(1, std::min(nch, std::max(1, rows / 8)));
+      chunk_rows = (rows + nch - 1) / nch;
+    }
+    g.chunk = std::max(1, std::min(chunk_rows, rows));
+    g.n_chunks = (rows + g.chunk - 1) / g.chunk;
+    return;
+  }
   if (!fd_variant_built(g.warps, g.cells, 4)) { g.warps = 3; g.cells = 1; }
   if (!fd_variant_built(g.warps, g.cells, g.ring_fwd)) g.ring_fwd = 4;
   if (!fd_variant_built(g.warps, g.cells, g.ring_adj)) g.ring_adj = 4;
@@ -190,6 +211,34 @@ static int adj_lead_impl(const AdjArgs<T>& a, int it, cudaStream_t st) {
   return SWD_OK;
 }
 
+template <int NW, int NS, bool SNAP>
+static int fwd_warp_launch(const FwdArgs<float>& a, int it, cudaStream_t st) {
+  constexpr size_t smem = warp_smem_bytes<NW, NS>();
+  static int ready = set_smem(fd_fwd_warp<NW, NS, SNAP>, smem);
+  if (ready != SWD_OK) return ready;
+  const long warps = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
+  fd_fwd_warp<NW, NS, SNAP><<<(unsigned)((warps + NW - 1) / NW), 32 * NW, smem, st>>>(a, it);
+  count_launch(1);
+  return SWD_OK;
+}
+template <int NW, int NS>
+static int fwd_warp_impl(const FwdArgs<float>& a, int it, cudaStream_t st) {
+  if (a.snap && it % a.g.nt_wf == 0) return fwd_warp_launch<NW, NS, true>(a, it, st);
+  return fwd_warp_launch<NW, NS, false>(a, it, st);
+}
+template <int NW, int NS, bool IMG>
+static int adj_warp_impl(const AdjArgs<float>& a, int it, cudaStream_t st) {
+  constexpr size_t smem = warp_smem_bytes<NW, NS>();
+  static int ready = set_smem(fd_adj_warp<NW, NS, IMG>, smem);
+  if (ready != SWD_OK) return ready;
+  const long warps = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
+  fd_adj_warp<NW, NS, IMG><<<(unsigned)((warps + NW - 1) / NW), 32 * NW, smem, st>>>(a, it);
+  count_launch(1);
+  return SWD_OK;
+}
+// (warps per CTA, row slots) of the warp-streaming kernels
+#define SWD_WARP_SHAPES(X) X(2, 4) X(4, 4) X(8, 4) X(2, 6) X(4, 6) X(8, 6) X(4, 8) X(2, 8)
+
 template <typename T, int NF, int W, int C, int D, bool GB, bool IMG>
 static int adj_impl(const AdjArgs<T>& a, int it, cudaStream_t st) {
   constexpr size_t smem = smem_bytes<T, W, C, D, GB>();
@@ -207,6 +256,16 @@ template <typename T, int NF>
 int launch_fwd_step(const FwdArgs<T>& a, int it, cudaStream_t st) {
   if (a.mb) return fwd_impl<T, NF, 4, 1, 4, true>(a, it, st);
   if constexpr (NF == 3 && sizeof(T) == 4) {
+    if (a.g.sched == 2) {
+      switch (a.g.warps * 10 + a.g.ring_fwd) {
+#define X(w, s) case w * 10 + s: return fwd_warp_impl<w, s>(a, it, st);
+        SWD_WARP_SHAPES(X)
+#undef X
+        default: break;
+      }
+      set_error("internal: unsupported FD kernel variant");
+      return SWD_ERR_INVALID;
+    }
     const int key = a.g.warps * 100 + a.g.cells * 10 + a.g.ring_fwd;
     if (a.g.sched == 1) {
       switch (key) {
@@ -233,6 +292,16 @@ template <typename T, int NF, bool IMG>
 static int adj_dispatch(const AdjArgs<T>& a, int it, cudaStream_t st) {
   if (a.mb) return adj_impl<T, NF, 4, 1, 4, true, IMG>(a, it, st);
   if constexpr (NF == 3 && sizeof(T) == 4) {
+    if (a.g.sched == 2) {
+      switch (a.g.warps * 10 + a.g.ring_adj) {
+#define X(w, s) case w * 10 + s: return adj_warp_impl<w, s, IMG>(a, it, st);
+        SWD_WARP_SHAPES(X)
+#undef X
+        default: break;
+      }
+      set_error("internal: unsupported FD kernel variant");
+      return SWD_ERR_INVALID;
+    }
     const int key = a.g.warps * 100 + a.g.cells * 10 + a.g.ring_adj;
     if (a.g.sched == 1) {
       switch (key) {

@@ -33,7 +33,8 @@ struct FdGeom {
   int warps;                 // warps per CTA
   int cells;                 // output columns per thread; a CTA owns 32*warps*cells columns
   int ring_fwd, ring_adj;    // rows in the shared-memory ring of the forward / adjoint kernels (4, 6, 8)
-  int sched;                 // 0: two barriers per row (fd_smem.cuh); 1: one, velocities a row ahead (fd_lead.cuh)
+  int sched;                 // 0: two barriers per row (fd_smem.cuh); 1: one, velocities a row ahead (fd_lead.cuh);
+                             // 2: warp streaming, no shared memory (fd_warp.cuh; warps = warps per CTA)
   size_t field;              // NZ * pitch
 };
 

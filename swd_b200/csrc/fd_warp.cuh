@@ -1,0 +1,396 @@
+// Warp-streaming FD time steps (engine path: FP32, b/b1 from the row index, 3 snapshot fields).
+//
+// Each warp owns a strip of 32 columns x = xs-1 .. xs+30 of one shot and streams down a
+// chunk of rows, one column per lane.  Horizontal neighbours come from the adjacent lanes
+// through warp shuffles.  The step at a column depends on the columns next to it only, so
+// lanes 1..30 produce the strip's 30 outputs and lanes 0 and 31 are halo lanes that compute
+// values for their neighbours and write nothing.  Vertical neighbours stay in registers:
+// rows k and k+1 are held by each lane.  The rows ahead are staged by cp.async into NS
+// shared-memory slots per warp, each lane copying and later reading only its own column, so
+// no barrier of any kind is needed and the rows in flight cost no registers: rows k+2 ..
+// k+NS-1 are outstanding while row k is computed.  The state of a shot is stored
+// cell-interleaved for this schedule: float4 {uu, ww, xx, zz} [NZ][pitch] followed by
+// xz [NZ][pitch] (the same 5*NZ*pitch floats as the other schedules), so a row costs a lane
+// three 16/4-byte copies and two stores.  The arithmetic is that of fd_smem.cuh, expression
+// for expression (the file is compiled with -fmad=false), so the results are bit-identical.
+//
+// Reference loops:  core/eigen_staggerfd_single.cpp:207-357 (forward),
+//                   core/eigen_e2drtm_single.cpp:181-283 (adjoint + imaging).
+#pragma once
+#include <type_traits>
+
+#include "fd_kernels.cuh"
+
+namespace swd {
+
+constexpr int kWarpOut = 30;  // output columns per warp (32 lanes minus two halo lanes)
+
+__device__ __forceinline__ float shfl_l(float v) { return __shfl_up_sync(kFull, v, 1); }   // value at x-1
+__device__ __forceinline__ float shfl_r(float v) { return __shfl_down_sync(kFull, v, 1); } // value at x+1
+
+// One padded row of a lane's column: the five state fields and {temp, ca, cl, cm1}.
+struct WRow {
+  float uu, ww, xx, zz, xz;
+  float4 m;
+};
+
+// A staging slot: one row of a warp's 32 columns.
+struct WSlot {
+  float4 q[32];   // {uu, ww, xx, zz}
+  float4 m[32];   // {temp, ca, cl, cm1}
+  float xz[32];
+};
+
+template <int NW, int NS>
+constexpr size_t warp_smem_bytes() { return (size_t)NW * NS * sizeof(WSlot); }
+
+__device__ __forceinline__ void wcp16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src) : "memory");
+}
+__device__ __forceinline__ void wcp4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src) : "memory");
+}
+__device__ __forceinline__ void wcp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void wcp_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+struct WStage {
+  const float4* q;    // this lane's column of {uu, ww, xx, zz}, row 0
+  const float* xz;    // this lane's column of xz, row 0
+  const float4* mat;  // this lane's column of the materials, row 0
+  WSlot* slots;       // this warp's NS slots
+  int pitch, zmax, lane;
+  // Stage row z into a slot (rows beyond zmax are not needed: an empty copy group keeps the
+  // group count).  Lanes past the last column copy the last column instead: their values only
+  // reach border columns, which are never updated or written.
+  __device__ __forceinline__ void issue(int slot, int z) const {
+    if (z <= zmax) {
+      const size_t o = (size_t)z * pitch;
+      WSlot& s = slots[slot];
+      wcp16(&s.q[lane], q + o);
+      wcp16(&s.m[lane], mat + o);
+      wcp4(&s.xz[lane], xz + o);
+    }
+    wcp_commit();
+  }
+  __device__ __forceinline__ void read(WRow& r, int slot) const {
+    const WSlot& s = slots[slot];
+    const float4 v = s.q[lane];
+    r.uu = v.x;
+    r.ww = v.y;
+    r.xx = v.z;
+    r.zz = v.w;
+    r.xz = s.xz[lane];
+    r.m = s.m[lane];
+  }
+};
+
+// Map a warp of the launch to (strip, chunk, shot); false for the padding warps of the last CTA.
+__device__ __forceinline__ bool warp_tile(const FdGeom& g, int n_shots, int NW, int& strip, int& chunk, int& shot) {
+  const long wid = (long)blockIdx.x * NW + (threadIdx.x >> 5);
+  if (wid >= (long)g.n_strips * g.n_chunks * n_shots) return false;
+  strip = (int)(wid % g.n_strips);
+  const long rest = wid / g.n_strips;
+  chunk = (int)(rest % g.n_chunks);
+  shot = (int)(rest / g.n_chunks);
+  return true;
+}
+
+// ---------------------------------------------------------------- forward
+
+template <int NW, int NS, bool SNAP>
+__global__ void __launch_bounds__(32 * NW) fd_fwd_warp(FwdArgs<float> a, int it) {
+  static_assert(NS >= 4 && NS % 2 == 0, "rows k, k+1 in use, at least two in flight; even for the unrolled rotation");
+  using T = float;
+  const FdGeom& g = a.g;
+  int strip, chunk, shot;
+  if (!warp_tile(g, a.n_shots, NW, strip, chunk, shot)) return;  // whole warps only
+  const int lane = threadIdx.x & 31;
+  const int x = kWarpOut * strip + lane;
+  const int zs = 1 + chunk * g.chunk;
+  const int ze = min(zs + g.chunk, g.NZ - 1);
+  const size_t F = g.field;
+  const bool xin = x < g.NX;
+  const bool xint = x >= 1 && x <= g.NX - 2;
+  const bool own = xint && lane >= 1 && lane <= kWarpOut;
+  const int xc = xin ? x : g.NX - 1;
+  const float* sb = a.in + (size_t)shot * 5 * F;
+  extern __shared__ __align__(16) unsigned char wsmem[];
+  const WStage ld{reinterpret_cast<const float4*>(sb) + xc, sb + 4 * F + xc, a.mat + xc,
+                  reinterpret_cast<WSlot*>(wsmem) + (threadIdx.x >> 5) * NS, g.pitch, ze, lane};
+  float* obs = a.out + (size_t)shot * 5 * F;
+  float4* oq = reinterpret_cast<float4*>(obs) + xc;
+  float* oxz = obs + 4 * F + xc;
+  const int st = a.src_type;
+  const int2 sp = a.src[shot];
+  const T sv = a.s[it];
+  const T dtx = a.dtx;
+  const bool sc = x == sp.y, sr = x == sp.y + 1;
+  const bool s_w = sc && st != 1 && st != 4;    // ww(sz,sx) = s (type 5) or += s (types 2, 3)
+  const bool s_wr = sr && st == 2;              // ww(sz,sx+1) += s
+  const bool s_u = sc && (st == 2 || st == 3);  // uu(sz,sx) += s
+  const bool s_um = sc && st == 2;              // uu(sz-1,sx) -= s
+  const bool s_xz = sc && (st == 1 || st == 4); // xx/zz sources before the stress update
+  const int recj = (a.seis_w != nullptr && own && x >= g.gx && (x - g.gx) % g.dg == 0 && (x - g.gx) / g.dg < g.ng)
+                       ? (x - g.gx) / g.dg : -1;
+  const int z_img0 = g.pad_top + 1, z_img1 = g.pad_top + 1 + g.nz;
+  const size_t plane = (size_t)g.nz * g.nx;
+  const bool snapc = SNAP && own && x >= g.nbc && x < g.nbc + g.nx;
+  T* snap_base = SNAP ? a.snap + ((size_t)shot * g.nrec + (it / g.nt_wf - a.rec0)) * 3 * plane : nullptr;
+  auto bz = [&](int z) -> T { return z == g.pad_top ? T(2) * dtx : dtx; };  // b = b1 = dtx, doubled at the surface
+  auto vel_w = [&](bool inner, T ww, T xz, T xzl, T zz, T zzd, T te, T b1) -> T {
+    return inner ? te * ww + b1 * (((xz - xzl) + zzd) - zz) : ww;
+  };
+  auto vel_u = [&](bool inner, T uu, T xx, T xxr, T xz, T xzu, T te, T b) -> T {
+    return inner ? te * uu + b * (((xxr - xx) + xz) - xzu) : uu;
+  };
+  auto src_w = [&](int z, T r) -> T {
+    if (z == sp.x) {
+      if (s_w) r = (st == 5) ? sv : r + sv;
+      else if (s_wr) r = r + sv;
+    }
+    return r;
+  };
+  auto src_u = [&](int z, T r) -> T {
+    if (s_u && z == sp.x) r = r + sv;
+    if (s_um && z == sp.x - 1) r = r - sv;
+    return r;
+  };
+
+  // Row r is staged in slot (r - zs + 1) % NS; rows k and k+1 are held in the registers RR[0] /
+  // RR[1], alternating; the row loop is unrolled by NS so that slots and registers rotate
+  // without moves.
+#pragma unroll
+  for (int u = 0; u < NS; ++u) ld.issue(u, zs - 1 + u);
+  wcp_wait<NS - 2>();
+  WRow RR[2];
+  ld.read(RR[0], 0);
+  ld.read(RR[1], 1);
+  // prologue: new ww at row zs-1 and new uu at row zs
+  T wn_prev, un_cur;
+  {
+    const WRow& A = RR[0];
+    const WRow& B = RR[1];
+    const T xzl = shfl_l(A.xz);
+    wn_prev = src_w(zs - 1, vel_w(xint && zs - 1 >= 1, A.ww, A.xz, xzl, A.zz, B.zz, A.m.x, bz(zs - 1)));
+    const T xxr = shfl_r(B.xx);
+    un_cur = src_u(zs, vel_u(xint, B.uu, B.xx, xxr, B.xz, A.xz, B.m.x, bz(zs)));
+  }
+  // One row k: R0 = row k (registers), R1 receives row k+1 from slot s1, row k+NS-1 is staged
+  // into slot sp (row k-1's).  SLOW rows are those where a source, the receivers, the free
+  // surface or the bottom row need their checks; every other row takes the check-free path.
+  auto step = [&](auto slow_tag, const WRow& R0, WRow& R1, int s1, int spf, int k) {
+    constexpr bool SLOW = decltype(slow_tag)::value;
+    ld.issue(spf, k + NS - 1);
+    wcp_wait<NS - 2>();  // row k+1 has landed
+    ld.read(R1, s1);
+    const bool inner1 = !SLOW || k + 1 <= g.NZ - 2;
+    // velocities: ww at row k, uu at row k+1 (:224-228, source :286-300)
+    const T xzl = shfl_l(R0.xz);
+    T wn = vel_w(xint, R0.ww, R0.xz, xzl, R0.zz, R1.zz, R0.m.x, SLOW ? bz(k) : dtx);
+    const T xxr = shfl_r(R1.xx);
+    T un_next = vel_u(xint && inner1, R1.uu, R1.xx, xxr, R1.xz, R0.xz, R1.m.x, SLOW ? bz(k + 1) : dtx);
+    if (SLOW) {
+      wn = src_w(k, wn);
+      un_next = src_u(k + 1, un_next);
+    }
+    // strains at row k (:302-306)
+    const T ucl = shfl_l(un_cur);
+    const T wnr = shfl_r(wn);
+    const T fux = un_cur - ucl;
+    const T fuz = un_next - un_cur;
+    const T bwx = wnr - wn;
+    const T bwz = wn - wn_prev;
+    // stresses at row k (:334-336), source types 1/4 first (:286-298), free surface (:340)
+    T xo = R0.xx, zo = R0.zz;
+    if (SLOW && s_xz && k == sp.x) {
+      if (st == 1) { xo = xo + sv; zo = zo + sv; }
+      else { zo = zo + sv; }
+    }
+    const T te = R0.m.x, ca = R0.m.y, cl = R0.m.z, cm1 = R0.m.w;
+    const T xxn = te * xo + (ca * fux + cl * bwz) * dtx;
+    T zzn = te * zo + (ca * bwz + cl * fux) * dtx;
+    const T xzn = te * R0.xz + (cm1 * (fuz + bwx)) * dtx;
+    if (SLOW && k == g.pad_top) zzn = T(0);
+    if (own) {
+      const size_t o = (size_t)k * g.pitch;
+      oq[o] = make_float4(un_cur, wn, xxn, zzn);
+      oxz[o] = xzn;
+    }
+    if (SLOW && recj >= 0 && k == g.gz) {  // :342-345
+      const size_t r = ((size_t)shot * g.nt + it) * g.ng + recj;
+      a.seis_w[r] = wn;
+      if (a.seis_u) a.seis_u[r] = un_cur;
+    }
+    if (SNAP && snapc && k >= z_img0 && k < z_img1) {  // :346-351 (the adjoint needs fux, bwz, fuz+bwx)
+      T* s0 = snap_base + ((size_t)(k - z_img0) * g.nx + (x - g.nbc));
+      s0[0] = fux;
+      s0[plane] = bwz;
+      s0[2 * plane] = fuz + bwx;
+    }
+    wn_prev = wn;
+    un_cur = un_next;
+  };
+  auto row = [&](const WRow& R0, WRow& R1, int s1, int spf, int k) {
+    if (k == g.pad_top || k == g.gz || k == g.NZ - 2 || (k >= sp.x - 2 && k <= sp.x))
+      step(std::true_type{}, R0, R1, s1, spf, k);
+    else
+      step(std::false_type{}, R0, R1, s1, spf, k);
+  };
+  // row k = zs + u (mod NS): in RR[(u + 1) & 1], row k+1 goes to RR[u & 1] from slot (u + 2) % NS
+  int k = zs;
+  for (; k + NS <= ze; k += NS) {
+#pragma unroll
+    for (int u = 0; u < NS; ++u) row(RR[(u + 1) & 1], RR[u & 1], (u + 2) % NS, u, k + u);
+  }
+#pragma unroll
+  for (int u = 0; u < NS - 1; ++u)
+    if (k + u < ze) row(RR[(u + 1) & 1], RR[u & 1], (u + 2) % NS, u, k + u);
+  wcp_wait<0>();  // no copy may still target this warp's slots at exit
+}
+
+// ---------------------------------------------------------------- adjoint
+
+template <int NW, int NS, bool IMG>
+__global__ void __launch_bounds__(32 * NW) fd_adj_warp(AdjArgs<float> a, int it) {
+  static_assert(NS >= 4 && NS % 2 == 0, "rows k, k+1 in use, at least two in flight; even for the unrolled rotation");
+  using T = float;
+  const FdGeom& g = a.g;
+  int strip, chunk, shot;
+  if (!warp_tile(g, a.n_shots, NW, strip, chunk, shot)) return;
+  const int lane = threadIdx.x & 31;
+  const int x = kWarpOut * strip + lane;
+  const int zs = 1 + chunk * g.chunk;
+  const int ze = min(zs + g.chunk, g.NZ - 1);
+  const size_t F = g.field;
+  const bool xin = x < g.NX;
+  const bool xint = x >= 1 && x <= g.NX - 2;
+  const bool own = xint && lane >= 1 && lane <= kWarpOut;
+  const int xc = xin ? x : g.NX - 1;
+  const float* sb = a.in + (size_t)shot * 5 * F;
+  extern __shared__ __align__(16) unsigned char wsmem[];
+  const WStage ld{reinterpret_cast<const float4*>(sb) + xc, sb + 4 * F + xc, a.mat + xc,
+                  reinterpret_cast<WSlot*>(wsmem) + (threadIdx.x >> 5) * NS, g.pitch, ze, lane};
+  float* obs = a.out + (size_t)shot * 5 * F;
+  float4* oq = reinterpret_cast<float4*>(obs) + xc;
+  float* oxz = obs + 4 * F + xc;
+  const T dtx = a.dtx;
+  // dt*res at receiver columns (:238-242); halo lanes inject too, their ww feeds the neighbours
+  const bool rec = xin && x >= g.gx && (x - g.gx) % g.dg == 0 && (x - g.gx) / g.dg < g.ng;
+  const T inj = rec ? a.dt * a.res[((size_t)shot * g.nt + it) * g.ng + (x - g.gx) / g.dg] : T(0);
+  const int z_img0 = g.pad_top + 1, z_img1 = g.pad_top + 1 + g.nz;
+  const size_t plane = (size_t)g.nz * g.nx;
+  const bool ximg = own && x >= g.nbc && x < g.nbc + g.nx;
+  const T* snap_b = IMG ? a.snap + ((size_t)shot * g.nrec + (it / g.nt_wf - a.rec0)) * 3 * plane : nullptr;
+  double* img_b = a.img + (size_t)shot * 3 * plane;
+  auto bz = [&](int z) -> T { return z == g.pad_top ? T(2) * dtx : dtx; };
+  // material*stress products of a row: ca*xx, cl*zz, cm1*xz, cl*xx, ca*zz
+  struct Prod { T p1, p2, p3, q1, q2; };
+  auto prod = [](const WRow& r) -> Prod {
+    return Prod{r.m.y * r.xx, r.m.z * r.zz, r.m.w * r.xz, r.m.z * r.xx, r.m.y * r.zz};
+  };
+  struct Img { T fx, bz, sg; double c0, c1, c2; };
+  auto load_img = [&](Img& m, int z) {
+    if (IMG && ximg && z >= z_img0 && z < z_img1 && z < ze) {
+      const size_t cell = (size_t)(z - z_img0) * g.nx + (x - g.nbc);
+      const T* s0 = snap_b + cell;
+      m.fx = s0[0]; m.bz = s0[plane]; m.sg = s0[2 * plane];
+      m.c0 = img_b[cell]; m.c1 = img_b[plane + cell]; m.c2 = img_b[2 * plane + cell];
+    }
+  };
+  // new ww at row k (rows r0 = k, r1 = k+1, products q0 / q1, p3 of row k at x+1)
+  auto vel_w = [&](bool inner, const WRow& r0, const Prod& q0, const Prod& q1, T p3r, int k) -> T {
+    T r = adj_vel_w(inner, r0.ww, q1.q1, q0.q1, q1.q2, q0.q2, p3r, q0.p3, r0.m.x, bz(k));
+    if (rec && k == g.gz) r = r + inj;
+    return r;
+  };
+
+#pragma unroll
+  for (int u = 0; u < NS; ++u) ld.issue(u, zs - 1 + u);
+  wcp_wait<NS - 2>();
+  WRow RR[2];
+  ld.read(RR[0], 0);
+  ld.read(RR[1], 1);
+  Prod QP[2] = {prod(RR[0]), prod(RR[1])};  // products of rows k and k+1
+  Img IM[2] = {};                           // imaging operands of rows k and k+1
+  load_img(IM[0], zs);
+  T wn_prev, un_cur;
+  {
+    const WRow& A = RR[0];
+    const WRow& B = RR[1];
+    wn_prev = vel_w(xint && zs - 1 >= 1, A, QP[0], QP[1], shfl_r(QP[0].p3), zs - 1);
+    const T p1l = shfl_l(QP[1].p1), p2l = shfl_l(QP[1].p2);
+    un_cur = adj_vel_u(xint, B.uu, QP[1].p1, p1l, QP[1].p2, p2l, QP[1].p3, QP[0].p3, B.m.x, bz(zs));
+  }
+  // One row k: R0 = row k with products Q0, R1 receives row k+1 from slot s1 and its products
+  // go to Q1, row k+NS-1 is staged into slot spf; im_c holds row k's imaging operands, im_n
+  // receives row k+1's.
+  auto step = [&](auto slow_tag, const WRow& R0, WRow& R1, int s1, int spf, const Prod& Q0, Prod& Q1,
+                  const Img& im_c, Img& im_n, int k) {
+    constexpr bool SLOW = decltype(slow_tag)::value;
+    ld.issue(spf, k + NS - 1);
+    load_img(im_n, k + 1);
+    wcp_wait<NS - 2>();  // row k+1 has landed
+    ld.read(R1, s1);
+    const bool inner1 = !SLOW || k + 1 <= g.NZ - 2;
+    Q1 = prod(R1);
+    // velocities: ww at row k, uu at row k+1 (:182-187), injection (:238-242)
+    T wn = adj_vel_w(xint, R0.ww, Q1.q1, Q0.q1, Q1.q2, Q0.q2, shfl_r(Q0.p3), Q0.p3, R0.m.x, SLOW ? bz(k) : dtx);
+    if (SLOW && rec && k == g.gz) wn = wn + inj;
+    const T p1l = shfl_l(Q1.p1), p2l = shfl_l(Q1.p2);
+    const T un_next = adj_vel_u(xint && inner1, R1.uu, Q1.p1, p1l, Q1.p2, p2l, Q1.p3, Q0.p3, R1.m.x,
+                                SLOW ? bz(k + 1) : dtx);
+    // adjoint stresses at row k (:245-248), free surface (:270)
+    const T un_r = shfl_r(un_cur);
+    const T wn_l = shfl_l(wn);
+    const T te = R0.m.x;
+    const T xxn = te * R0.xx - dtx * (un_r - un_cur);
+    T zzn = te * R0.zz - dtx * (wn - wn_prev);
+    const T xzn = (te * R0.xz - dtx * (un_next - un_cur)) - dtx * (wn - wn_l);
+    if (SLOW && k == g.pad_top) zzn = T(0);
+    if (own) {
+      const size_t o = (size_t)k * g.pitch;
+      oq[o] = make_float4(un_cur, wn, xxn, zzn);
+      oxz[o] = xzn;
+      if (IMG && ximg && k >= z_img0 && k < z_img1) {  // imaging condition (:274-279)
+        const size_t cell = (size_t)(k - z_img0) * g.nx + (x - g.nbc);
+        const T fx = im_c.fx, bzv = im_c.bz, sg = im_c.sg;
+        const T Fs = fx + bzv;
+        const T tcl = Fs * (xxn + zzn);
+        const T tcm = T(2) * ((xxn * fx + zzn * bzv) + T(0.5) * (xzn * sg));
+        const T til = Fs * Fs;
+        img_b[cell] = im_c.c0 + (double)tcl;
+        img_b[plane + cell] = im_c.c1 + (double)tcm;
+        img_b[2 * plane + cell] = im_c.c2 + (double)til;
+      }
+    }
+    wn_prev = wn;
+    un_cur = un_next;
+  };
+  auto row = [&](const WRow& R0, WRow& R1, int s1, int spf, const Prod& Q0, Prod& Q1, const Img& im_c, Img& im_n,
+                 int k) {
+    if (k == g.pad_top || k == g.gz || k == g.NZ - 2)
+      step(std::true_type{}, R0, R1, s1, spf, Q0, Q1, im_c, im_n, k);
+    else
+      step(std::false_type{}, R0, R1, s1, spf, Q0, Q1, im_c, im_n, k);
+  };
+  // unrolled by NS: slots rotate with period NS; rows, products and imaging operands with period 2
+  // (row k = zs + u: registers RR[(u + 1) & 1], products QP[(u + 1) & 1], imaging IM[u & 1])
+  int k = zs;
+  for (; k + NS <= ze; k += NS) {
+#pragma unroll
+    for (int u = 0; u < NS; ++u)
+      row(RR[(u + 1) & 1], RR[u & 1], (u + 2) % NS, u, QP[(u + 1) & 1], QP[u & 1], IM[u & 1], IM[(u + 1) & 1],
+          k + u);
+  }
+#pragma unroll
+  for (int u = 0; u < NS - 1; ++u)
+    if (k + u < ze)
+      row(RR[(u + 1) & 1], RR[u & 1], (u + 2) % NS, u, QP[(u + 1) & 1], QP[u & 1], IM[u & 1], IM[(u + 1) & 1],
+          k + u);
+  wcp_wait<0>();
+}
+
+}  // namespace swd
