@@ -32,9 +32,12 @@ import numpy as np  # noqa: E402
 METRIC = "shot-gradients/s (fwd+adj)"
 UNIT = "shot-gradients/s"
 # DRAM traffic per padded cell and time step of the FD step kernels (plain-step variants, 4 of
-# every 5 launches), from the ncu capture summarised in profiles/fd_step_kernels_batched-100x600.md:
+# every 5 launches) for each FD schedule, from the ncu captures summarised in
+# profiles/fd_step_kernels_batched-100x600.md (schedule 0) and
+# profiles/fd_warp_kernels_batched-100x600.md (schedule 2):
 # (dram__bytes_read.sum + dram__bytes_write.sum) per launch / (96 shots x 132 x 660 cells).
-NCU_BYTES_PER_CELL_STEP = {"fd_fwd_step": 36.1, "fd_adj_step": 36.1}
+NCU_BYTES_PER_CELL_STEP = {0: {"fd_fwd_step": 36.1, "fd_adj_step": 36.1},
+                           2: {"fd_fwd_step": 35.05, "fd_adj_step": 34.99}}
 # Compulsory DRAM bytes of the fused one-sweep kernels: 5 state fields read + 5 written per
 # shot-cell-step (materials are shared by the shots of a launch), plus per interior cell every
 # nt_wf steps the 3-field snapshot write (forward) or snapshot read + FP64 image update (adjoint).
@@ -579,11 +582,11 @@ def main():
 
     def roof(name, nbytes, comp, launch_ms):
         ach = nbytes / (launch_ms / 1e3) / 1e9
-        tr = NCU_BYTES_PER_CELL_STEP.get(name)
+        tr = NCU_BYTES_PER_CELL_STEP.get(info["fd_schedule"], {}).get(name)
         return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                 "fallback 6650 GB/s", "traffic": (tr * cells) if tr else None,
-                "traffic_source": "ncu, plain-step variant" if tr else None,
+                "traffic_source": f"ncu, plain-step variant of FD schedule {info['fd_schedule']}" if tr else None,
                 "algorithmic_bytes_per_launch": nbytes, "avg_launch_ms": launch_ms,
                 "compulsory_bytes_per_launch": comp,
                 "frac_compulsory": comp / (launch_ms / 1e3) / 1e9 / peak}
