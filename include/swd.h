@@ -229,7 +229,8 @@ typedef struct {
                           or SWD_PREC_BF16X2 / _BF16X3 (tcgen05 split-BF16, see swd_contract_*) */
   int fd_schedule;    /* FD kernels: 0 two CTA barriers per row, 1 one barrier with the velocities
                          a row ahead (shapes (2,1), (3,1), (4,1) ring 4, (3,1) ring 6), 2 warp
-                         streaming without shared memory (warps = 2, 4 or 8 per CTA); same bits */
+                         streaming (warps = 2, 4 or 8 per CTA, ring_* = 4, 6 or 8 staged rows),
+                         3 warp streaming with two time steps per launch; same bits */
   int adjoint_weight; /* adjoint source: 0 ADWDgrad_1 (SoftMax weights, SWD.m:190), 1 ADWDgrad_norm
                          (Gaussian weights around the picks, core/ADWDgrad_norm.m), 2 the WD residual
                          weight_data_muti3 with F1 = 0 (SWD.m:188; ind = fmin/df+1, win = npair+2*ind,

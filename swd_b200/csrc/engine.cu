@@ -279,6 +279,25 @@ static AdjArgs<float> adj_args(swd_engine* e, const FdGeom& g, int nb) {
   return a;
 }
 
+// Steps advanced by the forward launch at step it of [.., t1): two when the schedule pairs
+// steps, the pair ends inside the range and does not step over a checkpoint (ckev > 0: the
+// state at multiples of ckev is saved).
+static int fwd_span(const FdGeom& g, int it, int t1, int ckev) {
+  return (fd_pairs(g) && it + 1 < t1 && !(ckev > 0 && (it + 1) % ckev == 0)) ? 2 : 1;
+}
+static uint64_t fwd_launches(const FdGeom& g, int t0, int t1, int ckev) {
+  uint64_t n = 0;
+  for (int it = t0; it < t1; it += fwd_span(g, it, t1, ckev)) ++n;
+  return n;
+}
+// Adjoint steps it, it-1, .. down to t0: two per launch when the schedule pairs them.
+static int adj_span(const FdGeom& g, int it, int t0) { return (fd_pairs(g) && it - 1 >= t0) ? 2 : 1; }
+static uint64_t adj_launches(const FdGeom& g, int hi, int t0) {
+  uint64_t n = 0;
+  for (int it = hi; it >= t0; it -= adj_span(g, it, t0)) ++n;
+  return n;
+}
+
 // Forward of one batch: seismograms always; snapshots (store mode) or checkpoints (mode 2).
 static int forward_batch(swd_engine* e, int bi, int s0, int nb, bool keep_wavefield) {
   const FdGeom& g = e->g;
@@ -288,17 +307,22 @@ static int forward_batch(swd_engine* e, int bi, int s0, int nb, bool keep_wavefi
   const bool store = keep_wavefield && e->mode == 1;
   const bool ck = keep_wavefield && e->mode == 2;
   const long key = ((long)bi << 8) | (store ? 1 : ck ? 2 : 3);
-  return run_seq(e, key, g.nt, [&]() -> int {
+  const int ckev = ck ? e->ckpt : 0;
+  return run_seq(e, key, fwd_launches(g, 0, g.nt, ckev), [&]() -> int {
     FwdArgs<float> a = fwd_args(e, g, s0, nb);
     a.seis_w = e->seis.as<float>();
     a.snap = store ? e->snap.as<float>() : nullptr;
-    for (int it = 0; it < g.nt; ++it) {
+    int c = 0;
+    for (int it = 0; it < g.nt;) {
       if (ck && it % e->ckpt == 0)
-        SWD_CUDA(cudaMemcpyAsync(e->ckbuf.as<float>() + (size_t)(it / e->ckpt) * fieldB, S[it & 1],
+        SWD_CUDA(cudaMemcpyAsync(e->ckbuf.as<float>() + (size_t)(it / e->ckpt) * fieldB, S[c],
                                  (size_t)nb * 5 * g.field * sizeof(float), cudaMemcpyDeviceToDevice, e->st));
-      a.in = S[it & 1];
-      a.out = S[(it + 1) & 1];
-      launch_fwd_step<float, 3>(a, it, e->st);
+      a.in = S[c];
+      a.out = S[c ^ 1];
+      const int n = fwd_span(g, it, g.nt, ckev);
+      SWD_TRY(n == 2 ? launch_fwd_pair(a, it, e->st) : launch_fwd_step<float, 3>(a, it, e->st));
+      c ^= 1;
+      it += n;
     }
     SWD_CUDA(cudaGetLastError());
     return SWD_OK;
@@ -314,15 +338,17 @@ static int adjoint_batch(swd_engine* e, int bi, int s0, int nb) {
   SWD_CUDA(cudaMemsetAsync(e->img.p, 0, (size_t)e->B * 3 * e->plane * sizeof(double), e->st));
   int cur = 0;
   if (e->mode == 1) {
-    return run_seq(e, ((long)bi << 8) | 4, g.nt - 1, [&]() -> int {
+    return run_seq(e, ((long)bi << 8) | 4, adj_launches(g, g.nt - 2, 0), [&]() -> int {
       AdjArgs<float> a = adj_args(e, g, nb);
       a.snap = e->snap.as<float>();
       int c = 0;
-      for (int it = g.nt - 2; it >= 0; --it) {
+      for (int it = g.nt - 2; it >= 0;) {
         a.in = A[c];
         a.out = A[c ^ 1];
-        launch_adj_step<float, 3>(a, it, e->st);
+        const int n = adj_span(g, it, 0);
+        SWD_TRY(n == 2 ? launch_adj_pair(a, it, e->st) : launch_adj_step<float, 3>(a, it, e->st));
         c ^= 1;
+        it -= n;
       }
       SWD_CUDA(cudaGetLastError());
       return SWD_OK;
@@ -333,34 +359,40 @@ static int adjoint_batch(swd_engine* e, int bi, int s0, int nb) {
   for (int k = e->nseg - 1; k >= 0; --k) {
     const int t0 = k * e->ckpt, t1 = std::min(t0 + e->ckpt, g.nt);
     const int a_hi = std::min(t1 - 1, g.nt - 2);
-    const int nfs = t1 - t0, nas = a_hi >= t0 ? a_hi - t0 + 1 : 0;
+    const int nal = a_hi >= t0 ? (int)adj_launches(e->gseg, a_hi, t0) : 0;
     const int cur_in = cur;
     const long key = ((long)bi << 20) | ((long)k << 8) | 5;
-    SWD_TRY(run_seq(e, key, nfs + nas, [&]() -> int {
+    SWD_TRY(run_seq(e, key, fwd_launches(e->gseg, t0, t1, 0) + nal, [&]() -> int {
       SWD_CUDA(cudaMemcpyAsync(F[0], e->ckbuf.as<float>() + (size_t)k * fieldB, (size_t)nb * 5 * g.field * sizeof(float),
                                cudaMemcpyDeviceToDevice, e->st));
       FwdArgs<float> f = fwd_args(e, e->gseg, s0, nb);
       f.snap = e->snap.as<float>();
       f.rec0 = t0 / g.nt_wf;
-      for (int it = t0; it < t1; ++it) {
-        f.in = F[(it - t0) & 1];
-        f.out = F[(it - t0 + 1) & 1];
-        launch_fwd_step<float, 3>(f, it, e->st);
+      int cf = 0;
+      for (int it = t0; it < t1;) {
+        f.in = F[cf];
+        f.out = F[cf ^ 1];
+        const int n = fwd_span(e->gseg, it, t1, 0);
+        SWD_TRY(n == 2 ? launch_fwd_pair(f, it, e->st) : launch_fwd_step<float, 3>(f, it, e->st));
+        cf ^= 1;
+        it += n;
       }
       AdjArgs<float> a = adj_args(e, e->gseg, nb);
       a.snap = e->snap.as<float>();
       a.rec0 = t0 / g.nt_wf;
       int c = cur_in;
-      for (int it = a_hi; it >= t0; --it) {
+      for (int it = a_hi; it >= t0;) {
         a.in = A[c];
         a.out = A[c ^ 1];
-        launch_adj_step<float, 3>(a, it, e->st);
+        const int n = adj_span(e->gseg, it, t0);
+        SWD_TRY(n == 2 ? launch_adj_pair(a, it, e->st) : launch_adj_step<float, 3>(a, it, e->st));
         c ^= 1;
+        it -= n;
       }
       SWD_CUDA(cudaGetLastError());
       return SWD_OK;
     }));
-    cur ^= (nas & 1);
+    cur ^= (nal & 1);
   }
   return SWD_OK;
 }
@@ -394,15 +426,26 @@ static int autotune(swd_engine* e) {
     f.seis_w = e->seis.as<float>();
     AdjArgs<float> a = adj_args(e, gc, e->B);
     a.snap = e->snap.as<float>();
-    for (int i = -2; i < n; ++i) {  // two untimed warm-up launches
+    const bool two = fd_pairs(gc) && n >= 2;
+    const int n2 = two ? n & ~1 : n;  // steps timed
+    for (int i = -2, c = 0; i < n2; i += two ? 2 : 1, c ^= 1) {  // two untimed warm-up launches
       if (i == 0) SWD_CUDA(cudaEventRecord(t0, e->st));
       const int it = std::max(i, 0);
-      if (fwd) { f.in = S[i & 1]; f.out = S[(i + 1) & 1]; SWD_TRY(launch_fwd_step<float, 3>(f, it, e->st)); }
-      else { a.in = S[i & 1]; a.out = S[(i + 1) & 1]; SWD_TRY(launch_adj_step<float, 3>(a, it, e->st)); }
+      if (fwd) {
+        f.in = S[c];
+        f.out = S[c ^ 1];
+        SWD_TRY(two ? launch_fwd_pair(f, it, e->st) : launch_fwd_step<float, 3>(f, it, e->st));
+      } else {
+        a.in = S[c];
+        a.out = S[c ^ 1];
+        // adjoint pairs run steps it+1 and it (both index stored snapshots: it + 1 <= n <= span)
+        SWD_TRY(two ? launch_adj_pair(a, it + 1, e->st) : launch_adj_step<float, 3>(a, it, e->st));
+      }
     }
     SWD_CUDA(cudaEventRecord(t1, e->st));
     SWD_CUDA(cudaEventSynchronize(t1));
     SWD_CUDA(cudaEventElapsedTime(ms, t0, t1));
+    *ms = *ms * (float)n / (float)n2;  // per n steps, as the other variants
     return SWD_OK;
   };
   double best = 1e30;
@@ -444,32 +487,42 @@ static int autotune(swd_engine* e) {
     hw.sched = 2;
     hw.warps = 4;
     plan_decomposition(hw, e->B, 0);
-    std::vector<int> wch = {hw.chunk, std::max(8, hw.chunk * 2 / 3), std::min(rows, hw.chunk * 3 / 2)};
+    // two-step launches recompute two rows per chunk, so they also get chunks twice as long
+    std::vector<int> wch = {hw.chunk, std::max(8, hw.chunk * 2 / 3), std::min(rows, hw.chunk * 3 / 2),
+                            std::min(rows, hw.chunk * 2)};
     std::sort(wch.begin(), wch.end());
     wch.erase(std::unique(wch.begin(), wch.end()), wch.end());
     for (int nw : {4, 2, 8}) {
       for (int ch : wch) {
         double bf = 1e30, ba = 1e30;
-        int rf = 4, ra = 4;
-        for (int slots : {4, 6, 8}) {
-          if (slots == 8 && nw == 8) continue;
-          FdGeom gc = base;
-          gc.nrec = snap_nrec;
-          gc.sched = 2;
-          gc.warps = nw;
-          gc.ring_fwd = gc.ring_adj = slots;
-          plan_decomposition(gc, e->B, ch);
-          float mf = 0, ma = 0;
-          if ((rc = time_steps(gc, true, &mf)) != SWD_OK) break;
-          if ((rc = time_steps(gc, false, &ma)) != SWD_OK) break;
-          if (mf < bf) { bf = mf; rf = slots; }
-          if (ma < ba) { ba = ma; ra = slots; }
+        int rf = 4, ra = 4, pf = 0;
+        for (int pairs : {0, 1}) {  // one or two steps per launch, forward and adjoint alike
+          double pbf = 1e30, pba = 1e30;
+          int prf = 4, pra = 4;
+          for (int slots : {4, 6, 8}) {
+            if (slots == 8 && nw == 8) continue;
+            FdGeom gc = base;
+            gc.nrec = snap_nrec;
+            gc.sched = 2;
+            gc.pairs = pairs;
+            gc.warps = nw;
+            gc.ring_fwd = gc.ring_adj = slots;
+            plan_decomposition(gc, e->B, ch);
+            float mf = 0, ma = 0;
+            if ((rc = time_steps(gc, true, &mf)) != SWD_OK) break;
+            if ((rc = time_steps(gc, false, &ma)) != SWD_OK) break;
+            if (mf < pbf) { pbf = mf; prf = slots; }
+            if (ma < pba) { pba = ma; pra = slots; }
+          }
+          if (rc != SWD_OK) break;
+          if (pbf + pba < bf + ba) { bf = pbf; ba = pba; rf = prf; ra = pra; pf = pairs; }
         }
         if (rc != SWD_OK) break;
         if (bf + ba < best) {
           best = bf + ba;
           pick = base;
           pick.sched = 2;
+          pick.pairs = pf;
           pick.warps = nw;
           pick.ring_fwd = rf;
           pick.ring_adj = ra;
@@ -691,7 +744,9 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   g.cells = e->opt.cells;
   g.ring_fwd = e->opt.ring_fwd;
   g.ring_adj = e->opt.ring_adj;
-  g.sched = (e->opt.fd_schedule == 1 || e->opt.fd_schedule == 2) ? e->opt.fd_schedule : 0;
+  g.sched = (e->opt.fd_schedule == 1 || e->opt.fd_schedule == 2) ? e->opt.fd_schedule
+            : e->opt.fd_schedule == 3 ? 2 : 0;
+  g.pairs = e->opt.fd_schedule == 3 ? 1 : 0;  // warp streaming, two steps per launch
   plan_decomposition(g, std::max(1, std::min(e->opt.max_batch > 0 ? e->opt.max_batch : e->ns, e->ns)),
                      e->opt.chunk_rows);
   // Radon geometry
@@ -829,7 +884,7 @@ static void fill_info(const swd_engine* e, swd_engine_info_t* info) {
   info->ring_adj = e->g.ring_adj;
   info->tuned_fwd_us = e->tuned_fwd_us;
   info->tuned_adj_us = e->tuned_adj_us;
-  info->fd_schedule = e->g.sched;
+  info->fd_schedule = fd_pairs(e->g) ? 3 : e->g.sched;
 }
 
 int swd_engine_info(const swd_engine* e, swd_engine_info_t* info) {

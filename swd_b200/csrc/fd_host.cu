@@ -236,6 +236,42 @@ static int adj_warp_impl(const AdjArgs<float>& a, int it, cudaStream_t st) {
   count_launch(1);
   return SWD_OK;
 }
+template <int NW, int NS, int SS>
+static int fwd_warp2_launch(const FwdArgs<float>& a0, int it, cudaStream_t st) {
+  constexpr size_t smem = warp_smem_bytes<NW, NS>();
+  static int ready = set_smem(fd_fwd_warp2<NW, NS, SS>, smem);
+  if (ready != SWD_OK) return ready;
+  FwdArgs<float> a = a0;
+  a.g.n_strips = (a.g.NX - 2 + kWarpOut2 - 1) / kWarpOut2;  // 28-column strips
+  const long warps = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
+  fd_fwd_warp2<NW, NS, SS><<<(unsigned)((warps + NW - 1) / NW), 32 * NW, smem, st>>>(a, it);
+  count_launch(1);
+  return SWD_OK;
+}
+template <int NW, int NS>
+static int fwd_warp2_impl(const FwdArgs<float>& a, int it, cudaStream_t st) {
+  if (a.snap && it % a.g.nt_wf == 0) return fwd_warp2_launch<NW, NS, 0>(a, it, st);
+  if (a.snap && (it + 1) % a.g.nt_wf == 0) return fwd_warp2_launch<NW, NS, 1>(a, it, st);
+  return fwd_warp2_launch<NW, NS, -1>(a, it, st);
+}
+template <int NW, int NS, int IS>
+static int adj_warp2_launch(const AdjArgs<float>& a0, int it, cudaStream_t st) {
+  constexpr size_t smem = warp_smem_bytes<NW, NS>();
+  static int ready = set_smem(fd_adj_warp2<NW, NS, IS>, smem);
+  if (ready != SWD_OK) return ready;
+  AdjArgs<float> a = a0;
+  a.g.n_strips = (a.g.NX - 2 + kWarpOut2 - 1) / kWarpOut2;
+  const long warps = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
+  fd_adj_warp2<NW, NS, IS><<<(unsigned)((warps + NW - 1) / NW), 32 * NW, smem, st>>>(a, it);
+  count_launch(1);
+  return SWD_OK;
+}
+template <int NW, int NS>
+static int adj_warp2_impl(const AdjArgs<float>& a, int it, cudaStream_t st) {
+  if (it % a.g.nt_wf == 0) return adj_warp2_launch<NW, NS, 0>(a, it, st);
+  if ((it - 1) % a.g.nt_wf == 0) return adj_warp2_launch<NW, NS, 1>(a, it, st);
+  return adj_warp2_launch<NW, NS, -1>(a, it, st);
+}
 // (warps per CTA, row slots) of the warp-streaming kernels
 #define SWD_WARP_SHAPES(X) X(2, 4) X(4, 4) X(8, 4) X(2, 6) X(4, 6) X(8, 6) X(4, 8) X(2, 8)
 
@@ -331,6 +367,36 @@ int launch_adj_step(const AdjArgs<T>& a, int it, cudaStream_t st) {
   if (it % a.g.nt_wf == 0) return adj_dispatch<T, NF, true>(a, it, st);
   return adj_dispatch<T, NF, false>(a, it, st);
 }
+int launch_fwd_pair(const FwdArgs<float>& a, int it, cudaStream_t st) {
+  if (!fd_pairs(a.g) || a.mb || it + 1 >= a.g.nt) {
+    set_error("internal: two-step forward launch outside the warp-streaming schedule");
+    return SWD_ERR_INVALID;
+  }
+  switch (a.g.warps * 10 + a.g.ring_fwd) {
+#define X(w, s) case w * 10 + s: return fwd_warp2_impl<w, s>(a, it, st);
+    SWD_WARP_SHAPES(X)
+#undef X
+    default: break;
+  }
+  set_error("internal: unsupported FD kernel variant");
+  return SWD_ERR_INVALID;
+}
+
+int launch_adj_pair(const AdjArgs<float>& a, int it, cudaStream_t st) {
+  if (!fd_pairs(a.g) || a.mb || it < 1) {
+    set_error("internal: two-step adjoint launch outside the warp-streaming schedule");
+    return SWD_ERR_INVALID;
+  }
+  switch (a.g.warps * 10 + a.g.ring_adj) {
+#define X(w, s) case w * 10 + s: return adj_warp2_impl<w, s>(a, it, st);
+    SWD_WARP_SHAPES(X)
+#undef X
+    default: break;
+  }
+  set_error("internal: unsupported FD kernel variant");
+  return SWD_ERR_INVALID;
+}
+
 template int launch_fwd_step<float, 3>(const FwdArgs<float>&, int, cudaStream_t);
 template int launch_fwd_step<float, 4>(const FwdArgs<float>&, int, cudaStream_t);
 template int launch_fwd_step<double, 4>(const FwdArgs<double>&, int, cudaStream_t);

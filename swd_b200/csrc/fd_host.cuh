@@ -31,5 +31,12 @@ template <typename T, int NF>
 int launch_fwd_step(const FwdArgs<T>& a, int it, cudaStream_t st);
 template <typename T, int NF>
 int launch_adj_step(const AdjArgs<T>& a, int it, cudaStream_t st);
+// true when the forward and the adjoint advance two steps per launch under g (warp-streaming
+// schedule with pairs; needs nt_wf >= 2 so that at most one step of a pair is a snapshot step)
+inline bool fd_pairs(const FdGeom& g) { return g.sched == 2 && g.pairs && g.nt_wf >= 2; }
+// Forward steps it and it+1 in one launch (it+1 < nt), from a.in to a.out.
+int launch_fwd_pair(const FwdArgs<float>& a, int it, cudaStream_t st);
+// Adjoint steps it and it-1 in one launch (it >= 1), from a.in to a.out.
+int launch_adj_pair(const AdjArgs<float>& a, int it, cudaStream_t st);
 
 }  // namespace swd

@@ -34,7 +34,8 @@ struct FdGeom {
   int cells;                 // output columns per thread; a CTA owns 32*warps*cells columns
   int ring_fwd, ring_adj;    // rows in the shared-memory ring of the forward / adjoint kernels (4, 6, 8)
   int sched;                 // 0: two barriers per row (fd_smem.cuh); 1: one, velocities a row ahead (fd_lead.cuh);
-                             // 2: warp streaming, no shared memory (fd_warp.cuh; warps = warps per CTA)
+                             // 2: warp streaming (fd_warp.cuh; warps = warps per CTA)
+  int pairs;                 // schedule 2: forward and adjoint advance two steps per launch
   size_t field;              // NZ * pitch
 };
 

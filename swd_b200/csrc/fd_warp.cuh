@@ -67,7 +67,7 @@ struct WStage {
   // reach border columns, which are never updated or written.
   __device__ __forceinline__ void issue(int slot, int z) const {
     if (z <= zmax) {
-      const size_t o = (size_t)z * pitch;
+      const size_t o = (size_t)max(z, 0) * pitch;
       WSlot& s = slots[slot];
       wcp16(&s.q[lane], q + o);
       wcp16(&s.m[lane], mat + o);
@@ -251,6 +251,211 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp(FwdArgs<float> a, int it)
   wcp_wait<0>();  // no copy may still target this warp's slots at exit
 }
 
+// ---------------------------------------------------------------- forward, two steps per launch
+
+constexpr int kWarpOut2 = 28;  // output columns per warp of the two-step kernels (two halo lanes a side)
+
+// Steps it and it+1 in one sweep: the state after step it (S1) is formed row by row as in
+// fd_fwd_warp and kept in registers, and step it+1 runs one row behind it on S1, so S1 never
+// goes to memory and a launch moves the state once for two steps.  Lanes x = 28*strip-1 ..
+// 28*strip+30: S1 is valid on lanes 1..30, the new state on lanes 2..29, which write.  Border
+// cells keep their state, as the one-step kernels leave them unwritten.  SNAPSUB: which of
+// the two steps writes strain snapshots (-1 neither).
+template <int NW, int NS, int SNAPSUB>
+__global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it) {
+  static_assert(NS >= 4 && NS % 2 == 0, "rows k, k+1 in use, at least two in flight; even for the unrolled rotation");
+  using T = float;
+  const FdGeom& g = a.g;
+  int strip, chunk, shot;
+  if (!warp_tile(g, a.n_shots, NW, strip, chunk, shot)) return;
+  const int lane = threadIdx.x & 31;
+  const int x = kWarpOut2 * strip + lane - 1;
+  const int zs = 1 + chunk * g.chunk;
+  const int ze = min(zs + g.chunk, g.NZ - 1);
+  const size_t F = g.field;
+  const bool xint = x >= 1 && x <= g.NX - 2;
+  const bool own = xint && lane >= 2 && lane <= kWarpOut2 + 1;
+  const int xc = min(max(x, 0), g.NX - 1);
+  const float* sb = a.in + (size_t)shot * 5 * F;
+  extern __shared__ __align__(16) unsigned char wsmem[];
+  const WStage ld{reinterpret_cast<const float4*>(sb) + xc, sb + 4 * F + xc, a.mat + xc,
+                  reinterpret_cast<WSlot*>(wsmem) + (threadIdx.x >> 5) * NS, g.pitch, min(ze + 1, g.NZ - 1), lane};
+  float* obs = a.out + (size_t)shot * 5 * F;
+  float4* oq = reinterpret_cast<float4*>(obs) + xc;
+  float* oxz = obs + 4 * F + xc;
+  const int st = a.src_type;
+  const int2 sp = a.src[shot];
+  const T sv1 = a.s[it], sv2 = a.s[it + 1];
+  const T dtx = a.dtx;
+  const bool sc = x == sp.y, sr = x == sp.y + 1;
+  const bool s_w = sc && st != 1 && st != 4;
+  const bool s_wr = sr && st == 2;
+  const bool s_u = sc && (st == 2 || st == 3);
+  const bool s_um = sc && st == 2;
+  const bool s_xz = sc && (st == 1 || st == 4);
+  const int recj = (a.seis_w != nullptr && own && x >= g.gx && (x - g.gx) % g.dg == 0 && (x - g.gx) / g.dg < g.ng)
+                       ? (x - g.gx) / g.dg : -1;
+  const int z_img0 = g.pad_top + 1, z_img1 = g.pad_top + 1 + g.nz;
+  const size_t plane = (size_t)g.nz * g.nx;
+  const bool snapc = SNAPSUB >= 0 && own && x >= g.nbc && x < g.nbc + g.nx;
+  T* snap_base = SNAPSUB >= 0 ? a.snap + ((size_t)shot * g.nrec + ((it + (SNAPSUB > 0 ? 1 : 0)) / g.nt_wf - a.rec0)) *
+                                            3 * plane : nullptr;
+  auto bz = [&](int z) -> T { return z == g.pad_top ? T(2) * dtx : dtx; };
+  auto rowin = [&](int z) { return z >= 1 && z <= g.NZ - 2; };
+  auto vel_w = [&](bool inner, T ww, T xz, T xzl, T zz, T zzd, T te, T b1) -> T {
+    return inner ? te * ww + b1 * (((xz - xzl) + zzd) - zz) : ww;
+  };
+  auto vel_u = [&](bool inner, T uu, T xx, T xxr, T xz, T xzu, T te, T b) -> T {
+    return inner ? te * uu + b * (((xxr - xx) + xz) - xzu) : uu;
+  };
+  auto src_w = [&](int z, T r, T sv) -> T {
+    if (z == sp.x) {
+      if (s_w) r = (st == 5) ? sv : r + sv;
+      else if (s_wr) r = r + sv;
+    }
+    return r;
+  };
+  auto src_u = [&](int z, T r, T sv) -> T {
+    if (s_u && z == sp.x) r = r + sv;
+    if (s_um && z == sp.x - 1) r = r - sv;
+    return r;
+  };
+  // One row k of one step, on rows R0 = k and R1 = k+1 of the state before it (materials m0 of
+  // row k, temp t1 of row k+1); wn_prev = new ww of row k-1, un_cur = new uu of row k on entry,
+  // those of rows k and k+1 on exit.  Returns the new state of row k and its strains.
+  struct St { T uu, ww, xx, zz, xz; };
+  struct Strain { T fux, bwz, sg; };
+  auto one = [&](auto slow_tag, const St& R0, const float4& m0, const St& R1, T t1, int k, T sv, T& wn_prev,
+                 T& un_cur, Strain& sn) -> St {
+    constexpr bool SLOW = decltype(slow_tag)::value;
+    const bool in0 = !SLOW || rowin(k);
+    const bool in1 = !SLOW || rowin(k + 1);
+    const T xzl = shfl_l(R0.xz);
+    T wn = vel_w(xint && in0, R0.ww, R0.xz, xzl, R0.zz, R1.zz, m0.x, SLOW ? bz(k) : dtx);
+    const T xxr = shfl_r(R1.xx);
+    T un_next = vel_u(xint && in1, R1.uu, R1.xx, xxr, R1.xz, R0.xz, t1, SLOW ? bz(k + 1) : dtx);
+    if (SLOW) {
+      wn = src_w(k, wn, sv);
+      un_next = src_u(k + 1, un_next, sv);
+    }
+    const T ucl = shfl_l(un_cur);
+    const T wnr = shfl_r(wn);
+    const T fux = un_cur - ucl;
+    const T fuz = un_next - un_cur;
+    const T bwx = wnr - wn;
+    const T bwz = wn - wn_prev;
+    T xo = R0.xx, zo = R0.zz;
+    if (SLOW && s_xz && k == sp.x) {
+      if (st == 1) { xo = xo + sv; zo = zo + sv; }
+      else { zo = zo + sv; }
+    }
+    const T xxn = m0.x * xo + (m0.y * fux + m0.z * bwz) * dtx;
+    T zzn = m0.x * zo + (m0.y * bwz + m0.z * fux) * dtx;
+    const T xzn = m0.x * R0.xz + (m0.w * (fuz + bwx)) * dtx;
+    if (SLOW && k == g.pad_top) zzn = T(0);
+    St r{un_cur, wn, xxn, zzn, xzn};
+    if (!(xint && in0)) r = R0;  // border cells keep their state
+    sn = Strain{fux, bwz, fuz + bwx};
+    wn_prev = wn;
+    un_cur = un_next;
+    return r;
+  };
+  auto as_st = [](const WRow& w) { return St{w.uu, w.ww, w.xx, w.zz, w.xz}; };
+
+  // State row r is staged in slot (r - zs + 2) % NS and held in RR[(r - zs) & 1]; S1 row r in
+  // T1[(r - zs + 1) & 1].
+#pragma unroll
+  for (int u = 0; u < NS; ++u) ld.issue(u, zs - 2 + u);
+  wcp_wait<NS - 2>();
+  WRow RR[2];
+  ld.read(RR[0], 0);
+  ld.read(RR[1], 1);
+  T wn1, un1;  // first step: new ww of row k1-1, new uu of row k1
+  {
+    const WRow& A = RR[0];
+    const WRow& B = RR[1];
+    wn1 = src_w(zs - 2, vel_w(xint && rowin(zs - 2), A.ww, A.xz, shfl_l(A.xz), A.zz, B.zz, A.m.x, bz(zs - 2)), sv1);
+    un1 = src_u(zs - 1, vel_u(xint && rowin(zs - 1), B.uu, B.xx, shfl_r(B.xx), B.xz, A.xz, B.m.x, bz(zs - 1)), sv1);
+  }
+  St T1[2];      // S1 rows k1-1 and k1 (alternating)
+  float4 MT[2];  // their materials
+  T wn2, un2;    // second step: new ww of row k1-2, new uu of row k1-1
+  // First-step row k1 from state rows RR[c0] (k1) and RR[c0^1] (k1+1, read from slot s1 after
+  // staging row k1+NS-1 into slot spf, row k1-1's); its S1 row goes to T1[c1].
+  auto first = [&](auto slow_tag, int c0, int s1, int spf, int c1, int k1) {
+    ld.issue(spf, k1 + NS - 1);
+    wcp_wait<NS - 2>();
+    ld.read(RR[c0 ^ 1], s1);
+    const WRow& R0 = RR[c0];
+    const WRow& R1 = RR[c0 ^ 1];
+    Strain sn;
+    T1[c1] = one(slow_tag, as_st(R0), R0.m, as_st(R1), R1.m.x, k1, sv1, wn1, un1, sn);
+    MT[c1] = R0.m;
+    if (decltype(slow_tag)::value && recj >= 0 && k1 == g.gz && k1 >= zs && k1 < ze) {  // :342-345, step it
+      const size_t r = ((size_t)shot * g.nt + it) * g.ng + recj;
+      a.seis_w[r] = T1[c1].ww;
+      if (a.seis_u) a.seis_u[r] = T1[c1].uu;
+    }
+    if (SNAPSUB == 0 && snapc && k1 >= z_img0 && k1 < z_img1 && k1 >= zs && k1 < ze) {
+      T* s0 = snap_base + ((size_t)(k1 - z_img0) * g.nx + (x - g.nbc));
+      s0[0] = sn.fux;
+      s0[plane] = sn.bwz;
+      s0[2 * plane] = sn.sg;
+    }
+  };
+  // Second-step row j = k1-1 from S1 rows T1[c1^1] (j) and T1[c1] (k1); writes the new state.
+  auto second = [&](auto slow_tag, int c1, int j) {
+    Strain sn;
+    const St r = one(slow_tag, T1[c1 ^ 1], MT[c1 ^ 1], T1[c1], MT[c1].x, j, sv2, wn2, un2, sn);
+    if (own) {
+      const size_t o = (size_t)j * g.pitch;
+      oq[o] = make_float4(r.uu, r.ww, r.xx, r.zz);
+      oxz[o] = r.xz;
+    }
+    if (decltype(slow_tag)::value && recj >= 0 && j == g.gz) {  // step it+1
+      const size_t rr = ((size_t)shot * g.nt + it + 1) * g.ng + recj;
+      a.seis_w[rr] = r.ww;
+      if (a.seis_u) a.seis_u[rr] = r.uu;
+    }
+    if (SNAPSUB == 1 && snapc && j >= z_img0 && j < z_img1) {
+      T* s0 = snap_base + ((size_t)(j - z_img0) * g.nx + (x - g.nbc));
+      s0[0] = sn.fux;
+      s0[plane] = sn.bwz;
+      s0[2 * plane] = sn.sg;
+    }
+  };
+  auto slow1 = [&](int k) {
+    return k <= 1 || k >= g.NZ - 2 || k == g.pad_top || k == g.gz || (k >= sp.x - 2 && k <= sp.x);
+  };
+  // peeled: S1 rows zs-1 and zs, then the second step's prologue (new ww of row zs-1, new uu of row zs)
+  first(std::true_type{}, 1, 2 % NS, 0, 0, zs - 1);
+  first(std::true_type{}, 0, 3 % NS, 1, 1, zs);
+  {
+    const St& A = T1[0];
+    const St& B = T1[1];
+    wn2 = src_w(zs - 1, vel_w(xint && rowin(zs - 1), A.ww, A.xz, shfl_l(A.xz), A.zz, B.zz, MT[0].x, bz(zs - 1)), sv2);
+    un2 = src_u(zs, vel_u(xint, B.uu, B.xx, shfl_r(B.xx), B.xz, A.xz, MT[1].x, bz(zs)), sv2);
+  }
+  // Rows k1 = zs+1 .. ze, u = k1 - zs - 1: state row k1 is RR[(u + 1) & 1], row k1+1 comes from
+  // slot (u + 4) % NS, row k1-1's slot (u + 2) % NS is restaged, and S1 row k1 goes to T1[u & 1].
+  auto both = [&](auto slow_tag, int u, int k1) {
+    first(slow_tag, (u + 1) & 1, (u + 4) % NS, (u + 2) % NS, u & 1, k1);
+    second(slow_tag, u & 1, k1 - 1);
+  };
+  int k1 = zs + 1;
+  for (; k1 + NS <= ze + 1; k1 += NS) {
+#pragma unroll
+    for (int u = 0; u < NS; ++u) {
+      if (slow1(k1 + u) || slow1(k1 + u - 1)) both(std::true_type{}, u, k1 + u);
+      else both(std::false_type{}, u, k1 + u);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < NS - 1; ++u)
+    if (k1 + u <= ze) both(std::true_type{}, u, k1 + u);
+  wcp_wait<0>();
+}
+
 // ---------------------------------------------------------------- adjoint
 
 template <int NW, int NS, bool IMG>
@@ -390,6 +595,188 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp(AdjArgs<float> a, int it)
     if (k + u < ze)
       row(RR[(u + 1) & 1], RR[u & 1], (u + 2) % NS, u, QP[(u + 1) & 1], QP[u & 1], IM[u & 1], IM[(u + 1) & 1],
           k + u);
+  wcp_wait<0>();
+}
+
+// ---------------------------------------------------------------- adjoint, two steps per launch
+
+// Adjoint steps it and it-1 in one sweep, built as fd_fwd_warp2: the state after step it (S1)
+// is formed row by row in registers and step it-1 runs one row behind it.  IMGSUB: which of
+// the two steps applies the imaging condition (0: step it, 1: step it-1, -1 neither).
+template <int NW, int NS, int IMGSUB>
+__global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it) {
+  static_assert(NS >= 4 && NS % 2 == 0, "rows k, k+1 in use, at least two in flight; even for the unrolled rotation");
+  using T = float;
+  const FdGeom& g = a.g;
+  int strip, chunk, shot;
+  if (!warp_tile(g, a.n_shots, NW, strip, chunk, shot)) return;
+  const int lane = threadIdx.x & 31;
+  const int x = kWarpOut2 * strip + lane - 1;
+  const int zs = 1 + chunk * g.chunk;
+  const int ze = min(zs + g.chunk, g.NZ - 1);
+  const size_t F = g.field;
+  const bool xin = x >= 0 && x < g.NX;
+  const bool xint = x >= 1 && x <= g.NX - 2;
+  const bool own = xint && lane >= 2 && lane <= kWarpOut2 + 1;
+  const int xc = min(max(x, 0), g.NX - 1);
+  const float* sb = a.in + (size_t)shot * 5 * F;
+  extern __shared__ __align__(16) unsigned char wsmem[];
+  const WStage ld{reinterpret_cast<const float4*>(sb) + xc, sb + 4 * F + xc, a.mat + xc,
+                  reinterpret_cast<WSlot*>(wsmem) + (threadIdx.x >> 5) * NS, g.pitch, min(ze + 1, g.NZ - 1), lane};
+  float* obs = a.out + (size_t)shot * 5 * F;
+  float4* oq = reinterpret_cast<float4*>(obs) + xc;
+  float* oxz = obs + 4 * F + xc;
+  const T dtx = a.dtx;
+  // dt*res of steps it and it-1 at receiver columns (:238-242); halo lanes inject too
+  const bool rec = xin && x >= g.gx && (x - g.gx) % g.dg == 0 && (x - g.gx) / g.dg < g.ng;
+  const size_t rrow = ((size_t)shot * g.nt + it) * g.ng + (rec ? (x - g.gx) / g.dg : 0);
+  const T inj1 = rec ? a.dt * a.res[rrow] : T(0);
+  const T inj2 = rec ? a.dt * a.res[rrow - g.ng] : T(0);
+  const int z_img0 = g.pad_top + 1, z_img1 = g.pad_top + 1 + g.nz;
+  const size_t plane = (size_t)g.nz * g.nx;
+  const bool ximg = IMGSUB >= 0 && own && x >= g.nbc && x < g.nbc + g.nx;
+  const T* snap_b = IMGSUB >= 0 ? a.snap + ((size_t)shot * g.nrec + ((it - (IMGSUB > 0 ? 1 : 0)) / g.nt_wf - a.rec0)) *
+                                               3 * plane : nullptr;
+  double* img_b = a.img + (size_t)shot * 3 * plane;
+  auto bz = [&](int z) -> T { return z == g.pad_top ? T(2) * dtx : dtx; };
+  auto rowin = [&](int z) { return z >= 1 && z <= g.NZ - 2; };
+  struct St { T uu, ww, xx, zz, xz; };
+  struct Prod { T p1, p2, p3, q1, q2; };  // ca*xx, cl*zz, cm1*xz, cl*xx, ca*zz
+  auto prod = [](const St& r, const float4& m) -> Prod {
+    return Prod{m.y * r.xx, m.z * r.zz, m.w * r.xz, m.z * r.xx, m.y * r.zz};
+  };
+  struct Img { T fx, bz, sg; double c0, c1, c2; };
+  auto img_row = [&](int z) { return IMGSUB >= 0 && z >= z_img0 && z < z_img1 && z >= zs && z < ze; };
+  auto load_img = [&](Img& m, int z) {
+    if (ximg && img_row(z)) {
+      const size_t cell = (size_t)(z - z_img0) * g.nx + (x - g.nbc);
+      const T* s0 = snap_b + cell;
+      m.fx = s0[0]; m.bz = s0[plane]; m.sg = s0[2 * plane];
+      m.c0 = img_b[cell]; m.c1 = img_b[plane + cell]; m.c2 = img_b[2 * plane + cell];
+    }
+  };
+  auto image = [&](const Img& m, const St& r, int z) {  // imaging condition (:274-279)
+    if (ximg && img_row(z)) {
+      const size_t cell = (size_t)(z - z_img0) * g.nx + (x - g.nbc);
+      const T Fs = m.fx + m.bz;
+      const T tcl = Fs * (r.xx + r.zz);
+      const T tcm = T(2) * ((r.xx * m.fx + r.zz * m.bz) + T(0.5) * (r.xz * m.sg));
+      const T til = Fs * Fs;
+      img_b[cell] = m.c0 + (double)tcl;
+      img_b[plane + cell] = m.c1 + (double)tcm;
+      img_b[2 * plane + cell] = m.c2 + (double)til;
+    }
+  };
+  // One row k of one adjoint step on rows R0 = k (materials m0, products Q0) and R1 = k+1
+  // (temp t1, products Q1); wn_prev / un_cur as in fd_adj_warp.  Returns the new state of row k.
+  auto one = [&](auto slow_tag, const St& R0, const float4& m0, const Prod& Q0, const St& R1, T t1, const Prod& Q1,
+                 int k, T inj, T& wn_prev, T& un_cur) -> St {
+    constexpr bool SLOW = decltype(slow_tag)::value;
+    const bool in0 = !SLOW || rowin(k);
+    const bool in1 = !SLOW || rowin(k + 1);
+    T wn = adj_vel_w(xint && in0, R0.ww, Q1.q1, Q0.q1, Q1.q2, Q0.q2, shfl_r(Q0.p3), Q0.p3, m0.x, SLOW ? bz(k) : dtx);
+    if (SLOW && rec && k == g.gz) wn = wn + inj;
+    const T p1l = shfl_l(Q1.p1), p2l = shfl_l(Q1.p2);
+    const T un_next = adj_vel_u(xint && in1, R1.uu, Q1.p1, p1l, Q1.p2, p2l, Q1.p3, Q0.p3, t1, SLOW ? bz(k + 1) : dtx);
+    const T un_r = shfl_r(un_cur);
+    const T wn_l = shfl_l(wn);
+    const T te = m0.x;
+    const T xxn = te * R0.xx - dtx * (un_r - un_cur);
+    T zzn = te * R0.zz - dtx * (wn - wn_prev);
+    const T xzn = (te * R0.xz - dtx * (un_next - un_cur)) - dtx * (wn - wn_l);
+    if (SLOW && k == g.pad_top) zzn = T(0);
+    St r{un_cur, wn, xxn, zzn, xzn};
+    if (!(xint && in0)) r = R0;  // border cells keep their state
+    wn_prev = wn;
+    un_cur = un_next;
+    return r;
+  };
+  auto as_st = [](const WRow& w) { return St{w.uu, w.ww, w.xx, w.zz, w.xz}; };
+
+  // state rows staged from zs-2: row r in slot (r - zs + 2) % NS and RR[(r - zs) & 1]
+#pragma unroll
+  for (int u = 0; u < NS; ++u) ld.issue(u, zs - 2 + u);
+  wcp_wait<NS - 2>();
+  WRow RR[2];
+  ld.read(RR[0], 0);
+  ld.read(RR[1], 1);
+  Prod QR[2] = {prod(as_st(RR[0]), RR[0].m), prod(as_st(RR[1]), RR[1].m)};  // products of the state rows
+  T wn1, un1;  // first step: new ww of row k1-1, new uu of row k1
+  {
+    const St B = as_st(RR[1]);
+    const int k = zs - 2;
+    T w = adj_vel_w(xint && rowin(k), RR[0].ww, QR[1].q1, QR[0].q1, QR[1].q2, QR[0].q2, shfl_r(QR[0].p3), QR[0].p3,
+                    RR[0].m.x, bz(k));
+    if (rec && k == g.gz) w = w + inj1;
+    wn1 = w;
+    const T p1l = shfl_l(QR[1].p1), p2l = shfl_l(QR[1].p2);
+    un1 = adj_vel_u(xint && rowin(k + 1), B.uu, QR[1].p1, p1l, QR[1].p2, p2l, QR[1].p3, QR[0].p3, RR[1].m.x,
+                    bz(k + 1));
+  }
+  St T1[2];      // S1 rows, T1[(r - zs + 1) & 1]
+  float4 MT[2];  // their materials
+  Prod QT[2];    // their products
+  Img IM[2] = {};  // imaging operands of row r in IM[(r - zs) & 1]
+  T wn2, un2;    // second step: new ww of row k1-2, new uu of row k1-1
+  // first-step row k1 (slot and register bookkeeping as in fd_fwd_warp2)
+  auto first = [&](auto slow_tag, int c0, int s1, int spf, int c1, int k1) {
+    ld.issue(spf, k1 + NS - 1);
+    wcp_wait<NS - 2>();
+    ld.read(RR[c0 ^ 1], s1);
+    QR[c0 ^ 1] = prod(as_st(RR[c0 ^ 1]), RR[c0 ^ 1].m);
+    const WRow& R0 = RR[c0];
+    const WRow& R1 = RR[c0 ^ 1];
+    T1[c1] = one(slow_tag, as_st(R0), R0.m, QR[c0], as_st(R1), R1.m.x, QR[c0 ^ 1], k1, inj1, wn1, un1);
+    MT[c1] = R0.m;
+    QT[c1] = prod(T1[c1], R0.m);
+    if (IMGSUB == 0) {  // row k1's operands in IM[c1 ^ 1], row k1+1's go to IM[c1]
+      load_img(IM[c1], k1 + 1);
+      image(IM[c1 ^ 1], T1[c1], k1);
+    }
+  };
+  // second-step row j = k1-1 from S1 rows T1[c1^1] (j) and T1[c1] (k1); writes the new state
+  auto second = [&](auto slow_tag, int c1, int j) {
+    const St r = one(slow_tag, T1[c1 ^ 1], MT[c1 ^ 1], QT[c1 ^ 1], T1[c1], MT[c1].x, QT[c1], j, inj2, wn2, un2);
+    if (own) {
+      const size_t o = (size_t)j * g.pitch;
+      oq[o] = make_float4(r.uu, r.ww, r.xx, r.zz);
+      oxz[o] = r.xz;
+    }
+    if (IMGSUB == 1) {  // row j's operands in IM[c1], row j+1's go to IM[c1 ^ 1]
+      load_img(IM[c1 ^ 1], j + 1);
+      image(IM[c1], r, j);
+    }
+  };
+  auto slow1 = [&](int k) { return k <= 1 || k >= g.NZ - 2 || k == g.pad_top || k == g.gz; };
+  first(std::true_type{}, 1, 2 % NS, 0, 0, zs - 1);
+  first(std::true_type{}, 0, 3 % NS, 1, 1, zs);
+  {
+    const St& A = T1[0];
+    const St& B = T1[1];
+    const int k = zs - 1;
+    T w = adj_vel_w(xint && rowin(k), A.ww, QT[1].q1, QT[0].q1, QT[1].q2, QT[0].q2, shfl_r(QT[0].p3), QT[0].p3,
+                    MT[0].x, bz(k));
+    if (rec && k == g.gz) w = w + inj2;
+    wn2 = w;
+    const T p1l = shfl_l(QT[1].p1), p2l = shfl_l(QT[1].p2);
+    un2 = adj_vel_u(xint, B.uu, QT[1].p1, p1l, QT[1].p2, p2l, QT[1].p3, QT[0].p3, MT[1].x, bz(zs));
+  }
+  if (IMGSUB == 1) load_img(IM[0], zs);
+  auto both = [&](auto slow_tag, int u, int k1) {
+    first(slow_tag, (u + 1) & 1, (u + 4) % NS, (u + 2) % NS, u & 1, k1);
+    second(slow_tag, u & 1, k1 - 1);
+  };
+  int k1 = zs + 1;
+  for (; k1 + NS <= ze + 1; k1 += NS) {
+#pragma unroll
+    for (int u = 0; u < NS; ++u) {
+      if (slow1(k1 + u) || slow1(k1 + u - 1)) both(std::true_type{}, u, k1 + u);
+      else both(std::false_type{}, u, k1 + u);
+    }
+  }
+#pragma unroll
+  for (int u = 0; u < NS - 1; ++u)
+    if (k1 + u <= ze) both(std::true_type{}, u, k1 + u);
   wcp_wait<0>();
 }
 

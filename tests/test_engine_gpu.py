@@ -70,7 +70,13 @@ def test_modes_are_bit_identical(tiny_case):
                {"snapshot_mode": 1, "fd_schedule": 2, "warps": 2, "chunk_rows": 3},
                {"snapshot_mode": 2, "fd_schedule": 2, "warps": 8, "chunk_rows": 2, "use_graphs": False},
                {"snapshot_mode": 1, "fd_schedule": 2, "ring_fwd": 6, "ring_adj": 8, "chunk_rows": 9},
-               {"snapshot_mode": 2, "fd_schedule": 2, "warps": 8, "ring_fwd": 8, "ring_adj": 6, "chunk_rows": 5}):
+               {"snapshot_mode": 2, "fd_schedule": 2, "warps": 8, "ring_fwd": 8, "ring_adj": 6, "chunk_rows": 5},
+               # two time steps per launch: pairs end at checkpoints (odd and even intervals)
+               {"snapshot_mode": 1, "fd_schedule": 3}, {"snapshot_mode": 2, "ckpt_interval": 35, "fd_schedule": 3},
+               {"snapshot_mode": 2, "ckpt_interval": 20, "fd_schedule": 3, "chunk_rows": 1},
+               {"snapshot_mode": 1, "fd_schedule": 3, "warps": 8, "ring_fwd": 6, "chunk_rows": 4},
+               {"snapshot_mode": 1, "fd_schedule": 3, "warps": 2, "ring_fwd": 8, "ring_adj": 6, "chunk_rows": 2,
+                "use_graphs": False}):
         with GradientEngine(s, **kw) as e:
             e.set_observed(cr0_r, cr0_l)
             outs.append(e.gradient(s.vp, s.vs))
@@ -79,10 +85,11 @@ def test_modes_are_bit_identical(tiny_case):
             assert np.array_equal(o[k], outs[0][k]), k
 
 
-@pytest.mark.parametrize("sched", [1, 2])
+@pytest.mark.parametrize("sched", [1, 2, 3])
 def test_other_schedules_on_the_plain_survey_match_the_oracle(O, sched):
-    """The one-barrier (1) and warp-streaming (2) schedules against the oracle on the 30 x 120
-    survey (source near the top, receivers on the free-surface row, several chunks)."""
+    """The one-barrier (1), warp-streaming (2) and two-steps-per-launch (3) schedules against the
+    oracle on the 30 x 120 survey (source near the top, receivers on the free-surface row,
+    several chunks)."""
     s = configs.plain_c1(ns=3, nt=1000)
     cr0_r, cr0_l = O.observed_curves(s, s.vs_true)
     ref = O.gradient(s, s.vs, cr0_r, cr0_l)
