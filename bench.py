@@ -31,16 +31,18 @@ import numpy as np  # noqa: E402
 
 METRIC = "shot-gradients/s (fwd+adj)"
 UNIT = "shot-gradients/s"
-# DRAM traffic per padded cell and time step of the FD step kernels (plain-step variants, 4 of
-# every 5 launches) for each FD schedule, from the ncu captures summarised in
-# profiles/fd_step_kernels_batched-100x600.md (schedule 0) and
-# profiles/fd_warp_kernels_batched-100x600.md (schedule 2):
+# DRAM traffic per padded cell and launch of the FD step kernels (plain variants, without the
+# snapshot or imaging step) for each FD schedule, from the ncu captures summarised in
+# profiles/fd_step_kernels_batched-100x600.md (schedule 0), profiles/fd_warp_kernels_batched-100x600.md
+# (schedule 2) and profiles/fd_warp2_kernels_batched-100x600.md (schedule 3, two steps per launch):
 # (dram__bytes_read.sum + dram__bytes_write.sum) per launch / (96 shots x 132 x 660 cells).
-NCU_BYTES_PER_CELL_STEP = {0: {"fd_fwd_step": 36.1, "fd_adj_step": 36.1},
-                           2: {"fd_fwd_step": 35.05, "fd_adj_step": 34.99}}
+NCU_BYTES_PER_CELL_LAUNCH = {0: {"fd_fwd_step": 36.1, "fd_adj_step": 36.1},
+                             2: {"fd_fwd_step": 35.05, "fd_adj_step": 34.99},
+                             3: {"fd_fwd_step": 35.35, "fd_adj_step": 35.29}}
 # Compulsory DRAM bytes of the fused one-sweep kernels: 5 state fields read + 5 written per
-# shot-cell-step (materials are shared by the shots of a launch), plus per interior cell every
-# nt_wf steps the 3-field snapshot write (forward) or snapshot read + FP64 image update (adjoint).
+# shot-cell and launch (a launch advances one step, or two under schedule 3; materials are
+# shared by the shots of a launch), plus per interior cell every nt_wf steps the 3-field
+# snapshot write (forward) or snapshot read + FP64 image update (adjoint).
 COMPULSORY_STATE_B = 40
 
 
@@ -571,22 +573,24 @@ def main():
     # algorithmic bytes per launch (one time step of every shot): the reference's two-phase
     # schedule, 84 B per padded cell-step, plus 16 B snapshot write (forward) or 16 B snapshot
     # read + 48 B FP64 image update (adjoint) per interior cell every nt_wf steps
-    fwd_bytes = cells * 84 + inner * 16 / s.nt_wf
-    adj_bytes = cells * 84 + inner * (16 + 48) / s.nt_wf
-    fwd_comp = cells * COMPULSORY_STATE_B + inner * 12 / s.nt_wf
-    adj_comp = cells * COMPULSORY_STATE_B + inner * (12 + 48) / s.nt_wf
-    fwd_launch_ms = fwd_ms / s.nt
+    spl = 2 if info["fd_schedule"] == 3 else 1  # time steps per launch
+    fwd_bytes = spl * (cells * 84 + inner * 16 / s.nt_wf)
+    adj_bytes = spl * (cells * 84 + inner * (16 + 48) / s.nt_wf)
+    fwd_comp = cells * COMPULSORY_STATE_B + spl * inner * 12 / s.nt_wf
+    adj_comp = cells * COMPULSORY_STATE_B + spl * inner * (12 + 48) / s.nt_wf
+    fwd_launch_ms = fwd_ms / s.nt * spl
     # checkpoint mode: the adjoint phase also re-runs the forward steps segment by segment
-    adj_launch_ms = ((adj_ms - fwd_ms) if info["mode"] == 2 else adj_ms) / (s.nt - 1)
+    adj_launch_ms = ((adj_ms - fwd_ms) if info["mode"] == 2 else adj_ms) / (s.nt - 1) * spl
     peak, peak_kind = peaks()
 
     def roof(name, nbytes, comp, launch_ms):
         ach = nbytes / (launch_ms / 1e3) / 1e9
-        tr = NCU_BYTES_PER_CELL_STEP.get(info["fd_schedule"], {}).get(name)
+        tr = NCU_BYTES_PER_CELL_LAUNCH.get(info["fd_schedule"], {}).get(name)
         return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                 "fallback 6650 GB/s", "traffic": (tr * cells) if tr else None,
-                "traffic_source": f"ncu, plain-step variant of FD schedule {info['fd_schedule']}" if tr else None,
+                "traffic_source": f"ncu, plain variant of FD schedule {info['fd_schedule']}" if tr else None,
+                "steps_per_launch": spl,
                 "algorithmic_bytes_per_launch": nbytes, "avg_launch_ms": launch_ms,
                 "compulsory_bytes_per_launch": comp,
                 "frac_compulsory": comp / (launch_ms / 1e3) / 1e9 / peak}
