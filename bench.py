@@ -33,10 +33,10 @@ METRIC = "shot-gradients/s (fwd+adj)"
 UNIT = "shot-gradients/s"
 # DRAM traffic per padded cell and launch of the FD step kernels (plain variants, without the
 # snapshot or imaging step) for each FD schedule, from the ncu captures summarised in
-# profiles/fd_step_kernels_batched-100x600.md (schedule 0), profiles/fd_warp_kernels_batched-100x600.md
+# profiles/fd_step_kernels_batched-100x600.md (schedule 4), profiles/fd_warp_kernels_batched-100x600.md
 # (schedule 2) and profiles/fd_warp2_kernels_batched-100x600.md (schedule 3, two steps per launch):
 # (dram__bytes_read.sum + dram__bytes_write.sum) per launch / (96 shots x 132 x 660 cells).
-NCU_BYTES_PER_CELL_LAUNCH = {0: {"fd_fwd_step": 36.1, "fd_adj_step": 36.1},
+NCU_BYTES_PER_CELL_LAUNCH = {4: {"fd_fwd_step": 36.1, "fd_adj_step": 36.1},
                              2: {"fd_fwd_step": 35.05, "fd_adj_step": 34.99},
                              3: {"fd_fwd_step": 35.35, "fd_adj_step": 35.29}}
 # Compulsory DRAM bytes of the fused one-sweep kernels: 5 state fields read + 5 written per
@@ -67,7 +67,8 @@ def parse():
     p.add_argument("--ring", type=int, default=0)
     p.add_argument("--chunk", type=int, default=0)
     p.add_argument("--sched", type=int, default=-1,
-                   help="FD schedule: 0 two barriers per row, 1 one barrier, 2 warp streaming (-1: autotuned)")
+                   help="FD schedule: 0 or 3 warp streaming, two steps per launch; 1 one barrier per row; "
+                        "2 warp streaming, one step; 4 two barriers per row (-1: autotuned)")
     p.add_argument("--serve", type=int, default=0,
                    help="served request stream: number of requests (0: run the gradient bench instead)")
     p.add_argument("--rate", type=float, default=2.0, help="served stream: Poisson arrival rate, requests/s")

@@ -227,10 +227,12 @@ typedef struct {
                          (overrides warps, cells, ring_*, chunk_rows, fd_schedule) */
   int radon_precision; /* forward Radon contraction: SWD_PREC_FP64 (0, default, as the reference)
                           or SWD_PREC_BF16X2 / _BF16X3 (tcgen05 split-BF16, see swd_contract_*) */
-  int fd_schedule;    /* FD kernels: 0 two CTA barriers per row, 1 one barrier with the velocities
-                         a row ahead (shapes (2,1), (3,1), (4,1) ring 4, (3,1) ring 6), 2 warp
-                         streaming (warps = 2, 4 or 8 per CTA, ring_* = 4, 6 or 8 staged rows),
-                         3 warp streaming with two time steps per launch; same bits */
+  int fd_schedule;    /* FD kernels, all giving the same bits: 0 (default) or 3 warp streaming
+                         with two time steps per launch, 2 warp streaming with one step per launch
+                         (both: warps = 2, 4 or 8 per CTA, ring_* = 4, 6 or 8 staged rows), 1 one
+                         CTA barrier per row with the velocities a row ahead (shapes (2,1), (3,1),
+                         (4,1) ring 4, (3,1) ring 6), 4 two CTA barriers per row (shared-memory
+                         ring; the shapes of warps/cells/ring_*) */
   int adjoint_weight; /* adjoint source: 0 ADWDgrad_1 (SoftMax weights, SWD.m:190), 1 ADWDgrad_norm
                          (Gaussian weights around the picks, core/ADWDgrad_norm.m), 2 the WD residual
                          weight_data_muti3 with F1 = 0 (SWD.m:188; ind = fmin/df+1, win = npair+2*ind,

@@ -744,9 +744,11 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   g.cells = e->opt.cells;
   g.ring_fwd = e->opt.ring_fwd;
   g.ring_adj = e->opt.ring_adj;
-  g.sched = (e->opt.fd_schedule == 1 || e->opt.fd_schedule == 2) ? e->opt.fd_schedule
-            : e->opt.fd_schedule == 3 ? 2 : 0;
-  g.pairs = e->opt.fd_schedule == 3 ? 1 : 0;  // warp streaming, two steps per launch
+  // fd_schedule: 0 (default) and 3 warp streaming with two steps per launch, 1 one barrier per
+  // row, 2 warp streaming one step per launch, 4 two barriers per row
+  const int fs = e->opt.fd_schedule;
+  g.sched = fs == 1 ? 1 : fs == 4 ? 0 : 2;
+  g.pairs = (fs == 0 || fs == 3) ? 1 : 0;
   plan_decomposition(g, std::max(1, std::min(e->opt.max_batch > 0 ? e->opt.max_batch : e->ns, e->ns)),
                      e->opt.chunk_rows);
   // Radon geometry
@@ -884,7 +886,7 @@ static void fill_info(const swd_engine* e, swd_engine_info_t* info) {
   info->ring_adj = e->g.ring_adj;
   info->tuned_fwd_us = e->tuned_fwd_us;
   info->tuned_adj_us = e->tuned_adj_us;
-  info->fd_schedule = fd_pairs(e->g) ? 3 : e->g.sched;
+  info->fd_schedule = fd_pairs(e->g) ? 3 : e->g.sched == 0 ? 4 : e->g.sched;
 }
 
 int swd_engine_info(const swd_engine* e, swd_engine_info_t* info) {

@@ -131,8 +131,9 @@ void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
     g.n_strips = (g.NX - 2 + kWarpOut - 1) / kWarpOut;
     if (chunk_rows <= 0) {
       // about 5 waves of warps (148 SMs x 28 resident warps): short chunks keep more rows in
-      // flight and every SM busy through the tail of a step; 96 shots of 132 x 660 -> 11 rows
-      const long target = 148L * 28 * 5;
+      // flight and every SM busy through the tail of a step; 96 shots of 132 x 660 -> 13 rows.
+      // Two-step launches recompute rows at each chunk edge and take half as many waves (26 rows).
+      const long target = g.pairs ? 148L * 28 * 5 / 2 : 148L * 28 * 5;
       const long per = (long)g.n_strips * n_shots;
       int nch = (int)((target + per - 1) / per);
       nch = std::max(1, std::min(nch, std::max(1, rows / 8)));

@@ -58,6 +58,10 @@ def test_modes_are_bit_identical(tiny_case):
     for kw in ({"snapshot_mode": 1}, {"snapshot_mode": 2, "ckpt_interval": 20}, {"snapshot_mode": 1, "max_batch": 1},
                {"snapshot_mode": 2},  # memory-optimal checkpoint interval
                {"snapshot_mode": 1, "use_graphs": False, "chunk_rows": 3},
+               # two barriers per row (shared-memory ring), shapes and ring depths
+               {"snapshot_mode": 1, "fd_schedule": 4}, {"snapshot_mode": 2, "ckpt_interval": 20, "fd_schedule": 4},
+               {"snapshot_mode": 1, "fd_schedule": 4, "warps": 1, "cells": 2, "chunk_rows": 3},
+               {"snapshot_mode": 1, "fd_schedule": 4, "warps": 2, "cells": 1, "ring_fwd": 6, "ring_adj": 8},
                # one barrier per row (velocities a row ahead): same bits in every mode and chunking
                {"snapshot_mode": 1, "fd_schedule": 1}, {"snapshot_mode": 2, "ckpt_interval": 20, "fd_schedule": 1},
                {"snapshot_mode": 1, "fd_schedule": 1, "chunk_rows": 3},
@@ -85,11 +89,11 @@ def test_modes_are_bit_identical(tiny_case):
             assert np.array_equal(o[k], outs[0][k]), k
 
 
-@pytest.mark.parametrize("sched", [1, 2, 3])
+@pytest.mark.parametrize("sched", [1, 2, 3, 4])
 def test_other_schedules_on_the_plain_survey_match_the_oracle(O, sched):
-    """The one-barrier (1), warp-streaming (2) and two-steps-per-launch (3) schedules against the
-    oracle on the 30 x 120 survey (source near the top, receivers on the free-surface row,
-    several chunks)."""
+    """The one-barrier (1), warp-streaming (2), two-steps-per-launch (3, the default) and
+    two-barrier (4) schedules against the oracle on the 30 x 120 survey (source near the top,
+    receivers on the free-surface row, several chunks)."""
     s = configs.plain_c1(ns=3, nt=1000)
     cr0_r, cr0_l = O.observed_curves(s, s.vs_true)
     ref = O.gradient(s, s.vs, cr0_r, cr0_l)
