@@ -66,6 +66,8 @@ def parse():
     p.add_argument("--cells", type=int, default=0)
     p.add_argument("--ring", type=int, default=0)
     p.add_argument("--chunk", type=int, default=0)
+    p.add_argument("--image-precision", choices=["fp64", "fp32"], default="fp64",
+                   help="per-shot imaging sums: fp64 (default) or fp32 as the reference accumulates them")
     p.add_argument("--sched", type=int, default=-1,
                    help="FD schedule: 0 or 3 warp streaming, two steps per launch; 1 one barrier per row; "
                         "2 warp streaming, one step; 4 two barriers per row (-1: autotuned)")
@@ -489,7 +491,7 @@ def main():
     sg = ShardedGradient(s, world, rank, device=local, snapshot_mode=args.snapshot_mode,
                          ckpt_interval=args.ckpt, warps=args.warps, cells=args.cells, ring_fwd=args.ring,
                          ring_adj=args.ring, chunk_rows=args.chunk, autotune=tune,
-                         fd_schedule=max(args.sched, 0))
+                         fd_schedule=max(args.sched, 0), image_precision=args.image_precision)
     eng = sg.engine
     info = eng.info
     # observed curves of the "true" model (setup, SWD.m:155-162), then resident inputs
@@ -607,7 +609,7 @@ def main():
                 info["mode"]], "batch": info["batch"], "engine_bytes": info["bytes"],
                 "fd_variant": {k: info[k] for k in ("fd_schedule", "warps", "cells", "ring_fwd", "ring_adj",
                                                     "chunk_rows")} |
-                {"autotuned": tune},
+                {"autotuned": tune}, "image_sums": args.image_precision,
                 "parallelism": f"{s.ns} shots split round-robin over {world} GPU(s), one FP64 all-reduce of "
                                f"the shot sums per step", "shots_this_rank": nloc}),
             "e2e": {"value": s.ns / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,

@@ -70,6 +70,7 @@ struct AdjArgs {
   const T* res;                       // adjoint source [shot][nt][ng]
   const T* snap;                      // forward strain snapshots [shot][nrec][NF][nz][nx]
   double* img;                        // [shot][cl,cm,illum][nz][nx]
+  float* img32;                       // when set: FP32 images (as the reference accumulates), img unused
   T dtx, dt;
   int rec0;                           // snapshot it/nt_wf is read from index it/nt_wf - rec0
   int n_shots;

@@ -338,6 +338,7 @@ fd_adj_lead(AdjArgs<T> a, int it) {
   };
   const T* snap_b = IMG ? a.snap + ((size_t)shot * g.nrec + (it / g.nt_wf - a.rec0)) * NF * plane : nullptr;
   double* img_b = a.img + (size_t)shot * 3 * plane;
+  float* img_f = a.img32 ? a.img32 + (size_t)shot * 3 * plane : nullptr;  // FP32 images, as the reference
   struct Img { T fx, bz, sg; double c0, c1, c2; };
   auto load_img = [&](Img& m, int h, int z) {
     if (IMG && ximg[h] && z >= z_img0 && z < z_img1) {
@@ -348,7 +349,11 @@ fd_adj_lead(AdjArgs<T> a, int it) {
       } else {
         m.fx = s0[0]; m.bz = s0[plane]; m.sg = s0[2 * plane];
       }
-      m.c0 = img_b[cell]; m.c1 = img_b[plane + cell]; m.c2 = img_b[2 * plane + cell];
+      if (img_f) {
+        m.c0 = img_f[cell]; m.c1 = img_f[plane + cell]; m.c2 = img_f[2 * plane + cell];
+      } else {
+        m.c0 = img_b[cell]; m.c1 = img_b[plane + cell]; m.c2 = img_b[2 * plane + cell];
+      }
     }
   };
 
@@ -451,9 +456,15 @@ fd_adj_lead(AdjArgs<T> a, int it) {
           const T tcl = Fs * (xxn + zzn);
           const T tcm = T(2) * ((xxn * fx + zzn * bz) + T(0.5) * (xzn * sg));
           const T til = Fs * Fs;
-          img_b[cell] = im_c[h].c0 + (double)tcl;
-          img_b[plane + cell] = im_c[h].c1 + (double)tcm;
-          img_b[2 * plane + cell] = im_c[h].c2 + (double)til;
+          if (img_f) {  // accumulate in FP32 like the reference
+            img_f[cell] = (float)((T)(im_c[h].c0) + tcl);
+            img_f[plane + cell] = (float)((T)(im_c[h].c1) + tcm);
+            img_f[2 * plane + cell] = (float)((T)(im_c[h].c2) + til);
+          } else {
+            img_b[cell] = im_c[h].c0 + (double)tcl;
+            img_b[plane + cell] = im_c[h].c1 + (double)tcm;
+            img_b[2 * plane + cell] = im_c[h].c2 + (double)til;
+          }
         }
       }
       wn_prev[h] = wn_cur[h];

@@ -490,6 +490,7 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp(AdjArgs<float> a, int it)
   const bool ximg = own && x >= g.nbc && x < g.nbc + g.nx;
   const T* snap_b = IMG ? a.snap + ((size_t)shot * g.nrec + (it / g.nt_wf - a.rec0)) * 3 * plane : nullptr;
   double* img_b = a.img + (size_t)shot * 3 * plane;
+  float* img_f = a.img32 ? a.img32 + (size_t)shot * 3 * plane : nullptr;  // FP32 images, as the reference
   auto bz = [&](int z) -> T { return z == g.pad_top ? T(2) * dtx : dtx; };
   // material*stress products of a row: ca*xx, cl*zz, cm1*xz, cl*xx, ca*zz
   struct Prod { T p1, p2, p3, q1, q2; };
@@ -502,7 +503,11 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp(AdjArgs<float> a, int it)
       const size_t cell = (size_t)(z - z_img0) * g.nx + (x - g.nbc);
       const T* s0 = snap_b + cell;
       m.fx = s0[0]; m.bz = s0[plane]; m.sg = s0[2 * plane];
-      m.c0 = img_b[cell]; m.c1 = img_b[plane + cell]; m.c2 = img_b[2 * plane + cell];
+      if (img_f) {
+        m.c0 = img_f[cell]; m.c1 = img_f[plane + cell]; m.c2 = img_f[2 * plane + cell];
+      } else {
+        m.c0 = img_b[cell]; m.c1 = img_b[plane + cell]; m.c2 = img_b[2 * plane + cell];
+      }
     }
   };
   // new ww at row k (rows r0 = k, r1 = k+1, products q0 / q1, p3 of row k at x+1)
@@ -566,9 +571,15 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp(AdjArgs<float> a, int it)
         const T tcl = Fs * (xxn + zzn);
         const T tcm = T(2) * ((xxn * fx + zzn * bzv) + T(0.5) * (xzn * sg));
         const T til = Fs * Fs;
-        img_b[cell] = im_c.c0 + (double)tcl;
-        img_b[plane + cell] = im_c.c1 + (double)tcm;
-        img_b[2 * plane + cell] = im_c.c2 + (double)til;
+        if (img_f) {  // accumulate in FP32 like the reference
+          img_f[cell] = (float)((T)(im_c.c0) + tcl);
+          img_f[plane + cell] = (float)((T)(im_c.c1) + tcm);
+          img_f[2 * plane + cell] = (float)((T)(im_c.c2) + til);
+        } else {
+          img_b[cell] = im_c.c0 + (double)tcl;
+          img_b[plane + cell] = im_c.c1 + (double)tcm;
+          img_b[2 * plane + cell] = im_c.c2 + (double)til;
+        }
       }
     }
     wn_prev = wn;
@@ -638,6 +649,7 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
   const T* snap_b = IMGSUB >= 0 ? a.snap + ((size_t)shot * g.nrec + ((it - (IMGSUB > 0 ? 1 : 0)) / g.nt_wf - a.rec0)) *
                                                3 * plane : nullptr;
   double* img_b = a.img + (size_t)shot * 3 * plane;
+  float* img_f = a.img32 ? a.img32 + (size_t)shot * 3 * plane : nullptr;  // FP32 images, as the reference
   auto bz = [&](int z) -> T { return z == g.pad_top ? T(2) * dtx : dtx; };
   auto rowin = [&](int z) { return z >= 1 && z <= g.NZ - 2; };
   struct St { T uu, ww, xx, zz, xz; };
@@ -652,7 +664,11 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
       const size_t cell = (size_t)(z - z_img0) * g.nx + (x - g.nbc);
       const T* s0 = snap_b + cell;
       m.fx = s0[0]; m.bz = s0[plane]; m.sg = s0[2 * plane];
-      m.c0 = img_b[cell]; m.c1 = img_b[plane + cell]; m.c2 = img_b[2 * plane + cell];
+      if (img_f) {
+        m.c0 = img_f[cell]; m.c1 = img_f[plane + cell]; m.c2 = img_f[2 * plane + cell];
+      } else {
+        m.c0 = img_b[cell]; m.c1 = img_b[plane + cell]; m.c2 = img_b[2 * plane + cell];
+      }
     }
   };
   auto image = [&](const Img& m, const St& r, int z) {  // imaging condition (:274-279)
@@ -662,9 +678,15 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
       const T tcl = Fs * (r.xx + r.zz);
       const T tcm = T(2) * ((r.xx * m.fx + r.zz * m.bz) + T(0.5) * (r.xz * m.sg));
       const T til = Fs * Fs;
-      img_b[cell] = m.c0 + (double)tcl;
-      img_b[plane + cell] = m.c1 + (double)tcm;
-      img_b[2 * plane + cell] = m.c2 + (double)til;
+      if (img_f) {  // accumulate in FP32 like the reference
+        img_f[cell] = (float)((T)(m.c0) + tcl);
+        img_f[plane + cell] = (float)((T)(m.c1) + tcm);
+        img_f[2 * plane + cell] = (float)((T)(m.c2) + til);
+      } else {
+        img_b[cell] = m.c0 + (double)tcl;
+        img_b[plane + cell] = m.c1 + (double)tcm;
+        img_b[2 * plane + cell] = m.c2 + (double)til;
+      }
     }
   };
   // One row k of one adjoint step on rows R0 = k (materials m0, products Q0) and R1 = k+1

@@ -37,7 +37,7 @@ class EngineOpts(ctypes.Structure):
     _fields_ = [("hbm_budget", ctypes.c_size_t), ("max_batch", _i), ("snapshot_mode", _i), ("ckpt_interval", _i),
                 ("use_graphs", _i), ("chunk_rows", _i), ("device", _i), ("warps", _i), ("cells", _i),
                 ("ring_fwd", _i), ("ring_adj", _i), ("autotune", _i), ("radon_precision", _i),
-                ("fd_schedule", _i), ("adjoint_weight", _i)]
+                ("fd_schedule", _i), ("adjoint_weight", _i), ("image_precision", _i)]
 
 
 class EngineInfo(ctypes.Structure):
@@ -117,14 +117,15 @@ class GradientEngine:
 
     def __init__(self, survey, hbm_budget=0, max_batch=0, snapshot_mode=0, ckpt_interval=0, use_graphs=True,
                  chunk_rows=0, device=0, source=None, warps=0, cells=0, ring_fwd=0, ring_adj=0, autotune=False,
-                 radon_precision="fp64", fd_schedule=0, adjoint_weight="softmax"):
+                 radon_precision="fp64", fd_schedule=0, adjoint_weight="softmax", image_precision="fp64"):
         L = _bind()
         self.survey = survey
         self._sc = survey_struct(survey)
         opts = EngineOpts(int(hbm_budget), int(max_batch), int(snapshot_mode), int(ckpt_interval), int(use_graphs),
                           int(chunk_rows), int(device), int(warps), int(cells), int(ring_fwd),
                           int(ring_adj), int(bool(autotune)), _RPREC[radon_precision], int(fd_schedule),
-                          {"softmax": 0, "gauss": 1, "wd": 2}[adjoint_weight])
+                          {"softmax": 0, "gauss": 1, "wd": 2}[adjoint_weight],
+                          {"fp64": 0, "fp32": 1}[image_precision])
         h = ctypes.c_void_p()
         call("swd_engine_create", ctypes.byref(self._sc), ctypes.byref(opts), ctypes.byref(h))
         self._h = h

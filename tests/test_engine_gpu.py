@@ -225,3 +225,18 @@ def test_wd_adjoint_source_matches_oracle(tiny_case):
     assert np.array_equal(out["cr_pre_r"], ref["cr_pre_r"])
     for k in ("g_cl", "g_cm", "g_illum", "dk_vs"):
         assert _rel(out[k], ref[k]) < TOL, k
+
+
+@pytest.mark.parametrize("sched,mode", [(0, 1), (0, 2), (4, 1)])
+def test_fp32_images_match_the_reference_accumulation(O, tiny_case, sched, mode):
+    """image_precision='fp32' sums each shot's imaging terms in FP32, as the reference's MEX
+    does; against the oracle's FP32-accumulating shot loop the shot sums come out identical."""
+    s, cr0_r, cr0_l, _ = tiny_case
+    ref = O.gradient(s, s.vs, cr0_r, cr0_l, accum_fp64=False)
+    with GradientEngine(s, image_precision="fp32", fd_schedule=sched, snapshot_mode=mode, ckpt_interval=35) as e:
+        e.set_observed(cr0_r, cr0_l)
+        out = e.gradient(s.vp, s.vs)
+    assert np.array_equal(out["cr_pre_r"], ref["cr_pre_r"])
+    for k in ("g_cl", "g_cm", "g_illum"):
+        assert np.array_equal(out[k], ref[k]), k
+    assert _rel(out["dk_vs"], ref["dk_vs"]) < 1e-12
