@@ -746,6 +746,9 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
               i + 1, e->sz[i], e->sx[i]);
   }
   e->plane = (size_t)g.nz * g.nx;
+  // the warp-streaming kernels index a shot's fields and images with 32-bit offsets
+  SWD_CHECK(5.0 * (double)g.field < 2147483647.0 && 3.0 * (double)e->plane < 2147483647.0,
+            "grid too large: 5 * nzbc * pitch and 3 * nz * nx must stay below 2^31");
   g.warps = e->opt.warps;
   g.cells = e->opt.cells;
   g.ring_fwd = e->opt.ring_fwd;

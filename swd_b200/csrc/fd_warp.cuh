@@ -67,7 +67,7 @@ struct WStage {
   // reach border columns, which are never updated or written.
   __device__ __forceinline__ void issue(int slot, int z) const {
     if (z <= zmax) {
-      const size_t o = (size_t)max(z, 0) * pitch;
+      const int o = max(z, 0) * pitch;  // 32-bit: the engine keeps 5 * NZ * pitch below 2^31
       WSlot& s = slots[slot];
       wcp16(&s.q[lane], q + o);
       wcp16(&s.m[lane], mat + o);
@@ -215,7 +215,7 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp(FwdArgs<float> a, int it)
     const T xzn = te * R0.xz + (cm1 * (fuz + bwx)) * dtx;
     if (SLOW && k == g.pad_top) zzn = T(0);
     if (own) {
-      const size_t o = (size_t)k * g.pitch;
+      const int o = k * g.pitch;
       oq[o] = make_float4(un_cur, wn, xxn, zzn);
       oxz[o] = xzn;
     }
@@ -225,7 +225,7 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp(FwdArgs<float> a, int it)
       if (a.seis_u) a.seis_u[r] = un_cur;
     }
     if (SNAP && snapc && k >= z_img0 && k < z_img1) {  // :346-351 (the adjoint needs fux, bwz, fuz+bwx)
-      T* s0 = snap_base + ((size_t)(k - z_img0) * g.nx + (x - g.nbc));
+      T* s0 = snap_base + ((k - z_img0) * g.nx + (x - g.nbc));
       s0[0] = fux;
       s0[plane] = bwz;
       s0[2 * plane] = fuz + bwx;
@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it
       if (a.seis_u) a.seis_u[r] = T1[c1].uu;
     }
     if (SNAPSUB == 0 && snapc && k1 >= z_img0 && k1 < z_img1 && k1 >= zs && k1 < ze) {
-      T* s0 = snap_base + ((size_t)(k1 - z_img0) * g.nx + (x - g.nbc));
+      T* s0 = snap_base + ((k1 - z_img0) * g.nx + (x - g.nbc));
       s0[0] = sn.fux;
       s0[plane] = sn.bwz;
       s0[2 * plane] = sn.sg;
@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it
     Strain sn;
     const St r = one(slow_tag, T1[c1 ^ 1], MT[c1 ^ 1], T1[c1], MT[c1].x, j, sv2, wn2, un2, sn);
     if (own) {
-      const size_t o = (size_t)j * g.pitch;
+      const int o = j * g.pitch;
       oq[o] = make_float4(r.uu, r.ww, r.xx, r.zz);
       oxz[o] = r.xz;
     }
@@ -418,7 +418,7 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it
       if (a.seis_u) a.seis_u[rr] = r.uu;
     }
     if (SNAPSUB == 1 && snapc && j >= z_img0 && j < z_img1) {
-      T* s0 = snap_base + ((size_t)(j - z_img0) * g.nx + (x - g.nbc));
+      T* s0 = snap_base + ((j - z_img0) * g.nx + (x - g.nbc));
       s0[0] = sn.fux;
       s0[plane] = sn.bwz;
       s0[2 * plane] = sn.sg;
@@ -500,7 +500,7 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp(AdjArgs<float> a, int it)
   struct Img { T fx, bz, sg; double c0, c1, c2; };
   auto load_img = [&](Img& m, int z) {
     if (IMG && ximg && z >= z_img0 && z < z_img1 && z < ze) {
-      const size_t cell = (size_t)(z - z_img0) * g.nx + (x - g.nbc);
+      const int cell = (z - z_img0) * g.nx + (x - g.nbc);
       const T* s0 = snap_b + cell;
       m.fx = s0[0]; m.bz = s0[plane]; m.sg = s0[2 * plane];
       if (img_f) {
@@ -561,11 +561,11 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp(AdjArgs<float> a, int it)
     const T xzn = (te * R0.xz - dtx * (un_next - un_cur)) - dtx * (wn - wn_l);
     if (SLOW && k == g.pad_top) zzn = T(0);
     if (own) {
-      const size_t o = (size_t)k * g.pitch;
+      const int o = k * g.pitch;
       oq[o] = make_float4(un_cur, wn, xxn, zzn);
       oxz[o] = xzn;
       if (IMG && ximg && k >= z_img0 && k < z_img1) {  // imaging condition (:274-279)
-        const size_t cell = (size_t)(k - z_img0) * g.nx + (x - g.nbc);
+        const int cell = (k - z_img0) * g.nx + (x - g.nbc);
         const T fx = im_c.fx, bzv = im_c.bz, sg = im_c.sg;
         const T Fs = fx + bzv;
         const T tcl = Fs * (xxn + zzn);
@@ -661,7 +661,7 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
   auto img_row = [&](int z) { return IMGSUB >= 0 && z >= z_img0 && z < z_img1 && z >= zs && z < ze; };
   auto load_img = [&](Img& m, int z) {
     if (ximg && img_row(z)) {
-      const size_t cell = (size_t)(z - z_img0) * g.nx + (x - g.nbc);
+      const int cell = (z - z_img0) * g.nx + (x - g.nbc);
       const T* s0 = snap_b + cell;
       m.fx = s0[0]; m.bz = s0[plane]; m.sg = s0[2 * plane];
       if (img_f) {
@@ -673,7 +673,7 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
   };
   auto image = [&](const Img& m, const St& r, int z) {  // imaging condition (:274-279)
     if (ximg && img_row(z)) {
-      const size_t cell = (size_t)(z - z_img0) * g.nx + (x - g.nbc);
+      const int cell = (z - z_img0) * g.nx + (x - g.nbc);
       const T Fs = m.fx + m.bz;
       const T tcl = Fs * (r.xx + r.zz);
       const T tcm = T(2) * ((r.xx * m.fx + r.zz * m.bz) + T(0.5) * (r.xz * m.sg));
@@ -760,7 +760,7 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
   auto second = [&](auto slow_tag, int c1, int j) {
     const St r = one(slow_tag, T1[c1 ^ 1], MT[c1 ^ 1], QT[c1 ^ 1], T1[c1], MT[c1].x, QT[c1], j, inj2, wn2, un2);
     if (own) {
-      const size_t o = (size_t)j * g.pitch;
+      const int o = j * g.pitch;
       oq[o] = make_float4(r.uu, r.ww, r.xx, r.zz);
       oxz[o] = r.xz;
     }
