@@ -257,7 +257,7 @@ static int fwd_warp2_impl(const FwdArgs<float>& a, int it, cudaStream_t st) {
 }
 template <int NW, int NS, int IS>
 static int adj_warp2_launch(const AdjArgs<float>& a0, int it, cudaStream_t st) {
-  constexpr size_t smem = warp_smem_bytes<NW, NS>();
+  constexpr size_t smem = IS >= 0 ? warp_img_smem_bytes<NW, NS>() : warp_smem_bytes<NW, NS>();
   static int ready = set_smem(fd_adj_warp2<NW, NS, IS>, smem);
   if (ready != SWD_OK) return ready;
   AdjArgs<float> a = a0;

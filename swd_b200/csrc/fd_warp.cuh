@@ -41,8 +41,18 @@ struct WSlot {
   float xz[32];
 };
 
+// The imaging operands of one row of a warp's 32 columns: the forward strains (fux, bwz,
+// fuz+bwx) and the three image sums (FP64, or FP32 in the first half of each c row).
+struct WImgSlot {
+  float fx[32], bz[32], sg[32];
+  double c[3][32];
+};
+
 template <int NW, int NS>
 constexpr size_t warp_smem_bytes() { return (size_t)NW * NS * sizeof(WSlot); }
+// two-step adjoint launches that image stage the imaging operands beside the rows
+template <int NW, int NS>
+constexpr size_t warp_img_smem_bytes() { return (size_t)NW * NS * (sizeof(WSlot) + sizeof(WImgSlot)); }
 
 __device__ __forceinline__ void wcp16(void* dst, const void* src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
@@ -50,6 +60,10 @@ __device__ __forceinline__ void wcp16(void* dst, const void* src) {
 }
 __device__ __forceinline__ void wcp4(void* dst, const void* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src) : "memory");
+}
+__device__ __forceinline__ void wcp8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
                "l"(src) : "memory");
 }
 __device__ __forceinline__ void wcp_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
@@ -659,16 +673,36 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
   };
   struct Img { T fx, bz, sg; double c0, c1, c2; };
   auto img_row = [&](int z) { return IMGSUB >= 0 && z >= z_img0 && z < z_img1 && z >= zs && z < ze; };
-  auto load_img = [&](Img& m, int z) {
-    if (ximg && img_row(z)) {
+  // Imaging operands are staged by cp.async beside the state rows (same slot, same copy group),
+  // so their DRAM latency hides behind the rows in flight instead of costing registers.
+  WImgSlot* islots = reinterpret_cast<WImgSlot*>(wsmem + (size_t)NW * NS * sizeof(WSlot)) + (threadIdx.x >> 5) * NS;
+  auto issue_img = [&](int slot, int z) {
+    if (IMGSUB >= 0 && ximg && img_row(z)) {
       const int cell = (z - z_img0) * g.nx + (x - g.nbc);
-      const T* s0 = snap_b + cell;
-      m.fx = s0[0]; m.bz = s0[plane]; m.sg = s0[2 * plane];
-      if (img_f) {
-        m.c0 = img_f[cell]; m.c1 = img_f[plane + cell]; m.c2 = img_f[2 * plane + cell];
-      } else {
-        m.c0 = img_b[cell]; m.c1 = img_b[plane + cell]; m.c2 = img_b[2 * plane + cell];
+      WImgSlot& s = islots[slot];
+      wcp4(&s.fx[lane], snap_b + cell);
+      wcp4(&s.bz[lane], snap_b + plane + cell);
+      wcp4(&s.sg[lane], snap_b + 2 * plane + cell);
+#pragma unroll
+      for (int i = 0; i < 3; ++i) {
+        if (img_f) wcp4(reinterpret_cast<float*>(s.c[i]) + lane, img_f + i * plane + cell);
+        else wcp8(&s.c[i][lane], img_b + i * plane + cell);
       }
+    }
+  };
+  auto read_img = [&](Img& m, int slot) {
+    const WImgSlot& s = islots[slot];
+    m.fx = s.fx[lane];
+    m.bz = s.bz[lane];
+    m.sg = s.sg[lane];
+    if (img_f) {
+      m.c0 = reinterpret_cast<const float*>(s.c[0])[lane];
+      m.c1 = reinterpret_cast<const float*>(s.c[1])[lane];
+      m.c2 = reinterpret_cast<const float*>(s.c[2])[lane];
+    } else {
+      m.c0 = s.c[0][lane];
+      m.c1 = s.c[1][lane];
+      m.c2 = s.c[2][lane];
     }
   };
   auto image = [&](const Img& m, const St& r, int z) {  // imaging condition (:274-279)
@@ -717,7 +751,10 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
 
   // state rows staged from zs-2: row r in slot (r - zs + 2) % NS and RR[(r - zs) & 1]
 #pragma unroll
-  for (int u = 0; u < NS; ++u) ld.issue(u, zs - 2 + u);
+  for (int u = 0; u < NS; ++u) {
+    issue_img(u, zs - 2 + u);
+    ld.issue(u, zs - 2 + u);
+  }
   wcp_wait<NS - 2>();
   WRow RR[2];
   ld.read(RR[0], 0);
@@ -738,10 +775,13 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
   St T1[2];      // S1 rows, T1[(r - zs + 1) & 1]
   float4 MT[2];  // their materials
   Prod QT[2];    // their products
-  Img IM[2] = {};  // imaging operands of row r in IM[(r - zs) & 1]
+  Img IMp{};  // imaging operands of the second step's row (read before its slot is restaged)
   T wn2, un2;    // second step: new ww of row k1-2, new uu of row k1-1
   // first-step row k1 (slot and register bookkeeping as in fd_fwd_warp2)
-  auto first = [&](auto slow_tag, int c0, int s1, int spf, int c1, int k1) {
+  // s0: slot of state row k1 (its imaging operands when step it images)
+  auto first = [&](auto slow_tag, int c0, int s0, int s1, int spf, int c1, int k1) {
+    if (IMGSUB == 1) read_img(IMp, spf);  // row k1-1, which the second step images next
+    issue_img(spf, k1 + NS - 1);
     ld.issue(spf, k1 + NS - 1);
     wcp_wait<NS - 2>();
     ld.read(RR[c0 ^ 1], s1);
@@ -751,9 +791,10 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
     T1[c1] = one(slow_tag, as_st(R0), R0.m, QR[c0], as_st(R1), R1.m.x, QR[c0 ^ 1], k1, inj1, wn1, un1);
     MT[c1] = R0.m;
     QT[c1] = prod(T1[c1], R0.m);
-    if (IMGSUB == 0) {  // row k1's operands in IM[c1 ^ 1], row k1+1's go to IM[c1]
-      load_img(IM[c1], k1 + 1);
-      image(IM[c1 ^ 1], T1[c1], k1);
+    if (IMGSUB == 0) {
+      Img m;
+      read_img(m, s0);
+      image(m, T1[c1], k1);
     }
   };
   // second-step row j = k1-1 from S1 rows T1[c1^1] (j) and T1[c1] (k1); writes the new state
@@ -764,14 +805,11 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
       oq[o] = make_float4(r.uu, r.ww, r.xx, r.zz);
       oxz[o] = r.xz;
     }
-    if (IMGSUB == 1) {  // row j's operands in IM[c1], row j+1's go to IM[c1 ^ 1]
-      load_img(IM[c1 ^ 1], j + 1);
-      image(IM[c1], r, j);
-    }
+    if (IMGSUB == 1) image(IMp, r, j);
   };
   auto slow1 = [&](int k) { return k <= 1 || k >= g.NZ - 2 || k == g.pad_top || k == g.gz; };
-  first(std::true_type{}, 1, 2 % NS, 0, 0, zs - 1);
-  first(std::true_type{}, 0, 3 % NS, 1, 1, zs);
+  first(std::true_type{}, 1, 1, 2 % NS, 0, 0, zs - 1);
+  first(std::true_type{}, 0, 2 % NS, 3 % NS, 1, 1, zs);
   {
     const St& A = T1[0];
     const St& B = T1[1];
@@ -783,9 +821,8 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
     const T p1l = shfl_l(QT[1].p1), p2l = shfl_l(QT[1].p2);
     un2 = adj_vel_u(xint, B.uu, QT[1].p1, p1l, QT[1].p2, p2l, QT[1].p3, QT[0].p3, MT[1].x, bz(zs));
   }
-  if (IMGSUB == 1) load_img(IM[0], zs);
   auto both = [&](auto slow_tag, int u, int k1) {
-    first(slow_tag, (u + 1) & 1, (u + 4) % NS, (u + 2) % NS, u & 1, k1);
+    first(slow_tag, (u + 1) & 1, (u + 3) % NS, (u + 4) % NS, (u + 2) % NS, u & 1, k1);
     second(slow_tag, u & 1, k1 - 1);
   };
   int k1 = zs + 1;
