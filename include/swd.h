@@ -159,6 +159,17 @@ int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_a
                  const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
                  double* a_data_res);
 
+/* Replaces ADWDgradlimband(...) (core/ADWDgradlimband.m:1-102, same arguments as ADWDgrad_1):
+ * the weights are mlr.^SoftArgNorm normalised by their column sum (its derivative weights
+ * SoftArgNorm*(mlr.^SoftArgNorm).^(SoftArgNorm-1) over the same sum), without the SoftArgNorm
+ * factor of ADWDgrad_1, and the adjoint spectrum is extended by linear ramps over the 25 bins
+ * below lf and above nf.  Needs lf >= 26.  The reference has no caller for it; with
+ * SoftArgNorm = 1e4 (SWD.m:114) mlr.^SoftArgNorm overflows there as it does here. */
+int swd_adwdgrad_limband(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
+                         const double* grad_output_r, const double* grad_output_l, const double* space_m,
+                         const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
+                         double* a_data_res);
+
 /* Replaces ADWDgrad_norm(...) (core/ADWDgrad_norm.m:1-102, same arguments as ADWDgrad_1):
  * the SoftMax weights are replaced by normpdf(1:np, cr, 16) around the picks
  * (core/paddingMl_norm.m:1-9).  cr_r / cr_l: npair, saveForBackward.cr_r / cr_l = cr_pre - vmin

@@ -6,7 +6,8 @@
  * holds the transform's parameters); a side the reference skips for this shot
  * (ADWDgrad_1.m:13, :46) is not read, as in the reference.  With SWD_ADWD_NORM set, the
  * structs also carry cr_r / cr_l (the picks minus vmin, SWD.m:178, :184), around which
- * ADWDgrad_norm.m weights the spectrum with normpdf(1:np, cr, 16).
+ * ADWDgrad_norm.m weights the spectrum with normpdf(1:np, cr, 16).  With SWD_ADWD_LIMBAND set,
+ * the call is ADWDgradlimband (core/ADWDgradlimband.m).
  */
 #include <math.h>
 #include <string.h>
@@ -77,10 +78,15 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
   plhs[0] = mxCreateDoubleMatrix((mwSize)nt, (mwSize)ng, mxREAL);
   if (!have_p) return; /* neither side runs: zeros(nt,ng) as the reference returns */
   const double* space = swd_in_double(prhs[11], "space_M", (size_t)np * npair);
+#ifndef SWD_ADWD_LIMBAND
+#define SWD_ADWD_LIMBAND 0
+#endif
   const int rc = SWD_ADWD_NORM ? swd_adwdgrad_norm(&p, ns, is, w, beta, go[0], go[1], space, mm[0], raw[0], cr[0],
                                                   mm[1], raw[1], cr[1], mxGetPr(plhs[0]))
-                               : swd_adwdgrad(&p, ns, is, w, beta, go[0], go[1], space, mm[0], raw[0], mm[1], raw[1],
-                                              mxGetPr(plhs[0]));
+                 : SWD_ADWD_LIMBAND ? swd_adwdgrad_limband(&p, ns, is, w, beta, go[0], go[1], space, mm[0], raw[0],
+                                                           mm[1], raw[1], mxGetPr(plhs[0]))
+                                    : swd_adwdgrad(&p, ns, is, w, beta, go[0], go[1], space, mm[0], raw[0], mm[1],
+                                                   raw[1], mxGetPr(plhs[0]));
   for (int s = 0; s < 2; ++s)
     if (mm[s]) mxFree(mm[s]);
   swd_mex_fail(rc, SWD_NAME);

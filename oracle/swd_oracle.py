@@ -563,21 +563,31 @@ def normpdf_cols(npv, cr):
     return np.exp(-0.5 * z * z) / (np.sqrt(2 * np.pi) * 16.0)
 
 
-def adwd_side(nt, ng, npair, soft_arg_norm, grad_output, save, side, a_data_res, cr=None):
+def adwd_side(nt, ng, npair, soft_arg_norm, grad_output, save, side, a_data_res, cr=None, limband=False):
     """One side of core/ADWDgrad_1.m:15-44 (right) / :47-77 (left), written into a_data_res.
-    cr given: ADWDgrad_norm.m:22-23, the weights are normpdf around cr = cr_pre - vmin."""
+    cr given: ADWDgrad_norm.m:22-23, the weights are normpdf around cr = cr_pre - vmin.
+    limband: core/ADWDgradlimband.m:13-53, power-normalised weights and the 25-bin ramps."""
     lf, nf, ccn = save["lf"], save["nf"], save["ccn"]
     pos = save["uxtpos"]
     noff = len(pos)
-    mlr = save["ml_raw"] ** (1.0 / 40.0)
-    E = softmax_cols(mlr * soft_arg_norm) if cr is None else normpdf_cols(mlr.shape[0], cr)
-    npv = E.shape[0]
-    space = np.arange(1, npv + 1, dtype=np.float64)[:, None]
     go = np.array(grad_output, np.float64).copy()
     go[go == 0] = 1
-    mean_s = (space * E).sum(axis=0, keepdims=True)
-    test3 = E * space - mean_s * E
-    gradml = test3 * 2 * go[None, :npair] * soft_arg_norm
+    if limband:  # ADWDgradlimband.m:20-31
+        P = save["ml_raw"] ** soft_arg_norm
+        P1 = soft_arg_norm * P ** (soft_arg_norm - 1)
+        S = P.sum(axis=0, keepdims=True)
+        N, N1 = P1 / S, P / S
+        space = np.arange(1, N.shape[0] + 1, dtype=np.float64)[:, None]
+        test3 = N * space - (space * N1).sum(axis=0, keepdims=True) * N
+        gradml = test3 * 2 * go[None, :npair] * 1
+    else:
+        mlr = save["ml_raw"] ** (1.0 / 40.0)
+        E = softmax_cols(mlr * soft_arg_norm) if cr is None else normpdf_cols(mlr.shape[0], cr)
+        npv = E.shape[0]
+        space = np.arange(1, npv + 1, dtype=np.float64)[:, None]
+        mean_s = (space * E).sum(axis=0, keepdims=True)
+        test3 = E * space - mean_s * E
+        gradml = test3 * 2 * go[None, :npair] * soft_arg_norm
     mm = save["mm"][:, lf - 1:nf]
     with np.errstate(invalid="ignore", divide="ignore"):
         ph = mm / np.abs(mm)
@@ -588,6 +598,14 @@ def adwd_side(nt, ng, npair, soft_arg_norm, grad_output, save, side, a_data_res,
     for j in range(lf, nf + 1):
         K = np.exp(1j * (th0 * (j - 1)))
         G[:, j - 1] = K.conj().T @ gm[:, j - lf]
+    if limband:  # ADWDgradlimband.m:41-48; ifft(.., ccn) drops columns past ccn
+        if lf - 25 < 1:
+            raise ValueError("ADWDgradlimband indexes column lf-25, which needs lf >= 26")
+        for i in range(lf - 25, lf + 1):
+            G[:, i - 1] = G[:, lf - 1] * ((i - lf + 25) / 25)
+        for i in range(nf, nf + 26):
+            if i <= ccn:
+                G[:, i - 1] = G[:, nf - 1] * ((nf - i + 25) / 25)
     g = np.real(np.fft.ifft(G, ccn, axis=1))[:, :nt]      # noff x nt
     if side == "r":
         a_data_res[:, [p - 1 for p in pos]] = g.T
@@ -685,6 +703,16 @@ def wd_direct(x, k_lo, fac, ntpad):
     X = E @ x
     d = (np.asarray(fac) - 1) * X
     return x + 2.0 / ntpad * np.real(d @ E.conj())
+
+
+def ADWDgradlimband(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, saver, savel):
+    """core/ADWDgradlimband.m:1-102."""
+    a = np.zeros((nt, ng))
+    if has_right(is_, ns, m, M, w):
+        adwd_side(nt, ng, npair, SoftArgNorm, grad_outputr, saver, "r", a, limband=True)
+    if has_left(is_, m, M, w):
+        adwd_side(nt, ng, npair, SoftArgNorm, grad_outputl, savel, "l", a, limband=True)
+    return a
 
 
 def has_right(is_, ns, m, M, w):

@@ -6,6 +6,7 @@
 // All gathers of a batch run in one launch per stage.  The DFT evaluates only
 // the bins lf..nf that the reference keeps; the Radon sum runs in double like
 // MATLAB; the SoftMax uses a max-shifted FP64 log-sum-exp.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -475,7 +476,8 @@ __global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const
                                                               const double* __restrict__ dc,
                                                               const double* __restrict__ space_m, double beta,
                                                               const double2* __restrict__ K, double2* Gx,
-                                                              const double* __restrict__ pick, double pick_off) {
+                                                              const double* __restrict__ pick, double pick_off,
+                                                              int limband) {
   extern __shared__ double2 sgm[];
   __shared__ double red[33];
   const int f = blockIdx.x, gi = blockIdx.y;
@@ -486,9 +488,15 @@ __global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const
   // Weights over p.  ADWDgrad_1.m:22-23: E = softmax(beta * mlr.^(1/40)), max-shifted in FP64.
   // ADWDgrad_norm.m:22-23 (pick != null): E = normpdf(1:np, cr, 16) around the pick cr =
   // cr_pre - vmin (paddingMl_norm.m:5-7), not normalised.
+  // ADWDgradlimband.m:20-24 (limband): P = mlr.^beta normalised by its column sum S; the
+  // derivative weights are N = beta*P.^(beta-1)/S, the mean is taken with N1 = P/S.
   double zmax = 0.0, se = 1.0, mu = 0.0;
   if (pick) {
     mu = pick[(size_t)gi * g.npair + f] - pick_off;
+  } else if (limband) {
+    se = 0.0;
+    for (int p = threadIdx.x; p < g.np; p += blockDim.x) se += pow(mr[p], beta);
+    se = block_sum(se, red);
   } else {
     zmax = -1.0 / 0.0;
     for (int p = threadIdx.x; p < g.np; p += blockDim.x) zmax = fmax(zmax, pow(mr[p], 1.0 / 40.0) * beta);
@@ -498,6 +506,7 @@ __global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const
     se = block_sum(se, red);
   }
   auto weight = [&](int p) -> double {
+    if (limband) return (beta * pow(pow(mr[p], beta), beta - 1.0)) / se;
     if (pick) {
       const double z = ((double)(p + 1) - mu) / 16.0;
       return exp(-0.5 * (z * z)) / (2.5066282746310002 * 16.0);  // sqrt(2*pi) * sigma
@@ -506,7 +515,7 @@ __global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const
   };
   double sm = 0.0;
   for (int p = threadIdx.x; p < g.np; p += blockDim.x) {
-    const double E = weight(p);
+    const double E = limband ? pow(mr[p], beta) / se : weight(p);  // N1 for limband
     const double s = space_m ? space_m[(size_t)f * g.np + p] : (double)(p + 1);
     sm += s * E;
   }
@@ -516,7 +525,7 @@ __global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const
   for (int p = threadIdx.x; p < g.np; p += blockDim.x) {
     const double E = weight(p);
     const double s = space_m ? space_m[(size_t)f * g.np + p] : (double)(p + 1);
-    const double gml = (((E * s - sm * E) * 2.0) * d) * beta;   // :28-31
+    const double gml = (((E * s - sm * E) * 2.0) * d) * (limband ? 1.0 : beta);   // :28-31 (limband :29-31)
     const double2 m = MM[col * g.np + p];
     const double mag = hypot(m.x, m.y);
     double2 ph = make_double2(m.x / mag, m.y / mag);              // :32-33
@@ -545,12 +554,13 @@ __global__ void __launch_bounds__(256) softmax_adjoint_kernel(RadonGeom g, const
 
 int softmax_adjoint(const RadonGeom& g, const Gather* d_gath, int G, const double* mlraw, const double2* MM,
                     const double* dc, const double* space_m, double beta, const double2* K, double2* Gx,
-                    cudaStream_t st, const double* pick, double pick_off) {
+                    cudaStream_t st, const double* pick, double pick_off, int limband) {
   dim3 grid(g.npair, G);
   const size_t smem = (size_t)g.np * sizeof(double2);
   if (smem > 48 * 1024)
     SWD_CUDA(cudaFuncSetAttribute(softmax_adjoint_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  softmax_adjoint_kernel<<<grid, 256, smem, st>>>(g, d_gath, mlraw, MM, dc, space_m, beta, K, Gx, pick, pick_off);
+  softmax_adjoint_kernel<<<grid, 256, smem, st>>>(g, d_gath, mlraw, MM, dc, space_m, beta, K, Gx, pick, pick_off,
+                                                  limband);
   count_launch(1);
   SWD_CUDA(cudaGetLastError());
   return SWD_OK;
@@ -560,9 +570,12 @@ int softmax_adjoint(const RadonGeom& g, const Gather* d_gath, int G, const doubl
 
 constexpr int kIdftT = 64;
 
+// TA / TB (nullable, [ntd]): sum_i w_i exp(+i th_i t) over the taper bins below lf / above nf
+// (ADWDgradlimband.m:41-48), which carry copies of the bins lf / nf scaled by w_i.
 template <typename O>
 __global__ void __launch_bounds__(256) idft_kernel(RadonGeom g, const Gather* gs, const double2* __restrict__ Gx,
-                                                   const double2* __restrict__ W, O* out, size_t ostride) {
+                                                   const double2* __restrict__ W, O* out, size_t ostride,
+                                                   const double2* __restrict__ TA, const double2* __restrict__ TB) {
   extern __shared__ double2 sg[];  // [npair][32]
   const Gather gg = gs[blockIdx.z];
   if (gg.valid <= 0) return;
@@ -590,27 +603,31 @@ __global__ void __launch_bounds__(256) idft_kernel(RadonGeom g, const Gather* gs
       const double2 v = sg[f * 32 + lane];
       acc += v.x * w.x + v.y * w.y;
     }
+    if (TA) {
+      const double2 vl = sg[lane], vn = sg[(g.npair - 1) * 32 + lane], a = TA[t], b = TB[t];
+      acc += (vl.x * a.x - vl.y * a.y) + (vn.x * b.x - vn.y * b.y);
+    }
     if (write) o[(size_t)t * g.ng + colx] = (O)(acc / inv);
   }
 }
 
 template <typename O>
 int radon_idft_scatter(const RadonGeom& g, const Gather* d_gath, int G, const double2* Gx, const double2* W, O* out,
-                       size_t ostride, cudaStream_t st) {
+                       size_t ostride, cudaStream_t st, const double2* TA, const double2* TB) {
   SWD_CHECK(g.ccn >= g.nt, "ADWDgrad_1 needs ccn = fix(1/df/dt) (%d) >= nt (%d)", g.ccn, g.nt);
   dim3 grid((g.nt + kIdftT - 1) / kIdftT, (g.offset + 31) / 32, G);
   const size_t smem = (size_t)g.npair * 32 * sizeof(double2);
   if (smem > 48 * 1024)
     SWD_CUDA(cudaFuncSetAttribute(idft_kernel<O>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  idft_kernel<O><<<grid, 256, smem, st>>>(g, d_gath, Gx, W, out, ostride);
+  idft_kernel<O><<<grid, 256, smem, st>>>(g, d_gath, Gx, W, out, ostride, TA, TB);
   count_launch(1);
   SWD_CUDA(cudaGetLastError());
   return SWD_OK;
 }
 template int radon_idft_scatter<float>(const RadonGeom&, const Gather*, int, const double2*, const double2*, float*,
-                                       size_t, cudaStream_t);
+                                       size_t, cudaStream_t, const double2*, const double2*);
 template int radon_idft_scatter<double>(const RadonGeom&, const Gather*, int, const double2*, const double2*,
-                                        double*, size_t, cudaStream_t);
+                                        double*, size_t, cudaStream_t, const double2*, const double2*);
 
 }  // namespace swd
 
@@ -710,15 +727,18 @@ int swd_pick(const double* ml, int np_, int npair, double vmin, const double* cr
 
 }  // extern "C"
 
-// ADWDgrad_1 (picks null) or ADWDgrad_norm (picks cr_r / cr_l) of one shot.
+// ADWDgrad_1 (mode 0), ADWDgrad_norm (mode 1, picks cr_r / cr_l) or ADWDgradlimband (mode 2) of one shot.
 static int adwdgrad_impl(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
                          const double* grad_output_r, const double* grad_output_l, const double* space_m,
                          const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
-                         const double* cr_r, const double* cr_l, bool gauss, double* a_data_res) {
+                         const double* cr_r, const double* cr_l, int mode, double* a_data_res) {
+  const bool gauss = mode == 1;
   RadonGeom g{};
   SWD_TRY(radon_geom(p, g));
   SWD_CHECK(a_data_res, "null a_data_res");
   SWD_CHECK(g.ccn >= g.nt, "ADWDgrad_1 needs ccn = fix(1/df/dt) (%d) >= nt (%d)", g.ccn, g.nt);
+  // ADWDgradlimband.m:41-48 writes bins lf-25 .. nf+25 (1-based); the first must exist
+  SWD_CHECK(mode != 2 || g.lf - 25 >= 1, "ADWDgradlimband needs lf - 25 >= 1 (lf = %d)", g.lf);
   Gather gg[2];
   const double* mm[2] = {mm_r, mm_l};
   const double* raw[2] = {ml_raw_r, ml_raw_l};
@@ -733,7 +753,7 @@ static int adwdgrad_impl(const swd_radon_params* p, int ns, int is, int w, doubl
     }
   }
   const size_t spec = (size_t)g.npair * g.np, nsz = (size_t)g.nt * g.ng;
-  DevBuf b_W, b_K, b_MM, b_raw, b_dc, b_sm, b_Gx, b_out, b_out_t, b_g, b_cr;
+  DevBuf b_W, b_K, b_MM, b_raw, b_dc, b_sm, b_Gx, b_out, b_out_t, b_g, b_cr, b_tab;
   if (gauss) SWD_TRY(b_cr.alloc(2 * (size_t)g.npair * sizeof(double)));
   SWD_TRY(b_W.alloc((size_t)g.npair * g.ntd * sizeof(double2)));
   SWD_TRY(b_K.alloc((size_t)g.npair * g.offset * g.np * sizeof(double2)));
@@ -746,6 +766,31 @@ static int adwdgrad_impl(const swd_radon_params* p, int ns, int is, int w, doubl
   SWD_TRY(b_g.alloc(2 * sizeof(Gather)));
   if (space_m) SWD_TRY(b_sm.alloc(spec * sizeof(double)));
   cudaStream_t st = 0;
+  if (mode == 2) {
+    // taper tables: bins i = lf-25 .. lf-1 carry bin lf times (i-lf+25)/25, bins nf+1 .. nf+25
+    // carry bin nf times (nf-i+25)/25; ifft(.., ccn) drops bins past ccn (ADWDgradlimband.m:41-50)
+    std::vector<double2> tab(2 * (size_t)g.ntd);
+    const double two_pi = 2.0 * 3.141592653589793;
+    for (int t = 0; t < g.ntd; ++t) {
+      double ar = 0, ai = 0, br = 0, bi = 0;
+      for (int i = g.lf - 25; i <= g.lf - 1; ++i) {
+        const double wgt = (double)(i - g.lf + 25) / 25.0;
+        const double th = two_pi * (double)(((long long)(i - 1) * t) % g.ccn) / (double)g.ccn;
+        ar += wgt * std::cos(th);
+        ai += wgt * std::sin(th);
+      }
+      for (int i = g.nf + 1; i <= std::min(g.nf + 25, g.ccn); ++i) {
+        const double wgt = (double)(g.nf - i + 25) / 25.0;
+        const double th = two_pi * (double)(((long long)(i - 1) * t) % g.ccn) / (double)g.ccn;
+        br += wgt * std::cos(th);
+        bi += wgt * std::sin(th);
+      }
+      tab[t] = make_double2(ar, ai);
+      tab[(size_t)g.ntd + t] = make_double2(br, bi);
+    }
+    SWD_TRY(b_tab.alloc(tab.size() * sizeof(double2)));
+    SWD_CUDA(cudaMemcpy(b_tab.p, tab.data(), tab.size() * sizeof(double2), cudaMemcpyHostToDevice));
+  }
   for (int s = 0; s < 2; ++s) {
     if (gg[s].valid != 1) continue;
     SWD_CUDA(cudaMemcpyAsync(b_MM.as<double2>() + s * spec, mm[s] + (size_t)(g.lf - 1) * g.np * 2,
@@ -765,9 +810,10 @@ static int adwdgrad_impl(const swd_radon_params* p, int ns, int is, int w, doubl
   SWD_TRY(radon_tables(g, b_W.as<double2>(), b_K.as<double2>(), st));
   SWD_TRY(softmax_adjoint(g, b_g.as<Gather>(), 2, b_raw.as<double>(), b_MM.as<double2>(), b_dc.as<double>(),
                           space_m ? b_sm.as<double>() : nullptr, soft_arg_norm, b_K.as<double2>(),
-                          b_Gx.as<double2>(), st, gauss ? b_cr.as<double>() : nullptr));
+                          b_Gx.as<double2>(), st, gauss ? b_cr.as<double>() : nullptr, 0.0, mode == 2));
   SWD_TRY(radon_idft_scatter<double>(g, b_g.as<Gather>(), 2, b_Gx.as<double2>(), b_W.as<double2>(),
-                                     b_out.as<double>(), 0, st));
+                                     b_out.as<double>(), 0, st, mode == 2 ? b_tab.as<double2>() : nullptr,
+                                     mode == 2 ? b_tab.as<double2>() + g.ntd : nullptr));
   // [nt][ng] -> MATLAB nt x ng
   SWD_TRY(transpose<double, double>(b_out.as<double>(), 0, b_out_t.as<double>(), 0, 1, g.nt, g.ng, st));
   SWD_CUDA(cudaMemcpyAsync(a_data_res, b_out_t.p, nsz * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -782,7 +828,16 @@ int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_a
                  const double* mm_l, const double* ml_raw_l, double* a_data_res) {
   clear_error();
   return adwdgrad_impl(p, ns, is, w, soft_arg_norm, grad_output_r, grad_output_l, space_m, mm_r, ml_raw_r, mm_l,
-                       ml_raw_l, nullptr, nullptr, false, a_data_res);
+                       ml_raw_l, nullptr, nullptr, 0, a_data_res);
+}
+
+int swd_adwdgrad_limband(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
+                         const double* grad_output_r, const double* grad_output_l, const double* space_m,
+                         const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
+                         double* a_data_res) {
+  clear_error();
+  return adwdgrad_impl(p, ns, is, w, soft_arg_norm, grad_output_r, grad_output_l, space_m, mm_r, ml_raw_r, mm_l,
+                       ml_raw_l, nullptr, nullptr, 2, a_data_res);
 }
 
 int swd_adwdgrad_norm(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
@@ -791,7 +846,7 @@ int swd_adwdgrad_norm(const swd_radon_params* p, int ns, int is, int w, double s
                       const double* ml_raw_l, const double* cr_l, double* a_data_res) {
   clear_error();
   return adwdgrad_impl(p, ns, is, w, soft_arg_norm, grad_output_r, grad_output_l, space_m, mm_r, ml_raw_r, mm_l,
-                       ml_raw_l, cr_r, cr_l, true, a_data_res);
+                       ml_raw_l, cr_r, cr_l, 1, a_data_res);
 }
 
 }  // extern "C"

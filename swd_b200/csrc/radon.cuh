@@ -49,13 +49,15 @@ int radon_amplitudes(const RadonGeom& g, const Gather* d_gath, int G, const doub
 int pick_batch(int np, int npair, int G, int ini, int method, double vmin, const Gather* d_gath, const double* ml,
                const double* cr0, double* cr_pre, double* dc, double* res, int* status, cudaStream_t st);
 // SoftMax gradient + adjoint Radon: Gx[g][f][x] = sum_p conj(K[f][x][p]) * gm[g][f][p];
-// with `pick` ([g][f]) the weights are ADWDgrad_norm's Gaussian around pick - pick_off (= cr_pre - vmin)
+// with `pick` ([g][f]) the weights are ADWDgrad_norm's Gaussian around pick - pick_off (= cr_pre - vmin);
+// with `limband` they are ADWDgradlimband's power weights, mlr.^beta normalised per column
 int softmax_adjoint(const RadonGeom& g, const Gather* d_gath, int G, const double* mlraw, const double2* MM,
                     const double* dc, const double* space_m, double beta, const double2* K, double2* Gx,
-                    cudaStream_t st, const double* pick = nullptr, double pick_off = 0.0);
+                    cudaStream_t st, const double* pick = nullptr, double pick_off = 0.0, int limband = 0);
 // real(ifft(Gx, ccn))(1:nt) written into out[shot][t][col] (right: all x; left: x >= 1), ADWDgrad_1.m:42-44, 76
 template <typename O>
 int radon_idft_scatter(const RadonGeom& g, const Gather* d_gath, int G, const double2* Gx, const double2* W, O* out,
-                       size_t ostride, cudaStream_t st);
+                       size_t ostride, cudaStream_t st,
+                       const double2* TA = nullptr, const double2* TB = nullptr);
 
 }  // namespace swd

@@ -4,6 +4,7 @@
     LHDispPick                  core/LHDispPick.m:2 (pickFDC1, core/pickFDC1.m:1)
     ADWDgrad_1                  core/ADWDgrad_1.m:1
     ADWDgrad_norm               core/ADWDgrad_norm.m:1
+    ADWDgradlimband             core/ADWDgradlimband.m:1
     weight_data_muti3           core/weight_data_muti3.m:1 (the WD adjoint source)
 
 Each call runs on the GPU through libswd.so (FP64, like the reference's MATLAB
@@ -94,6 +95,14 @@ def ADWDgrad_norm(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, gr
                      saveForBackwardr, saveForBackwardl)
 
 
+def ADWDgradlimband(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
+                    saveForBackwardr, saveForBackwardl):
+    """[a_data_res]=ADWDgradlimband(...) (core/ADWDgradlimband.m:1): power-normalised weights
+    mlr.^SoftArgNorm and a 25-bin linear ramp below lf and above nf of the adjoint spectrum."""
+    return _adwdgrad(2, nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
+                     saveForBackwardr, saveForBackwardl)
+
+
 def ADWDgrad_1(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
                saveForBackwardr, saveForBackwardl):
     """[a_data_res]=ADWDgrad_1(...) (core/ADWDgrad_1.m:1)."""
@@ -123,7 +132,10 @@ def _adwdgrad(gauss, nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr,
     mml, rawl, gl = side(sl, grad_outputl, "mll")
     spm = None if space_M is None else np.asfortranarray(np.asarray(space_M, np.float64))
     cp = lambda x: None if x is None else x.ctypes.data_as(dp)
-    if gauss:
+    if gauss == 2:
+        call("swd_adwdgrad_limband", ctypes.byref(p), int(ns), int(is_), int(w), float(SoftArgNorm), cp(gr), cp(gl),
+             cp(spm), cp(mmr), cp(rawr), cp(mml), cp(rawl), ptr(a))
+    elif gauss:
         def picks(sv, key):
             return None if sv is None else np.ascontiguousarray(np.asarray(sv[key], np.float64).reshape(-1))
         crr, crl = picks(sr, "cr_r"), picks(sl, "cr_l")

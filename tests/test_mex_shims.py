@@ -17,7 +17,7 @@ import mexsim  # noqa: E402
 from swd_b200 import configs  # noqa: E402
 
 SHIMS = ["eigen_staggerfd_single", "eigen_staggerfd_double", "eigen_e2drtm_single", "eigen_e2drtm_double",
-         "RTrAD", "RTlAD", "RTr", "RTl", "LHDispPick", "ADWDgrad_1", "ADWDgrad_norm",
+         "RTrAD", "RTlAD", "RTr", "RTl", "LHDispPick", "ADWDgrad_1", "ADWDgrad_norm", "ADWDgradlimband",
          "weight_data_muti3"]
 
 

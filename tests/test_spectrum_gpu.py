@@ -157,3 +157,29 @@ def test_adwdgrad_norm_matches_oracle(O, survey, shots):
                                gs["l"])
         assert np.abs(ref).max() > 0
         assert _rel(got, ref) < 1e-9, is_
+
+
+@pytest.mark.parametrize("beta", [1.0, 2.5])
+def test_adwdgrad_limband_matches_oracle(O, beta):
+    """ADWDgradlimband: power-normalised weights and the 25-bin ramps below lf and above nf.
+    fmin 30 Hz puts lf at 31 (the ramp needs lf >= 26); SoftArgNorm stays small, since the
+    reference's mlr.^SoftArgNorm overflows at SWD.m's 1e4."""
+    import dataclasses
+    s = dataclasses.replace(configs.plain_c1(), fmin=30.0)
+    rng = np.random.default_rng(9)
+    for is_ in (1, 6, 12):
+        seis = _seis(O, s, is_)
+        saves = {}
+        for side in ("r", "l"):
+            saves[side] = O.radon(seis, is_, s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.ng, s.ds, s.offset, s.m,
+                                  s.M, side, s.dv)[2]
+        npair = saves["r"]["nf"] - saves["r"]["lf"] + 1
+        gr = rng.integers(-3, 4, npair).astype(float)
+        gl = rng.integers(-3, 4, npair).astype(float)
+        ref = O.ADWDgradlimband(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, beta, gr, gl, saves["r"], saves["l"])
+        p = SP.radon_params(s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.nt, s.ng, s.ds, s.offset, s.m, s.M, s.dv)
+        gs = {k: {"mm": v["mm"], ("mlr" if k == "r" else "mll"): v["ml_raw"], "params": p} for k, v in saves.items()}
+        got = SP.ADWDgradlimband(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, beta, gr, gl, None, gs["r"], gs["l"])
+        assert np.abs(ref).max() > 0
+        assert _rel(got, ref) < 1e-9, is_
+

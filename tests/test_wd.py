@@ -89,3 +89,17 @@ def test_wd_on_a_modelled_gather(O):
         ref = O.weight_data_muti3(seis, *args[1:])
         got = SP.weight_data_muti3(*args)
         assert _rel(got, ref) < 1e-12, is_
+
+
+def test_adwdgrad_limband_rejects_low_lf():
+    """The reference's ramp indexes column lf-25: with lf below 26 it fails, and so does the call
+    (before any device work)."""
+    from swd_b200 import spectrum as SP
+    from swd_b200._lib import SwdError
+    s = configs.plain_c1()  # fmin 5 Hz: lf = 6
+    p = SP.radon_params(s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.nt, s.ng, s.ds, s.offset, s.m, s.M, s.dv)
+    npv, npair = s.np_vel, s.npair
+    gs = {"mm": np.zeros((npv, 61), complex), "mlr": np.ones((npv, npair)), "params": p}
+    with pytest.raises(SwdError, match="lf - 25"):
+        SP.ADWDgradlimband(s.nt, s.ng, s.ns, npair, 2, s.w, s.m, s.M, 1.0, np.ones(npair), np.ones(npair), None,
+                           gs, dict(gs, mll=gs["mlr"]))
