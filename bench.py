@@ -42,7 +42,7 @@ NCU_BYTES_PER_CELL_LAUNCH = {4: {"fd_fwd_step": 36.1, "fd_adj_step": 36.1},
 # Compulsory DRAM bytes of the fused one-sweep kernels: 5 state fields read + 5 written per
 # shot-cell and launch (a launch advances one step, or two under schedule 3; materials are
 # shared by the shots of a launch), plus per interior cell every nt_wf steps the 3-field
-# snapshot write (forward) or snapshot read + FP64 image update (adjoint).
+# snapshot write (forward) or snapshot read + image update (adjoint; FP32 or FP64 sums).
 COMPULSORY_STATE_B = 40
 
 
@@ -66,8 +66,8 @@ def parse():
     p.add_argument("--cells", type=int, default=0)
     p.add_argument("--ring", type=int, default=0)
     p.add_argument("--chunk", type=int, default=0)
-    p.add_argument("--image-precision", choices=["fp64", "fp32"], default="fp64",
-                   help="per-shot imaging sums: fp64 (default) or fp32 as the reference accumulates them")
+    p.add_argument("--image-precision", choices=["fp32", "fp64"], default="fp32",
+                   help="per-shot imaging sums: fp32 as the reference accumulates them (default) or fp64")
     p.add_argument("--sched", type=int, default=-1,
                    help="FD schedule: 0 or 3 warp streaming, two steps per launch; 1 one barrier per row; "
                         "2 warp streaming, one step; 4 two barriers per row (-1: autotuned)")
@@ -573,14 +573,15 @@ def main():
     nloc = sg.local.ns  # shots of this rank: one FD launch steps all of them
     cells = s.nzbc * s.nxbc * nloc
     inner = s.nz * s.nx * nloc
-    # algorithmic bytes per launch (one time step of every shot): the reference's two-phase
-    # schedule, 84 B per padded cell-step, plus 16 B snapshot write (forward) or 16 B snapshot
-    # read + 48 B FP64 image update (adjoint) per interior cell every nt_wf steps
+    # algorithmic bytes per time step of every shot: the reference's two-phase schedule, 84 B
+    # per padded cell-step, plus 16 B snapshot write (forward) or 16 B snapshot read + 24 B
+    # FP32 image update (adjoint) per interior cell every nt_wf steps; times the steps per launch
     spl = 2 if info["fd_schedule"] == 3 else 1  # time steps per launch
     fwd_bytes = spl * (cells * 84 + inner * 16 / s.nt_wf)
-    adj_bytes = spl * (cells * 84 + inner * (16 + 48) / s.nt_wf)
+    img_rmw = 24 if args.image_precision == "fp32" else 48  # 3 image sums read and written
+    adj_bytes = spl * (cells * 84 + inner * (16 + 24) / s.nt_wf)  # the reference's FP32 image sums
     fwd_comp = cells * COMPULSORY_STATE_B + spl * inner * 12 / s.nt_wf
-    adj_comp = cells * COMPULSORY_STATE_B + spl * inner * (12 + 48) / s.nt_wf
+    adj_comp = cells * COMPULSORY_STATE_B + spl * inner * (12 + img_rmw) / s.nt_wf
     fwd_launch_ms = fwd_ms / s.nt * spl
     # checkpoint mode: the adjoint phase also re-runs the forward steps segment by segment
     adj_launch_ms = ((adj_ms - fwd_ms) if info["mode"] == 2 else adj_ms) / (s.nt - 1) * spl

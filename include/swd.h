@@ -248,9 +248,9 @@ typedef struct {
                          (Gaussian weights around the picks, core/ADWDgrad_norm.m), 2 the WD residual
                          weight_data_muti3 with F1 = 0 (SWD.m:188; ind = fmin/df+1, win = npair+2*ind,
                          refsx = floor(sx/dgx)+1, dg = dgx*dx as SWD.m:96-97,124-127 set them) */
-  int image_precision; /* per-shot imaging sums: 0 FP64 (default), 1 FP32 as the reference's MEX
-                          accumulates them (core/eigen_e2drtm_single.cpp:274-279); the shot sum is
-                          FP64 either way */
+  int image_precision; /* per-shot imaging sums: 0 (default) FP32, as the reference's single MEX
+                          accumulates them (core/eigen_e2drtm_single.cpp:274-279), 1 FP64; the
+                          sum over shots is FP64 in shot order either way */
 } swd_engine_opts;
 
 typedef struct {

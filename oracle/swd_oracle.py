@@ -798,9 +798,10 @@ def observed_curves(s, vs, single=True, vp=None):
     return cr, cl
 
 
-def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True, single=True, vp=None, weight="softmax"):
+def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=False, single=True, vp=None, weight="softmax"):
     """SWD_single.m:172-193 for one shot: forward (FP32), spectra, picks, ADWDgrad_1, adjoint.
-    single=False: SWD.m's double path (FP64 FD, adjoint source kept in double)."""
+    single=False: SWD.m's double path (FP64 FD, adjoint source kept in double).  accum_fp64=False
+    (default) sums the single path's images in FP32, as the reference's single MEX does."""
     inp = _survey_fd(s, is_, vs, single, vp=vp)
     _, sw, wf = mex_staggerfd(inp, s.source())
     sp = _spectra(s, sw.astype(np.float64), is_)
@@ -831,8 +832,9 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=True, single=True, vp=Non
     return out
 
 
-def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=True, single=True, vp=None, weight="softmax"):
-    """SWD_single.m:171-201 (SWD.m with single=False) with the shot sum in FP64 in shot order."""
+def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=False, single=True, vp=None, weight="softmax"):
+    """SWD_single.m:171-201 (SWD.m with single=False) with the shot sum in FP64 in shot order
+    (per-shot images as shot_gradient)."""
     from concurrent.futures import ThreadPoolExecutor
     shots = list(range(1, s.ns + 1))
     if threads > 1:

@@ -274,7 +274,7 @@ static AdjArgs<float> adj_args(swd_engine* e, const FdGeom& g, int nb) {
   a.mb = nullptr;
   a.res = e->res.as<float>();
   a.img = e->img.as<double>();
-  a.img32 = e->opt.image_precision == 1 ? e->img.as<float>() : nullptr;  // same buffer, half used
+  a.img32 = e->opt.image_precision == 0 ? e->img.as<float>() : nullptr;  // same buffer, half used
   a.dtx = (float)(e->sv.dt / e->sv.dx);
   a.dt = (float)e->sv.dt;
   a.n_shots = nb;
@@ -642,7 +642,7 @@ static int run(swd_engine* e, const double* vp, const double* vs, bool device_pt
     if (!grad) { SWD_TRY(mark(e, bi, 3)); continue; }
     SWD_TRY(adjoint_batch(e, bi, s0, nb));
     const size_t n3 = 3 * e->plane;
-    if (e->opt.image_precision == 1)
+    if (e->opt.image_precision == 0)
       shot_sum_kernel<float><<<(unsigned)((n3 + 255) / 256), 256, 0, e->st>>>(e->img.as<float>(), nb, e->plane,
                                                                               e->gsum.as<double>());
     else
@@ -768,7 +768,7 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   SWD_TRY(radon_geom(&rp, e->rg));
   SWD_CHECK(e->rg.ccn >= s->nt, "ADWDgrad_1 needs ccn = fix(1/df/dt) (%d) >= nt (%d)", e->rg.ccn, s->nt);
   SWD_CHECK(s->ini >= 1 && s->ini <= e->rg.npair, "ini (%d) must lie in 1..npair (%d)", s->ini, e->rg.npair);
-  SWD_CHECK(e->opt.image_precision == 0 || e->opt.image_precision == 1, "image_precision must be 0 (FP64) or 1 (FP32)");
+  SWD_CHECK(e->opt.image_precision == 0 || e->opt.image_precision == 1, "image_precision must be 0 (FP32) or 1 (FP64)");
   SWD_CHECK(e->opt.adjoint_weight >= 0 && e->opt.adjoint_weight <= 2,
             "adjoint_weight must be 0 (ADWDgrad_1), 1 (ADWDgrad_norm) or 2 (weight_data_muti3)");
   if (e->opt.adjoint_weight == 2) {

@@ -4,6 +4,7 @@
 #include <cstdarg>
 #include <cstring>
 #include <atomic>
+#include <type_traits>
 #include <vector>
 
 #include "fd_host.cuh"
@@ -594,6 +595,10 @@ int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, c
   AdjArgs<T> a{};
   a.g = g; a.mat = d_m1.as<V>(); a.mb = d_m2.as<V2>();
   a.res = d_res.as<T>(); a.snap = d_snap.as<T>(); a.img = d_img.as<double>();
+  // single in, single out: the images accumulate in FP32, as the reference's single MEX
+  // accumulates them (core/eigen_e2drtm_single.cpp:274-279); otherwise in FP64
+  constexpr bool f32img = std::is_same<T, float>::value && std::is_same<TO, float>::value;
+  if (f32img) a.img32 = d_img.as<float>();
   a.dtx = dtx; a.dt = dt; a.n_shots = 1;
   T* bufs[2] = {d_state.as<T>(), d_state.as<T>() + 5 * g.field};
   int cur = 0;
@@ -604,8 +609,11 @@ int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, c
     cur ^= 1;
   }
   SWD_CUDA(cudaGetLastError());
-  // images [3][nz][nx] (double) -> MATLAB nz x nx each, in the output type
-  SWD_TRY(transpose<double, TO>(d_img.as<double>(), plane, d_out.as<TO>(), plane, 3, nz, nx, st));
+  // images [3][nz][nx] -> MATLAB nz x nx each, in the output type
+  if constexpr (f32img)
+    SWD_TRY(transpose<float, float>(d_img.as<float>(), plane, d_out.as<float>(), plane, 3, nz, nx, st));
+  else
+    SWD_TRY(transpose<double, TO>(d_img.as<double>(), plane, d_out.as<TO>(), plane, 3, nz, nx, st));
   TO* outs[3] = {cl_img, cm_img, illum};
   for (int i = 0; i < 3; ++i)
     SWD_CUDA(cudaMemcpyAsync(outs[i], d_out.as<TO>() + i * plane, plane * sizeof(TO), cudaMemcpyDeviceToHost, st));

@@ -117,7 +117,7 @@ class GradientEngine:
 
     def __init__(self, survey, hbm_budget=0, max_batch=0, snapshot_mode=0, ckpt_interval=0, use_graphs=True,
                  chunk_rows=0, device=0, source=None, warps=0, cells=0, ring_fwd=0, ring_adj=0, autotune=False,
-                 radon_precision="fp64", fd_schedule=0, adjoint_weight="softmax", image_precision="fp64"):
+                 radon_precision="fp64", fd_schedule=0, adjoint_weight="softmax", image_precision="fp32"):
         L = _bind()
         self.survey = survey
         self._sc = survey_struct(survey)
@@ -125,7 +125,7 @@ class GradientEngine:
                           int(chunk_rows), int(device), int(warps), int(cells), int(ring_fwd),
                           int(ring_adj), int(bool(autotune)), _RPREC[radon_precision], int(fd_schedule),
                           {"softmax": 0, "gauss": 1, "wd": 2}[adjoint_weight],
-                          {"fp64": 0, "fp32": 1}[image_precision])
+                          {"fp32": 0, "fp64": 1}[image_precision])
         h = ctypes.c_void_p()
         call("swd_engine_create", ctypes.byref(self._sc), ctypes.byref(opts), ctypes.byref(h))
         self._h = h

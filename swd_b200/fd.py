@@ -62,7 +62,8 @@ def _mex_adj(fn, dt, out_dt, iv, temp, ca, cl, cm, cm1, b, b1, seismo_w, fux, fu
 
 
 def eigen_e2drtm_single(iv, temp, ca, cl, cm, cm1, b, b1, seismo_w, fux, fuz, bwx, bwz, fp64_out=False):
-    """[cl_img, cm_img, illum_div] = eigen_e2drtm_single(...); FP64 accumulation on the GPU."""
+    """[cl_img, cm_img, illum_div] = eigen_e2drtm_single(...): single images accumulated in FP32 as
+    the reference MEX does; fp64_out=True accumulates in FP64 and returns double images."""
     if fp64_out:
         return _mex_adj("swd_e2drtm_single_f64out", np.float32, np.float64, iv, temp, ca, cl, cm, cm1, b, b1,
                         seismo_w, fux, fuz, bwx, bwz)

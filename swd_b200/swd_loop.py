@@ -99,7 +99,7 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True):
     if single:
         a = a.astype(np.float32)  # SWD_single.m:193
         cl, cm, il = e2drtm_eigen(www, a, is_, s.nbc, s.nt, s.dtx, s.dx, s.dt, s.gx, np.ones(s.ng), s.source(),
-                                  s.vp_ratio * vs, vs, s.isfs, s.fd_order, 0, s.nt_wf, fp64_out=True)
+                                  s.vp_ratio * vs, vs, s.isfs, s.fd_order, 0, s.nt_wf)
     else:
         cl, cm, il = e2drtm_eigend(www, a, is_, s.nbc, s.nt, s.dtx, s.dx, s.dt, s.gx, np.ones(s.ng), s.source(),
                                    s.vp_ratio * vs, vs, s.isfs, s.fd_order, 0, s.nt_wf)

@@ -71,10 +71,12 @@ def test_e2drtm_single_bit_exact(O, survey):
     for g, r in zip(got, ref):
         assert np.abs(r).max() > 0
         assert np.array_equal(g, r)
+    # single images accumulate in FP32, as the reference's single MEX does
+    ref32 = O.mex_e2drtm(ainp, res, wf, accum_fp64=False)
     got32 = S.eigen_e2drtm_single(ainp.iv, ainp.temp, ainp.ca, ainp.cl, ainp.cm, ainp.cm1, ainp.b, ainp.b1, res,
                                   wf["fux"], wf["fuz"], wf["bwx"], wf["bwz"])
-    for g, r in zip(got32, ref):
-        assert np.array_equal(g, r.astype(np.float32))
+    for g, r in zip(got32, ref32):
+        assert g.dtype == np.float32 and np.array_equal(g, r.astype(np.float32))
 
 
 def test_e2drtm_double_bit_exact(O):
