@@ -243,7 +243,8 @@ typedef struct {
                          (both: warps = 2, 4 or 8 per CTA, ring_* = 4, 6 or 8 staged rows), 1 one
                          CTA barrier per row with the velocities a row ahead (shapes (2,1), (3,1),
                          (4,1) ring 4, (3,1) ring 6), 4 two CTA barriers per row (shared-memory
-                         ring; the shapes of warps/cells/ring_*) */
+                         ring; the shapes of warps/cells/ring_*), 5 as 3 with two shots per warp
+                         in packed FP32 pairs (warps = 2 or 4, ring_* = 4 or 6) */
   int adjoint_weight; /* adjoint source: 0 ADWDgrad_1 (SoftMax weights, SWD.m:190), 1 ADWDgrad_norm
                          (Gaussian weights around the picks, core/ADWDgrad_norm.m), 2 the WD residual
                          weight_data_muti3 with F1 = 0 (SWD.m:188; ind = fmin/df+1, win = npair+2*ind,

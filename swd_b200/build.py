@@ -9,6 +9,7 @@ the default contraction.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -25,6 +26,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path
 # file -> extra flags
 SOURCES = {
     "fd_host.cu": ["-fmad=false"],
+    "fd_warpx.cu": ["-fmad=false"],
     "model_prep.cu": ["-fmad=false"],
     "radon.cu": [],
     "engine.cu": ["-fmad=false"],
@@ -44,14 +46,18 @@ def build(force: bool = False, verbose: bool = False) -> str:
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(ROOT, "include", "swd.h"), __file__]
     if not force and os.path.exists(OUT) and os.path.getmtime(OUT) >= _newest(deps):
         return OUT
-    objs = []
+    jobs = []
     for src, extra in SOURCES.items():
         obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
         cmd = [NVCC, *ARCH, *COMMON, *extra, "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+        jobs.append((cmd, obj))
+    # the translation units are independent: compile them side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd, _ in jobs]:
+            f.result()
+    objs = [obj for _, obj in jobs]
     cmd = [NVCC, *ARCH, "-shared", "-o", OUT, *objs, "-lcudart"]
     if verbose:
         print(" ".join(cmd))

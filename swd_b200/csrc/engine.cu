@@ -498,11 +498,13 @@ static int autotune(swd_engine* e) {
       for (int ch : wch) {
         double bf = 1e30, ba = 1e30;
         int rf = 4, ra = 4, pf = 0;
-        for (int pairs : {0, 1}) {  // one or two steps per launch, forward and adjoint alike
+        // one or two steps per launch, forward and adjoint alike; 2: two steps, two shots per warp
+        for (int pairs : {0, 1, 2}) {
           double pbf = 1e30, pba = 1e30;
           int prf = 4, pra = 4;
           for (int slots : {4, 6, 8}) {
             if (slots == 8 && nw == 8) continue;
+            if (pairs == 2 && !fd_warpx_built(nw, slots)) continue;
             FdGeom gc = base;
             gc.nrec = snap_nrec;
             gc.sched = 2;
@@ -754,10 +756,12 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   g.ring_fwd = e->opt.ring_fwd;
   g.ring_adj = e->opt.ring_adj;
   // fd_schedule: 0 (default) and 3 warp streaming with two steps per launch, 1 one barrier per
-  // row, 2 warp streaming one step per launch, 4 two barriers per row
+  // row, 2 warp streaming one step per launch, 4 two barriers per row, 5 as 3 with two shots
+  // per warp in packed FP32 pairs
   const int fs = e->opt.fd_schedule;
+  SWD_CHECK(fs >= 0 && fs <= 5, "fd_schedule must lie in 0..5 (got %d)", fs);
   g.sched = fs == 1 ? 1 : fs == 4 ? 0 : 2;
-  g.pairs = (fs == 0 || fs == 3) ? 1 : 0;
+  g.pairs = (fs == 0 || fs == 3) ? 1 : fs == 5 ? 2 : 0;
   plan_decomposition(g, std::max(1, std::min(e->opt.max_batch > 0 ? e->opt.max_batch : e->ns, e->ns)),
                      e->opt.chunk_rows);
   // Radon geometry
@@ -896,7 +900,7 @@ static void fill_info(const swd_engine* e, swd_engine_info_t* info) {
   info->ring_adj = e->g.ring_adj;
   info->tuned_fwd_us = e->tuned_fwd_us;
   info->tuned_adj_us = e->tuned_adj_us;
-  info->fd_schedule = fd_pairs(e->g) ? 3 : e->g.sched == 0 ? 4 : e->g.sched;
+  info->fd_schedule = fd_pairs(e->g) ? (e->g.pairs == 2 ? 5 : 3) : e->g.sched == 0 ? 4 : e->g.sched;
 }
 
 int swd_engine_info(const swd_engine* e, swd_engine_info_t* info) {

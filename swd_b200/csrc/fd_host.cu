@@ -129,13 +129,19 @@ void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
     g.cells = 1;
     if (g.ring_fwd != 6 && !(g.ring_fwd == 8 && g.warps != 8)) g.ring_fwd = 4;
     if (g.ring_adj != 6 && !(g.ring_adj == 8 && g.warps != 8)) g.ring_adj = 4;
+    if (g.pairs == 2) {  // two shots per warp: 2 or 4 warps per CTA, 4 or 6 slots
+      if (g.warps != 2) g.warps = 4;
+      if (g.ring_fwd != 6) g.ring_fwd = 4;
+      if (g.ring_adj != 6) g.ring_adj = 4;
+    }
     g.n_strips = (g.NX - 2 + kWarpOut - 1) / kWarpOut;
     if (chunk_rows <= 0) {
       // about 5 waves of warps (148 SMs x 28 resident warps): short chunks keep more rows in
       // flight and every SM busy through the tail of a step; 96 shots of 132 x 660 -> 13 rows.
-      // Two-step launches recompute rows at each chunk edge and take half as many waves (26 rows).
-      const long target = g.pairs ? 148L * 28 * 5 / 2 : 148L * 28 * 5;
-      const long per = (long)g.n_strips * n_shots;
+      // Two-step launches recompute rows at each chunk edge and take half as many waves (26 rows);
+      // two-shot warps hold twice the registers (12 resident per SM) and count shot pairs.
+      const long target = g.pairs == 2 ? 148L * 12 * 5 / 2 : g.pairs ? 148L * 28 * 5 / 2 : 148L * 28 * 5;
+      const long per = (long)g.n_strips * (g.pairs == 2 ? (n_shots + 1) / 2 : n_shots);
       int nch = (int)((target + per - 1) / per);
       nch = std::max(1, std::min(nch, std::max(1, rows / 8)));
       chunk_rows = (rows + nch - 1) / nch;
@@ -374,6 +380,7 @@ int launch_fwd_pair(const FwdArgs<float>& a, int it, cudaStream_t st) {
     set_error("internal: two-step forward launch outside the warp-streaming schedule");
     return SWD_ERR_INVALID;
   }
+  if (a.g.pairs == 2) return launch_fwd_pair_x(a, it, st);
   switch (a.g.warps * 10 + a.g.ring_fwd) {
 #define X(w, s) case w * 10 + s: return fwd_warp2_impl<w, s>(a, it, st);
     SWD_WARP_SHAPES(X)
@@ -389,6 +396,7 @@ int launch_adj_pair(const AdjArgs<float>& a, int it, cudaStream_t st) {
     set_error("internal: two-step adjoint launch outside the warp-streaming schedule");
     return SWD_ERR_INVALID;
   }
+  if (a.g.pairs == 2) return launch_adj_pair_x(a, it, st);
   switch (a.g.warps * 10 + a.g.ring_adj) {
 #define X(w, s) case w * 10 + s: return adj_warp2_impl<w, s>(a, it, st);
     SWD_WARP_SHAPES(X)

@@ -35,7 +35,8 @@ struct FdGeom {
   int ring_fwd, ring_adj;    // rows in the shared-memory ring of the forward / adjoint kernels (4, 6, 8)
   int sched;                 // 0: two barriers per row (fd_smem.cuh); 1: one, velocities a row ahead (fd_lead.cuh);
                              // 2: warp streaming (fd_warp.cuh; warps = warps per CTA)
-  int pairs;                 // schedule 2: forward and adjoint advance two steps per launch
+  int pairs;                 // schedule 2: 1 = forward and adjoint advance two steps per launch; 2 = the same
+                             // with two shots per warp in packed FP32 pairs (fd_warpx.cuh)
   size_t field;              // NZ * pitch
 };
 

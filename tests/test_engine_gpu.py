@@ -80,6 +80,12 @@ def test_modes_are_bit_identical(tiny_case):
                {"snapshot_mode": 2, "ckpt_interval": 20, "fd_schedule": 3, "chunk_rows": 1},
                {"snapshot_mode": 1, "fd_schedule": 3, "warps": 8, "ring_fwd": 6, "chunk_rows": 4},
                {"snapshot_mode": 1, "fd_schedule": 3, "warps": 2, "ring_fwd": 8, "ring_adj": 6, "chunk_rows": 2,
+                "use_graphs": False},
+               # two steps per launch, two shots per warp (5 shots: the last warp carries one shot twice)
+               {"snapshot_mode": 1, "fd_schedule": 5}, {"snapshot_mode": 2, "ckpt_interval": 35, "fd_schedule": 5},
+               {"snapshot_mode": 2, "ckpt_interval": 20, "fd_schedule": 5, "chunk_rows": 1},
+               {"snapshot_mode": 1, "fd_schedule": 5, "warps": 2, "ring_fwd": 6, "chunk_rows": 3, "max_batch": 2},
+               {"snapshot_mode": 1, "fd_schedule": 5, "ring_adj": 6, "chunk_rows": 2, "max_batch": 3,
                 "use_graphs": False}):
         with GradientEngine(s, **kw) as e:
             e.set_observed(cr0_r, cr0_l)
@@ -89,11 +95,11 @@ def test_modes_are_bit_identical(tiny_case):
             assert np.array_equal(o[k], outs[0][k]), k
 
 
-@pytest.mark.parametrize("sched", [1, 2, 3, 4])
+@pytest.mark.parametrize("sched", [1, 2, 3, 4, 5])
 def test_other_schedules_on_the_plain_survey_match_the_oracle(O, sched):
-    """The one-barrier (1), warp-streaming (2), two-steps-per-launch (3, the default) and
-    two-barrier (4) schedules against the oracle on the 30 x 120 survey (source near the top,
-    receivers on the free-surface row, several chunks)."""
+    """The one-barrier (1), warp-streaming (2), two-steps-per-launch (3, the default),
+    two-barrier (4) and two-shots-per-warp (5) schedules against the oracle on the 30 x 120
+    survey (source near the top, receivers on the free-surface row, several chunks)."""
     s = configs.plain_c1(ns=3, nt=1000)
     cr0_r, cr0_l = O.observed_curves(s, s.vs_true)
     ref = O.gradient(s, s.vs, cr0_r, cr0_l)
@@ -227,8 +233,8 @@ def test_wd_adjoint_source_matches_oracle(tiny_case):
         assert _rel(out[k], ref[k]) < TOL, k
 
 
-@pytest.mark.parametrize("sched,mode,prec", [(0, 1, "fp32"), (0, 2, "fp32"), (4, 1, "fp32"), (0, 2, "fp64"),
-                                            (4, 1, "fp64")])
+@pytest.mark.parametrize("sched,mode,prec", [(0, 1, "fp32"), (0, 2, "fp32"), (4, 1, "fp32"), (5, 2, "fp32"),
+                                            (0, 2, "fp64"), (4, 1, "fp64"), (5, 1, "fp64")])
 def test_image_sums_match_the_oracle(O, tiny_case, sched, mode, prec):
     """image_precision='fp32' (the default) sums each shot's imaging terms in FP32, as the
     reference's single MEX does, and 'fp64' in FP64; against the oracle's shot loop with the same
