@@ -227,7 +227,8 @@ typedef struct {
   int ckpt_interval;  /* steps between forward checkpoints (mode 2; rounded to nt_wf; 0: the
                          interval that minimises checkpoint + snapshot memory per shot) */
   int use_graphs;     /* capture the time loops in CUDA graphs */
-  int chunk_rows;     /* rows per CTA in the FD kernels (0: heuristic) */
+  int chunk_rows;     /* rows per CTA in the FD kernels (0: heuristic; at most 60 for the warp
+                         schedules 0, 2, 3 and 5) */
   int device;
   int warps, cells;   /* FD kernels: warps per CTA and output columns per thread; (w,c) in
                          (1,2), (1,3), (2,1), (3,1), (4,1); others: (3,1) */

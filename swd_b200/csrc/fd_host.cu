@@ -146,7 +146,7 @@ void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
       nch = std::max(1, std::min(nch, std::max(1, rows / 8)));
       chunk_rows = (rows + nch - 1) / nch;
     }
-    g.chunk = std::max(1, std::min(chunk_rows, rows));
+    g.chunk = std::max(1, std::min({chunk_rows, rows, kWarpChunkMax}));
     g.n_chunks = (rows + g.chunk - 1) / g.chunk;
     return;
   }
@@ -249,6 +249,7 @@ static int fwd_warp2_launch(const FwdArgs<float>& a0, int it, cudaStream_t st) {
   constexpr size_t smem = warp_smem_bytes<NW, NS>();
   static int ready = set_smem(fd_fwd_warp2<NW, NS, SS>, smem);
   if (ready != SWD_OK) return ready;
+  SWD_CHECK(a0.g.chunk <= kWarpChunkMax, "internal: two-step chunk of %d rows (at most %d)", a0.g.chunk, kWarpChunkMax);
   FwdArgs<float> a = a0;
   a.g.n_strips = (a.g.NX - 2 + kWarpOut2 - 1) / kWarpOut2;  // 28-column strips
   const long warps = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;
@@ -267,6 +268,7 @@ static int adj_warp2_launch(const AdjArgs<float>& a0, int it, cudaStream_t st) {
   constexpr size_t smem = IS >= 0 ? warp_img_smem_bytes<NW, NS>() : warp_smem_bytes<NW, NS>();
   static int ready = set_smem(fd_adj_warp2<NW, NS, IS>, smem);
   if (ready != SWD_OK) return ready;
+  SWD_CHECK(a0.g.chunk <= kWarpChunkMax, "internal: two-step chunk of %d rows (at most %d)", a0.g.chunk, kWarpChunkMax);
   AdjArgs<float> a = a0;
   a.g.n_strips = (a.g.NX - 2 + kWarpOut2 - 1) / kWarpOut2;
   const long warps = (long)a.g.n_strips * a.g.n_chunks * a.n_shots;

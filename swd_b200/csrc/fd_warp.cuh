@@ -268,6 +268,17 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp(FwdArgs<float> a, int it)
 // ---------------------------------------------------------------- forward, two steps per launch
 
 constexpr int kWarpOut2 = 28;  // output columns per warp of the two-step kernels (two halo lanes a side)
+constexpr int kWarpChunkMax = 60;  // rows per chunk of the warp kernels (the two-step row masks below)
+
+// The two-step kernels mark the rows that take the checked path (sources, receivers, free
+// surface, top and bottom rows) as bits of a 64-bit mask over rows base .. base+63, base = zs-2,
+// so that a row's test is one bit test instead of a chain of compares.  row_span sets the bits
+// of rows lo..hi.  A chunk of at most kWarpChunkMax rows tests rows up to zs+60, inside the mask.
+__device__ __forceinline__ unsigned long long row_span(int base, int lo, int hi) {
+  lo = max(lo, base);
+  hi = min(hi, base + 63);
+  return lo > hi ? 0ull : (~0ull >> (63 - (hi - lo))) << (lo - base);
+}
 
 // Steps it and it+1 in one sweep: the state after step it (S1) is formed row by row as in
 // fd_fwd_warp and kept in registers, and step it+1 runs one row behind it on S1, so S1 never
@@ -438,9 +449,11 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it
       s0[2 * plane] = sn.sg;
     }
   };
-  auto slow1 = [&](int k) {
-    return k <= 1 || k >= g.NZ - 2 || k == g.pad_top || k == g.gz || (k >= sp.x - 2 && k <= sp.x);
-  };
+  // rows with checks: k <= 1, k >= NZ-2, the free surface, the receiver row, the source rows
+  const int mb = zs - 2;
+  const unsigned long long slowm = row_span(mb, mb, 1) | row_span(mb, g.NZ - 2, mb + 63) |
+                                   row_span(mb, g.pad_top, g.pad_top) | row_span(mb, g.gz, g.gz) |
+                                   row_span(mb, sp.x - 2, sp.x);
   // peeled: S1 rows zs-1 and zs, then the second step's prologue (new ww of row zs-1, new uu of row zs)
   first(std::true_type{}, 1, 2 % NS, 0, 0, zs - 1);
   first(std::true_type{}, 0, 3 % NS, 1, 1, zs);
@@ -458,9 +471,10 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it
   };
   int k1 = zs + 1;
   for (; k1 + NS <= ze + 1; k1 += NS) {
+    const unsigned m = (unsigned)(slowm >> (k1 - 1 - mb));  // bit i: row k1-1+i has checks
 #pragma unroll
     for (int u = 0; u < NS; ++u) {
-      if (slow1(k1 + u) || slow1(k1 + u - 1)) both(std::true_type{}, u, k1 + u);
+      if (m & (3u << u)) both(std::true_type{}, u, k1 + u);  // row k1+u or k1+u-1
       else both(std::false_type{}, u, k1 + u);
     }
   }
@@ -807,7 +821,10 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
     }
     if (IMGSUB == 1) image(IMp, r, j);
   };
-  auto slow1 = [&](int k) { return k <= 1 || k >= g.NZ - 2 || k == g.pad_top || k == g.gz; };
+  // rows with checks: k <= 1, k >= NZ-2, the free surface, the receiver row
+  const int mb = zs - 2;
+  const unsigned long long slowm = row_span(mb, mb, 1) | row_span(mb, g.NZ - 2, mb + 63) |
+                                   row_span(mb, g.pad_top, g.pad_top) | row_span(mb, g.gz, g.gz);
   first(std::true_type{}, 1, 1, 2 % NS, 0, 0, zs - 1);
   first(std::true_type{}, 0, 2 % NS, 3 % NS, 1, 1, zs);
   {
@@ -827,9 +844,10 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
   };
   int k1 = zs + 1;
   for (; k1 + NS <= ze + 1; k1 += NS) {
+    const unsigned m = (unsigned)(slowm >> (k1 - 1 - mb));  // bit i: row k1-1+i has checks
 #pragma unroll
     for (int u = 0; u < NS; ++u) {
-      if (slow1(k1 + u) || slow1(k1 + u - 1)) both(std::true_type{}, u, k1 + u);
+      if (m & (3u << u)) both(std::true_type{}, u, k1 + u);  // row k1+u or k1+u-1
       else both(std::false_type{}, u, k1 + u);
     }
   }

@@ -31,6 +31,7 @@ int fwd_launch(const FwdArgs<float>& a0, int it, cudaStream_t st) {
   constexpr size_t smem = warpx_smem_bytes<NW, NS>();
   static int ready = set_smem_x(fd_fwd_warp2x<NW, NS, SS>, smem);
   if (ready != SWD_OK) return ready;
+  SWD_CHECK(a0.g.chunk <= kWarpChunkMax, "internal: two-step chunk of %d rows (at most %d)", a0.g.chunk, kWarpChunkMax);
   FwdArgs<float> a = a0;
   a.g.n_strips = (a.g.NX - 2 + kWarpOut2 - 1) / kWarpOut2;
   const long warps = pair_warps(a.g, a.n_shots);
@@ -49,6 +50,7 @@ int adj_launch(const AdjArgs<float>& a0, int it, cudaStream_t st) {
   constexpr size_t smem = IS >= 0 ? warpx_img_smem_bytes<NW, NS>() : warpx_smem_bytes<NW, NS>();
   static int ready = set_smem_x(fd_adj_warp2x<NW, NS, IS>, smem);
   if (ready != SWD_OK) return ready;
+  SWD_CHECK(a0.g.chunk <= kWarpChunkMax, "internal: two-step chunk of %d rows (at most %d)", a0.g.chunk, kWarpChunkMax);
   AdjArgs<float> a = a0;
   a.g.n_strips = (a.g.NX - 2 + kWarpOut2 - 1) / kWarpOut2;
   const long warps = pair_warps(a.g, a.n_shots);

@@ -310,10 +310,10 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2x(FwdArgs<float> a, int i
     if (decltype(slow_tag)::value && recj >= 0 && j == g.gz) seis_write(r, it + 1);
     if (SNAPSUB == 1 && snapc && j >= z_img0 && j < z_img1) snap_write(sn, j);
   };
-  auto slow1 = [&](int k) {
-    return k <= 1 || k >= g.NZ - 2 || k == g.pad_top || k == g.gz || (k >= sp[0].x - 2 && k <= sp[0].x) ||
-           (k >= sp[1].x - 2 && k <= sp[1].x);
-  };
+  const int mb = zs - 2;  // rows with checks, as in fd_fwd_warp2, for both shots' sources
+  const unsigned long long slowm = row_span(mb, mb, 1) | row_span(mb, g.NZ - 2, mb + 63) |
+                                   row_span(mb, g.pad_top, g.pad_top) | row_span(mb, g.gz, g.gz) |
+                                   row_span(mb, sp[0].x - 2, sp[0].x) | row_span(mb, sp[1].x - 2, sp[1].x);
   first(std::true_type{}, 1, 2 % NS, 0, 0, zs - 1);
   first(std::true_type{}, 0, 3 % NS, 1, 1, zs);
   {
@@ -328,9 +328,10 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2x(FwdArgs<float> a, int i
   };
   int k1 = zs + 1;
   for (; k1 + NS <= ze + 1; k1 += NS) {
+    const unsigned m = (unsigned)(slowm >> (k1 - 1 - mb));  // bit i: row k1-1+i has checks
 #pragma unroll
     for (int u = 0; u < NS; ++u) {
-      if (slow1(k1 + u) || slow1(k1 + u - 1)) both(std::true_type{}, u, k1 + u);
+      if (m & (3u << u)) both(std::true_type{}, u, k1 + u);  // row k1+u or k1+u-1
       else both(std::false_type{}, u, k1 + u);
     }
   }
@@ -552,7 +553,9 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2x(AdjArgs<float> a, int i
     }
     if (IMGSUB == 1) image(IMp, r, j);
   };
-  auto slow1 = [&](int k) { return k <= 1 || k >= g.NZ - 2 || k == g.pad_top || k == g.gz; };
+  const int mb = zs - 2;  // rows with checks, as in fd_adj_warp2
+  const unsigned long long slowm = row_span(mb, mb, 1) | row_span(mb, g.NZ - 2, mb + 63) |
+                                   row_span(mb, g.pad_top, g.pad_top) | row_span(mb, g.gz, g.gz);
   first(std::true_type{}, 1, 1, 2 % NS, 0, 0, zs - 1);
   first(std::true_type{}, 0, 2 % NS, 3 % NS, 1, 1, zs);
   {
@@ -572,9 +575,10 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2x(AdjArgs<float> a, int i
   };
   int k1 = zs + 1;
   for (; k1 + NS <= ze + 1; k1 += NS) {
+    const unsigned m = (unsigned)(slowm >> (k1 - 1 - mb));  // bit i: row k1-1+i has checks
 #pragma unroll
     for (int u = 0; u < NS; ++u) {
-      if (slow1(k1 + u) || slow1(k1 + u - 1)) both(std::true_type{}, u, k1 + u);
+      if (m & (3u << u)) both(std::true_type{}, u, k1 + u);  // row k1+u or k1+u-1
       else both(std::false_type{}, u, k1 + u);
     }
   }
