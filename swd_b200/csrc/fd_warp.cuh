@@ -284,7 +284,10 @@ __device__ __forceinline__ unsigned long long row_span(int base, int lo, int hi)
 // fd_fwd_warp and kept in registers, and step it+1 runs one row behind it on S1, so S1 never
 // goes to memory and a launch moves the state once for two steps.  Lanes x = 28*strip-1 ..
 // 28*strip+30: S1 is valid on lanes 1..30, the new state on lanes 2..29, which write.  Border
-// cells keep their state, as the one-step kernels leave them unwritten.  SNAPSUB: which of
+// cells keep their state, as the one-step kernels leave them unwritten: on the checked rows by
+// a select, on the others because the engine's material table holds temp = 1 on the border
+// columns and border lanes use a time factor of 0, so their update returns the state exactly
+// (x*1 + 0*y = x for the finite values of a wavefield).  SNAPSUB: which of
 // the two steps writes strain snapshots (-1 neither).
 template <int NW, int NS, int SNAPSUB>
 __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it) {
@@ -312,6 +315,7 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it
   const int2 sp = a.src[shot];
   const T sv1 = a.s[it], sv2 = a.s[it + 1];
   const T dtx = a.dtx;
+  const T dl = xint ? dtx : T(0);  // time factor of the fast rows (0: border lane, state kept)
   const bool sc = x == sp.y, sr = x == sp.y + 1;
   const bool s_w = sc && st != 1 && st != 4;
   const bool s_wr = sr && st == 2;
@@ -355,10 +359,13 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it
     constexpr bool SLOW = decltype(slow_tag)::value;
     const bool in0 = !SLOW || rowin(k);
     const bool in1 = !SLOW || rowin(k + 1);
+    // Fast rows skip the border test: a border lane updates with its time factor dl = 0 and the
+    // engine's temp = 1 on border columns, which returns its state bit for bit.
+    const T d = SLOW ? dtx : dl;
     const T xzl = shfl_l(R0.xz);
-    T wn = vel_w(xint && in0, R0.ww, R0.xz, xzl, R0.zz, R1.zz, m0.x, SLOW ? bz(k) : dtx);
+    T wn = vel_w(!SLOW || (xint && in0), R0.ww, R0.xz, xzl, R0.zz, R1.zz, m0.x, SLOW ? bz(k) : dl);
     const T xxr = shfl_r(R1.xx);
-    T un_next = vel_u(xint && in1, R1.uu, R1.xx, xxr, R1.xz, R0.xz, t1, SLOW ? bz(k + 1) : dtx);
+    T un_next = vel_u(!SLOW || (xint && in1), R1.uu, R1.xx, xxr, R1.xz, R0.xz, t1, SLOW ? bz(k + 1) : dl);
     if (SLOW) {
       wn = src_w(k, wn, sv);
       un_next = src_u(k + 1, un_next, sv);
@@ -374,12 +381,12 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it
       if (st == 1) { xo = xo + sv; zo = zo + sv; }
       else { zo = zo + sv; }
     }
-    const T xxn = m0.x * xo + (m0.y * fux + m0.z * bwz) * dtx;
-    T zzn = m0.x * zo + (m0.y * bwz + m0.z * fux) * dtx;
-    const T xzn = m0.x * R0.xz + (m0.w * (fuz + bwx)) * dtx;
+    const T xxn = m0.x * xo + (m0.y * fux + m0.z * bwz) * d;
+    T zzn = m0.x * zo + (m0.y * bwz + m0.z * fux) * d;
+    const T xzn = m0.x * R0.xz + (m0.w * (fuz + bwx)) * d;
     if (SLOW && k == g.pad_top) zzn = T(0);
     St r{un_cur, wn, xxn, zzn, xzn};
-    if (!(xint && in0)) r = R0;  // border cells keep their state
+    if (SLOW && !(xint && in0)) r = R0;  // border cells keep their state
     sn = Strain{fux, bwz, fuz + bwx};
     wn_prev = wn;
     un_cur = un_next;
@@ -666,6 +673,7 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
   float4* oq = reinterpret_cast<float4*>(obs) + xc;
   float* oxz = obs + 4 * F + xc;
   const T dtx = a.dtx;
+  const T dl = xint ? dtx : T(0);  // time factor of the fast rows (0: border lane, state kept)
   // dt*res of steps it and it-1 at receiver columns (:238-242); halo lanes inject too
   const bool rec = xin && x >= g.gx && (x - g.gx) % g.dg == 0 && (x - g.gx) / g.dg < g.ng;
   const size_t rrow = ((size_t)shot * g.nt + it) * g.ng + (rec ? (x - g.gx) / g.dg : 0);
@@ -744,19 +752,22 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
     constexpr bool SLOW = decltype(slow_tag)::value;
     const bool in0 = !SLOW || rowin(k);
     const bool in1 = !SLOW || rowin(k + 1);
-    T wn = adj_vel_w(xint && in0, R0.ww, Q1.q1, Q0.q1, Q1.q2, Q0.q2, shfl_r(Q0.p3), Q0.p3, m0.x, SLOW ? bz(k) : dtx);
+    const T d = SLOW ? dtx : dl;  // fast rows: border lanes keep their state through dl = 0, temp = 1
+    T wn = adj_vel_w(!SLOW || (xint && in0), R0.ww, Q1.q1, Q0.q1, Q1.q2, Q0.q2, shfl_r(Q0.p3), Q0.p3, m0.x,
+                     SLOW ? bz(k) : dl);
     if (SLOW && rec && k == g.gz) wn = wn + inj;
     const T p1l = shfl_l(Q1.p1), p2l = shfl_l(Q1.p2);
-    const T un_next = adj_vel_u(xint && in1, R1.uu, Q1.p1, p1l, Q1.p2, p2l, Q1.p3, Q0.p3, t1, SLOW ? bz(k + 1) : dtx);
+    const T un_next = adj_vel_u(!SLOW || (xint && in1), R1.uu, Q1.p1, p1l, Q1.p2, p2l, Q1.p3, Q0.p3, t1,
+                                SLOW ? bz(k + 1) : dl);
     const T un_r = shfl_r(un_cur);
     const T wn_l = shfl_l(wn);
     const T te = m0.x;
-    const T xxn = te * R0.xx - dtx * (un_r - un_cur);
-    T zzn = te * R0.zz - dtx * (wn - wn_prev);
-    const T xzn = (te * R0.xz - dtx * (un_next - un_cur)) - dtx * (wn - wn_l);
+    const T xxn = te * R0.xx - d * (un_r - un_cur);
+    T zzn = te * R0.zz - d * (wn - wn_prev);
+    const T xzn = (te * R0.xz - d * (un_next - un_cur)) - d * (wn - wn_l);
     if (SLOW && k == g.pad_top) zzn = T(0);
     St r{un_cur, wn, xxn, zzn, xzn};
-    if (!(xint && in0)) r = R0;  // border cells keep their state
+    if (SLOW && !(xint && in0)) r = R0;  // border cells keep their state
     wn_prev = wn;
     un_cur = un_next;
     return r;

@@ -105,7 +105,11 @@ __global__ void prep_packed_kernel(PrepParams p, const double* vp, const double*
   T t, a_, l, m, bb;
   prep_cell<T>(p, kappa, vp, vs, z, x, t, a_, l, m, bb);
   typename Vec4<T>::type u;
-  u.x = t; u.y = a_; u.z = l; u.w = m;
+  // Border columns are never updated.  Their temp is used for nothing but their own update,
+  // so it is set to 1: the two-step warp kernels then keep those cells with a zero time factor
+  // instead of a select per row (fd_warp.cuh).
+  u.x = (x == 0 || x == p.NX - 1) ? (T)1 : t;
+  u.y = a_; u.z = l; u.w = m;
   mat[(size_t)z * pitch + x] = u;
 }
 
