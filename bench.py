@@ -38,7 +38,7 @@ UNIT = "shot-gradients/s"
 # (dram__bytes_read.sum + dram__bytes_write.sum) per launch / (96 shots x 132 x 660 cells).
 NCU_BYTES_PER_CELL_LAUNCH = {4: {"fd_fwd_step": 36.1, "fd_adj_step": 36.1},
                              2: {"fd_fwd_step": 35.05, "fd_adj_step": 34.99},
-                             3: {"fd_fwd_step": 35.35, "fd_adj_step": 35.29}}
+                             3: {"fd_fwd_step": 35.22, "fd_adj_step": 35.35}}
 # Compulsory DRAM bytes of the fused one-sweep kernels: 5 state fields read + 5 written per
 # shot-cell and launch (a launch advances one step, or two under schedule 3; materials are
 # shared by the shots of a launch), plus per interior cell every nt_wf steps the 3-field
