@@ -95,6 +95,24 @@ def test_modes_are_bit_identical(tiny_case):
             assert np.array_equal(o[k], outs[0][k]), k
 
 
+@pytest.mark.parametrize("sched", [0, 2, 5])
+def test_warp_chunks_are_capped_at_60_rows(sched):
+    """The warp schedules mark a chunk's checked rows in a 64-bit mask, so their chunks are at
+    most 60 rows: a 70-row grid asked for 500-row chunks runs 60 + 10 rows and gives the bits
+    of the two-barrier schedule (which has no such cap)."""
+    s = configs.tiny(nz=62, nx=24, nt=400, ns=3)
+    outs = []
+    for kw in ({"fd_schedule": 4}, {"fd_schedule": sched, "chunk_rows": 500}):
+        with GradientEngine(s, snapshot_mode=1, **kw) as e:
+            if kw["fd_schedule"] != 4:
+                assert e.info["nzbc"] - 2 > 60 and e.info["chunk_rows"] == 60
+            r, l = e.observed_curves(s.vp_true, s.vs_true)
+            e.set_observed(r, l)
+            outs.append(e.gradient(s.vp, s.vs))
+    for k in ("g_cl", "g_cm", "g_illum", "dk_vs", "cr_pre_r"):
+        assert np.array_equal(outs[1][k], outs[0][k]), k
+
+
 @pytest.mark.parametrize("sched", [1, 2, 3, 4, 5])
 def test_other_schedules_on_the_plain_survey_match_the_oracle(O, sched):
     """The one-barrier (1), warp-streaming (2), two-steps-per-launch (3, the default),
