@@ -158,6 +158,7 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2x(FwdArgs<float> a, int i
   const T sv1 = a.s[it], sv2 = a.s[it + 1];
   const T dtx = a.dtx;
   const F2 dtx2 = bc(dtx);
+  const F2 dl2 = bc(xint ? dtx : T(0));  // time factor of the fast rows (0: border lane, state kept)
   bool s_w[2], s_wr[2], s_u[2], s_um[2], s_xz[2];
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
@@ -215,10 +216,11 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2x(FwdArgs<float> a, int i
     constexpr bool SLOW = decltype(slow_tag)::value;
     const bool in0 = !SLOW || rowin(k);
     const bool in1 = !SLOW || rowin(k + 1);
+    const F2 d = SLOW ? dtx2 : dl2;  // fast rows: border lanes keep their state (as fd_fwd_warp2)
     const F2 xzl = shfl_l(R0.xz);
-    F2 wn = vel_w(xint && in0, R0.ww, R0.xz, xzl, R0.zz, R1.zz, m0.te, SLOW ? bz(k) : dtx2);
+    F2 wn = vel_w(!SLOW || (xint && in0), R0.ww, R0.xz, xzl, R0.zz, R1.zz, m0.te, SLOW ? bz(k) : dl2);
     const F2 xxr = shfl_r(R1.xx);
-    F2 un_next = vel_u(xint && in1, R1.uu, R1.xx, xxr, R1.xz, R0.xz, t1, SLOW ? bz(k + 1) : dtx2);
+    F2 un_next = vel_u(!SLOW || (xint && in1), R1.uu, R1.xx, xxr, R1.xz, R0.xz, t1, SLOW ? bz(k + 1) : dl2);
     if (SLOW) {
       wn = src_w(k, wn, sv);
       un_next = src_u(k + 1, un_next, sv);
@@ -238,12 +240,12 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2x(FwdArgs<float> a, int i
           else { at(zo, h) = at(zo, h) + sv; }
         }
     }
-    const F2 xxn = m0.te * xo + (m0.ca * fux + m0.cl * bwz) * dtx2;
-    F2 zzn = m0.te * zo + (m0.ca * bwz + m0.cl * fux) * dtx2;
-    const F2 xzn = m0.te * R0.xz + (m0.cm1 * (fuz + bwx)) * dtx2;
+    const F2 xxn = m0.te * xo + (m0.ca * fux + m0.cl * bwz) * d;
+    F2 zzn = m0.te * zo + (m0.ca * bwz + m0.cl * fux) * d;
+    const F2 xzn = m0.te * R0.xz + (m0.cm1 * (fuz + bwx)) * d;
     if (SLOW && k == g.pad_top) zzn = bc(T(0));
     St r{un_cur, wn, xxn, zzn, xzn};
-    if (!(xint && in0)) r = R0;  // border cells keep their state
+    if (SLOW && !(xint && in0)) r = R0;  // border cells keep their state
     sn = Strain{fux, bwz, fuz + bwx};
     wn_prev = wn;
     un_cur = un_next;
@@ -377,6 +379,7 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2x(AdjArgs<float> a, int i
   }
   const T dtx = a.dtx;
   const F2 dtx2 = bc(dtx);
+  const F2 dl2 = bc(xint ? dtx : T(0));  // time factor of the fast rows (0: border lane, state kept)
   // dt*res of steps it and it-1 at receiver columns (:238-242); halo lanes inject too
   const bool rec = xin && x >= g.gx && (x - g.gx) % g.dg == 0 && (x - g.gx) / g.dg < g.ng;
   F2 inj1 = bc(T(0)), inj2 = bc(T(0));
@@ -476,21 +479,22 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2x(AdjArgs<float> a, int i
     constexpr bool SLOW = decltype(slow_tag)::value;
     const bool in0 = !SLOW || rowin(k);
     const bool in1 = !SLOW || rowin(k + 1);
-    F2 wn = adj_vel_w(xint && in0, R0.ww, Q1.q1, Q0.q1, Q1.q2, Q0.q2, shfl_r(Q0.p3), Q0.p3, m0.te,
-                      SLOW ? bz(k) : dtx2);
+    const F2 d = SLOW ? dtx2 : dl2;  // fast rows: border lanes keep their state (as fd_adj_warp2)
+    F2 wn = adj_vel_w(!SLOW || (xint && in0), R0.ww, Q1.q1, Q0.q1, Q1.q2, Q0.q2, shfl_r(Q0.p3), Q0.p3, m0.te,
+                      SLOW ? bz(k) : dl2);
     if (SLOW && rec && k == g.gz) wn = wn + inj;
     const F2 p1l = shfl_l(Q1.p1), p2l = shfl_l(Q1.p2);
-    const F2 un_next = adj_vel_u(xint && in1, R1.uu, Q1.p1, p1l, Q1.p2, p2l, Q1.p3, Q0.p3, t1,
-                                 SLOW ? bz(k + 1) : dtx2);
+    const F2 un_next = adj_vel_u(!SLOW || (xint && in1), R1.uu, Q1.p1, p1l, Q1.p2, p2l, Q1.p3, Q0.p3, t1,
+                                 SLOW ? bz(k + 1) : dl2);
     const F2 un_r = shfl_r(un_cur);
     const F2 wn_l = shfl_l(wn);
     const F2 te = m0.te;
-    const F2 xxn = te * R0.xx - dtx2 * (un_r - un_cur);
-    F2 zzn = te * R0.zz - dtx2 * (wn - wn_prev);
-    const F2 xzn = (te * R0.xz - dtx2 * (un_next - un_cur)) - dtx2 * (wn - wn_l);
+    const F2 xxn = te * R0.xx - d * (un_r - un_cur);
+    F2 zzn = te * R0.zz - d * (wn - wn_prev);
+    const F2 xzn = (te * R0.xz - d * (un_next - un_cur)) - d * (wn - wn_l);
     if (SLOW && k == g.pad_top) zzn = bc(T(0));
     St r{un_cur, wn, xxn, zzn, xzn};
-    if (!(xint && in0)) r = R0;  // border cells keep their state
+    if (SLOW && !(xint && in0)) r = R0;  // border cells keep their state
     wn_prev = wn;
     un_cur = un_next;
     return r;
