@@ -723,6 +723,12 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   e->sv.sx = nullptr;
   e->sv.sz = nullptr;
   e->sv.shot_no = nullptr;
+  // option ranges: checked before the first CUDA call, so that they are reported on any host
+  SWD_CHECK(e->opt.fd_schedule >= 0 && e->opt.fd_schedule <= 5, "fd_schedule must lie in 0..5 (got %d)",
+            e->opt.fd_schedule);
+  SWD_CHECK(e->opt.image_precision == 0 || e->opt.image_precision == 1, "image_precision must be 0 (FP32) or 1 (FP64)");
+  SWD_CHECK(e->opt.adjoint_weight >= 0 && e->opt.adjoint_weight <= 2,
+            "adjoint_weight must be 0 (ADWDgrad_1), 1 (ADWDgrad_norm) or 2 (weight_data_muti3)");
   e->device = e->opt.device;
   SWD_CUDA(cudaSetDevice(e->device));
   // model prep / FD geometry
@@ -759,7 +765,6 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   // row, 2 warp streaming one step per launch, 4 two barriers per row, 5 as 3 with two shots
   // per warp in packed FP32 pairs
   const int fs = e->opt.fd_schedule;
-  SWD_CHECK(fs >= 0 && fs <= 5, "fd_schedule must lie in 0..5 (got %d)", fs);
   g.sched = fs == 1 ? 1 : fs == 4 ? 0 : 2;
   g.pairs = (fs == 0 || fs == 3) ? 1 : fs == 5 ? 2 : 0;
   plan_decomposition(g, std::max(1, std::min(e->opt.max_batch > 0 ? e->opt.max_batch : e->ns, e->ns)),
@@ -772,9 +777,6 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   SWD_TRY(radon_geom(&rp, e->rg));
   SWD_CHECK(e->rg.ccn >= s->nt, "ADWDgrad_1 needs ccn = fix(1/df/dt) (%d) >= nt (%d)", e->rg.ccn, s->nt);
   SWD_CHECK(s->ini >= 1 && s->ini <= e->rg.npair, "ini (%d) must lie in 1..npair (%d)", s->ini, e->rg.npair);
-  SWD_CHECK(e->opt.image_precision == 0 || e->opt.image_precision == 1, "image_precision must be 0 (FP32) or 1 (FP64)");
-  SWD_CHECK(e->opt.adjoint_weight >= 0 && e->opt.adjoint_weight <= 2,
-            "adjoint_weight must be 0 (ADWDgrad_1), 1 (ADWDgrad_norm) or 2 (weight_data_muti3)");
   if (e->opt.adjoint_weight == 2) {
     // SWD.m:124-127: ind = fmin/df+1, npair = length(fmin:df:fmax), win = npair+2*ind
     const double ind = s->fmin / s->df + 1;

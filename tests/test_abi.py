@@ -49,6 +49,26 @@ def test_calls_validate_before_touching_the_gpu():
     assert e.value.status == 1
 
 
+def test_engine_options_validate_before_touching_the_gpu():
+    """Out-of-range engine options are reported as such, before any CUDA call."""
+    import ctypes
+    from swd_b200 import _lib, configs
+    from swd_b200.engine import EngineOpts, GradientEngine, survey_struct
+    s = configs.tiny(nt=400, ns=2)
+    for fs in (-1, 6):
+        with pytest.raises(_lib.SwdError, match="fd_schedule must lie in 0..5") as e:
+            GradientEngine(s, fd_schedule=fs)
+        assert e.value.status == 1
+    sc = survey_struct(s)
+    for field, value, msg in (("image_precision", 2, "image_precision must be 0"),
+                              ("adjoint_weight", 3, "adjoint_weight must be 0")):
+        opts = EngineOpts()
+        setattr(opts, field, value)
+        h = ctypes.c_void_p()
+        with pytest.raises(_lib.SwdError, match=msg):
+            _lib.call("swd_engine_create", ctypes.byref(sc), ctypes.byref(opts), ctypes.byref(h))
+
+
 def test_product_never_imports_the_oracle():
     pkg = os.path.join(ROOT, "swd_b200")
     for dp, _, fs in os.walk(pkg):
