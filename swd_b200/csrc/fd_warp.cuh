@@ -274,7 +274,7 @@ constexpr int kWarpChunkMax = 60;  // rows per chunk of the warp kernels (the tw
 // surface, top and bottom rows) as bits of a 64-bit mask over rows base .. base+63, base = zs-2,
 // so that a row's test is one bit test instead of a chain of compares.  row_span sets the bits
 // of rows lo..hi.  A chunk of at most kWarpChunkMax rows tests rows up to zs+60, inside the mask.
-__device__ __forceinline__ unsigned long long row_span(int base, int lo, int hi) {
+__host__ __device__ __forceinline__ unsigned long long row_span(int base, int lo, int hi) {
   lo = max(lo, base);
   hi = min(hi, base + 63);
   return lo > hi ? 0ull : (~0ull >> (63 - (hi - lo))) << (lo - base);
