@@ -3,17 +3,21 @@
 // Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
 // this library; nothing in the product (swd_b200/) links or calls it.
 //
-// Parity status: UNPINNED.  The reference (zhangchang271/SWD) ships no tests,
-// golden vectors or known-answer outputs, and its MEX kernels cannot be built
-// here (they need the MATLAB C++ MEX API and Eigen, neither present).  This
-// file is a from-source restatement of
+// Parity status: PINNED for the FP32 instantiation.  The reference (zhangchang271/SWD)
+// ships no tests, golden vectors or stored outputs, and MATLAB, Eigen and the MEX headers
+// are absent here; instead its two MEX sources are compiled unmodified into oracle/_ref/
+// (oracle/ref_entry.cpp, oracle/ref_shim/, `make -C oracle ref`) and tests/ checks this
+// file against them bit for bit (seismograms, snapshots, FP32 images) on the tiny,
+// 30x120, 100x600 and 400x3000 grids.  This file is a from-source restatement of
 //   core/eigen_staggerfd_single.cpp:98-357   (forward time loop)
 //   core/eigen_e2drtm_single.cpp:69-283      (adjoint time loop + imaging)
 // as explicit loops in the same IEEE operation order as the Eigen expressions
 // (no FMA contraction: build with -ffp-contract=off), templated on the scalar
 // so that T=float is the single-precision MEX and T=double stands in for the
-// binary-only eigen_*_double MEX.  It is cross-checked bit-for-bit against an
-// independent numpy restatement (oracle/swd_oracle.py) in tests/.
+// binary-only eigen_*_double MEX (that instantiation has no source to pin it to; the
+// double wrappers differ from the single ones only in class, staggerfd_eigend.m:38,70,91).
+// It is also cross-checked bit-for-bit against an independent numpy restatement
+// (oracle/swd_oracle.py) in tests/.
 //
 // Arrays are MATLAB column-major: A(z,x) = A[z + x*nzbc].
 #include <cmath>

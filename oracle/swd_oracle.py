@@ -3,13 +3,17 @@
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
 leg may import this module; the product package ``swd_b200`` never does.
 
-Parity status: UNPINNED.  The reference (zhangchang271/SWD) has no tests,
-golden vectors or stored outputs, and it cannot run here (MATLAB, Octave,
-Eigen and the MATLAB MEX headers are all absent).  Every function below is a
-restatement of a reference function, cited by file:line, in double precision
-like MATLAB, so that the GPU path can be compared with it on identical
-seeded inputs.  Third-party semantics that the reference relies on but does
-not contain are restated from their published definitions:
+Parity status: the FD time loops are PINNED; the spectrum, pick and SoftMax steps are
+UNPINNED.  The reference (zhangchang271/SWD) has no tests, golden vectors or stored
+outputs, and MATLAB, Octave, Eigen and the MATLAB MEX headers are all absent.  Its two
+C++ MEX sources are compiled unmodified into ``oracle/_ref`` against stand-ins for the
+Eigen / MEX API subset they use (``oracle/swd_ref.py``), and tests/ check the C++
+restatement of the FD loops against them bit for bit.  The ``.m`` steps (Radon, pick,
+SoftMax gradient, assembly) have nothing that runs them here: every function below is a
+restatement of a reference function, cited by file:line, in double precision like
+MATLAB, so that the GPU path can be compared with it on identical seeded inputs.
+Third-party semantics that the reference relies on but does not contain are restated
+from their published definitions:
 
 * MATLAB ``fft``/``ifft``: the plain DFT definition (numpy's pocketfft).
 * MATLAB ``softmax`` (Deep Learning Toolbox): column-wise, max-shifted.
@@ -798,12 +802,27 @@ def observed_curves(s, vs, single=True, vp=None):
     return cr, cl
 
 
-def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=False, single=True, vp=None, weight="softmax"):
+def _fd_pair(fd, single, accum_fp64):
+    """The FD calls of a shot loop: this module's restatement (fd="oracle"), or the reference's
+    own MEX sources built into oracle/_ref (fd="reference"; single precision, FP32 image sums)."""
+    if fd == "oracle":
+        return mex_staggerfd, lambda inp, res, wf: mex_e2drtm(inp, res, wf, accum_fp64)
+    if fd != "reference" or not single or accum_fp64:
+        raise ValueError("fd='reference' runs the single MEX with its FP32 image sums only")
+    from oracle import swd_ref
+    return swd_ref.mex_staggerfd, lambda inp, res, wf: tuple(
+        a.astype(np.float64) for a in swd_ref.mex_e2drtm(inp, res, wf))
+
+
+def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=False, single=True, vp=None, weight="softmax",
+                  fd="oracle"):
     """SWD_single.m:172-193 for one shot: forward (FP32), spectra, picks, ADWDgrad_1, adjoint.
     single=False: SWD.m's double path (FP64 FD, adjoint source kept in double).  accum_fp64=False
-    (default) sums the single path's images in FP32, as the reference's single MEX does."""
+    (default) sums the single path's images in FP32, as the reference's single MEX does.
+    fd="reference" runs the FD steps on the reference's own MEX sources (oracle/_ref)."""
+    fwd, adj = _fd_pair(fd, single, accum_fp64)
     inp = _survey_fd(s, is_, vs, single, vp=vp)
-    _, sw, wf = mex_staggerfd(inp, s.source())
+    _, sw, wf = fwd(inp, s.source())
     sp = _spectra(s, sw.astype(np.float64), is_)
     npair = s.npair
     out = {"res_r": np.nan, "res_l": np.nan, "crp_r": np.ones(npair), "crp_l": np.ones(npair)}
@@ -828,21 +847,22 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=False, single=True, vp=No
                        sp.get("r", (0, 0, None))[2], sp.get("l", (0, 0, None))[2])
     out["adj_src"] = a.astype(np.float32) if single else a
     ainp = _survey_fd(s, is_, vs, single, adjoint=True, vp=vp)
-    out["cl"], out["cm"], out["il"] = mex_e2drtm(ainp, out["adj_src"], wf, accum_fp64)
+    out["cl"], out["cm"], out["il"] = adj(ainp, out["adj_src"], wf)
     return out
 
 
-def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=False, single=True, vp=None, weight="softmax"):
+def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=False, single=True, vp=None, weight="softmax",
+             fd="oracle"):
     """SWD_single.m:171-201 (SWD.m with single=False) with the shot sum in FP64 in shot order
     (per-shot images as shot_gradient)."""
     from concurrent.futures import ThreadPoolExecutor
     shots = list(range(1, s.ns + 1))
     if threads > 1:
         with ThreadPoolExecutor(threads) as ex:
-            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight),
+            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight, fd),
                               shots))
     else:
-        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight) for i in shots]
+        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight, fd) for i in shots]
     g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
     for p in per:
         for k in g:

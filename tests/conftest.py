@@ -26,3 +26,16 @@ def _oracle_built():
 def O():
     from oracle import swd_oracle
     return swd_oracle
+
+
+@pytest.fixture(scope="session")
+def R():
+    """The reference's own FD MEX sources built into oracle/_ref (make -C oracle ref).  They
+    are built where the reference tree is present and travel with the repository; a host
+    that has neither the built files nor the tree skips the tests that need them."""
+    from oracle import swd_ref
+    if not swd_ref.available():
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=False, capture_output=True)
+    if not swd_ref.available():
+        pytest.skip("oracle/_ref is not built and the reference sources are not here")
+    return swd_ref
