@@ -32,17 +32,18 @@ import numpy as np  # noqa: E402
 METRIC = "shot-gradients/s (fwd+adj)"
 UNIT = "shot-gradients/s"
 # DRAM traffic per padded cell and launch of the FD step kernels (plain variants, without the
-# snapshot or imaging step) for each FD schedule, from the ncu captures summarised in
-# profiles/fd_step_kernels_batched-100x600.md (schedule 4), profiles/fd_warp_kernels_batched-100x600.md
-# (schedule 2) and profiles/fd_warp2_kernels_batched-100x600.md (schedule 3, two steps per launch):
-# (dram__bytes_read.sum + dram__bytes_write.sum) per launch / (96 shots x 132 x 660 cells).
+# snapshot or imaging step) for each FD schedule, measured with ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) on one launch over 96 shots x 132 x 660 cells, divided by the cells.
+# A schedule without an entry has no capture yet and reports traffic null.
 NCU_BYTES_PER_CELL_LAUNCH = {4: {"fd_fwd_step": 36.1, "fd_adj_step": 36.1},
                              2: {"fd_fwd_step": 35.05, "fd_adj_step": 34.99},
                              3: {"fd_fwd_step": 35.22, "fd_adj_step": 35.35}}
 # Compulsory DRAM bytes of the fused one-sweep kernels: 5 state fields read + 5 written per
-# shot-cell and launch (a launch advances one step, or two under schedule 3; materials are
-# shared by the shots of a launch), plus per interior cell every nt_wf steps the 3-field
+# shot-cell and launch (a launch advances one step, or two under schedules 3 and 5; materials
+# are shared by the shots of a launch), plus per interior cell every nt_wf steps the 3-field
 # snapshot write (forward) or snapshot read + image update (adjoint; FP32 or FP64 sums).
+# These are the bytes roofline.achieved counts.  The reference's two-phase schedule moves
+# 84 B per cell-step (velocity pass, then stress pass); that figure is reported beside it.
 COMPULSORY_STATE_B = 40
 
 
@@ -160,14 +161,32 @@ def workload_config(s, extra=None):
     return c
 
 
-# ------------------------------------------------------------------ CPU baseline (the oracle port)
+# ------------------------------------------------------------------ CPU baseline (the reference's CPU path)
 
-def cpu_baseline(s, n_shots=0):
-    """Time the oracle's restated CPU path on a bounded sample: one full shot-gradient per host thread."""
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def cpu_baseline(s, n_shots=0, fd=None):
+    """Time the reference's CPU path on a bounded sample: one full shot-gradient per host thread
+    (SWD.m's parfor over shots).  The FD steps run the reference's own MEX sources built into
+    oracle/_ref (kind 'reference') when they are here, else the restated C++ oracle ('port');
+    the Radon / pick / SoftMax steps are the oracle's numpy restatement of the .m files either
+    way (MATLAB is not available to run them)."""
     import psutil
     from concurrent.futures import ThreadPoolExecutor
 
     from oracle import swd_oracle as O
+    from oracle import swd_ref
+    if fd is None:
+        fd = "reference" if swd_ref.available() else "oracle"
     cores = os.cpu_count() or 1
     mem_gb = psutil.virtual_memory().available / 2**30
     per_shot_gb = 4 * s.nz * s.nx * (s.nt // s.nt_wf) * 4 / 2**30 * 1.3 + 0.5
@@ -176,15 +195,20 @@ def cpu_baseline(s, n_shots=0):
     shots = [1 + (i * max(1, s.ns // n)) % s.ns for i in range(n)]
     t0 = time.perf_counter()
     with ThreadPoolExecutor(n) as ex:
-        list(ex.map(lambda i: O.shot_gradient(s, i, s.vs, cr0, cr0), shots))
+        list(ex.map(lambda i: O.shot_gradient(s, i, s.vs, cr0, cr0, fd=fd), shots))
     dt = time.perf_counter() - t0
-    return {"value": n / dt, "unit": UNIT, "cores": n, "kind": "port",
+    what = ("FD on the reference's MEX sources (oracle/_ref)" if fd == "reference" else
+            "FD on the restated C++ oracle")
+    return {"value": n / dt, "unit": UNIT, "cores": n, "kind": "reference" if fd == "reference" else "port",
+            "cpu_model": cpu_model(), "host_threads": cores,
             "sample": f"{n} full shot-gradients of the {s.nz}x{s.nx} survey (nt {s.nt}), one per host thread, "
-                      f"{dt:.1f} s wall on {cores} host threads"}
+                      f"{dt:.1f} s wall on {cores} host threads; {what}, Radon/pick/SoftMax on the numpy "
+                      f"restatement of the .m files"}
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU path (restated C++/numpy oracle; the MATLAB MEX cannot be built)."""
+    """--impl reference: the reference's CPU path (its FD MEX sources built unmodified in
+    oracle/_ref, the .m steps restated in numpy; MATLAB itself cannot run here)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
@@ -203,9 +227,9 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": statistics.mean(times) * 1e3,
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": workload_config(s, {"sample": info["sample"]}),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": "port",
-                             "sample": info["sample"]},
+            "config": workload_config(s),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+                             "cpu_model": info["cpu_model"], "sample": info["sample"]},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -574,31 +598,43 @@ def main():
     nloc = sg.local.ns  # shots of this rank: one FD launch steps all of them
     cells = s.nzbc * s.nxbc * nloc
     inner = s.nz * s.nx * nloc
-    # algorithmic bytes per time step of every shot: the reference's two-phase schedule, 84 B
-    # per padded cell-step, plus 16 B snapshot write (forward) or 16 B snapshot read + 24 B
-    # FP32 image update (adjoint) per interior cell every nt_wf steps; times the steps per launch
+    # the reference's two-phase schedule per time step of every shot: 84 B per padded cell-step,
+    # plus 16 B snapshot write (forward) or 16 B snapshot read + 24 B FP32 image update
+    # (adjoint) per interior cell every nt_wf steps; times the steps per launch
     spl = 2 if info["fd_schedule"] in (3, 5) else 1  # time steps per launch
     fwd_bytes = spl * (cells * 84 + inner * 16 / s.nt_wf)
     img_rmw = 24 if args.image_precision == "fp32" else 48  # 3 image sums read and written
     adj_bytes = spl * (cells * 84 + inner * (16 + 24) / s.nt_wf)  # the reference's FP32 image sums
-    fwd_comp = cells * COMPULSORY_STATE_B + spl * inner * 12 / s.nt_wf
-    adj_comp = cells * COMPULSORY_STATE_B + spl * inner * (12 + img_rmw) / s.nt_wf
+    # compulsory bytes of a launch: the state once in and out, the materials once (one float4 per
+    # cell, shared by the shots), 3 snapshot fields written (forward) or read with the 3 image
+    # sums read and written (adjoint) per interior cell every nt_wf steps
+    mat = s.nzbc * s.nxbc * 16
+    fwd_comp = cells * COMPULSORY_STATE_B + mat + spl * inner * 12 / s.nt_wf
+    adj_comp = cells * COMPULSORY_STATE_B + mat + spl * inner * (12 + img_rmw) / s.nt_wf
     fwd_launch_ms = fwd_ms / s.nt * spl
     # checkpoint mode: the adjoint phase also re-runs the forward steps segment by segment
     adj_launch_ms = ((adj_ms - fwd_ms) if info["mode"] == 2 else adj_ms) / (s.nt - 1) * spl
     peak, peak_kind = peaks()
 
-    def roof(name, nbytes, comp, launch_ms):
-        ach = nbytes / (launch_ms / 1e3) / 1e9
+    def roof(name, ref_bytes, comp, launch_ms):
+        # achieved: the compulsory bytes of one launch (state once in and out, materials,
+        # snapshot / image terms) over its average CUDA-event time
+        ach = comp / (launch_ms / 1e3) / 1e9
         tr = NCU_BYTES_PER_CELL_LAUNCH.get(info["fd_schedule"], {}).get(name)
         return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
-                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
-                "fallback 6650 GB/s", "traffic": (tr * cells) if tr else None,
-                "traffic_source": f"ncu, plain variant of FD schedule {info['fd_schedule']}" if tr else None,
-                "steps_per_launch": spl,
-                "algorithmic_bytes_per_launch": nbytes, "avg_launch_ms": launch_ms,
-                "compulsory_bytes_per_launch": comp,
-                "frac_compulsory": comp / (launch_ms / 1e3) / 1e9 / peak}
+                "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs, copy kernel)" if peak_kind == "measured"
+                else "fallback 6650 GB/s",
+                "traffic": (tr * cells) if tr else None,
+                "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum, plain variant of FD schedule "
+                                   f"{info['fd_schedule']}, per launch") if tr else
+                f"no ncu capture of FD schedule {info['fd_schedule']} yet",
+                "steps_per_launch": spl, "algorithmic_bytes_per_launch": comp,
+                "algorithmic_bytes": "compulsory: 40 B per shot-cell per launch (5 state fields in and out) + "
+                                     "snapshot write / snapshot read + image update per interior cell every "
+                                     "nt_wf steps",
+                "avg_launch_ms": launch_ms,
+                "reference_schedule_bytes_per_launch": ref_bytes,
+                "frac_reference_schedule": ref_bytes / (launch_ms / 1e3) / 1e9 / peak}
 
     rf = roof("fd_fwd_step", fwd_bytes, fwd_comp, fwd_launch_ms)
     ra = roof("fd_adj_step", adj_bytes, adj_comp, adj_launch_ms)
@@ -607,13 +643,14 @@ def main():
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "strong",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded layered model + Gaussian anomaly)",
-            "config": workload_config(s, {"adjoint": {1: "stored strain snapshots", 2: "checkpoint+recompute"}[
-                info["mode"]], "batch": info["batch"], "engine_bytes": info["bytes"],
-                "fd_variant": {k: info[k] for k in ("fd_schedule", "warps", "cells", "ring_fwd", "ring_adj",
-                                                    "chunk_rows")} |
-                {"autotuned": tune}, "image_sums": args.image_precision,
-                "parallelism": f"{s.ns} shots split round-robin over {world} GPU(s), one FP64 all-reduce of "
-                               f"the shot sums per step", "shots_this_rank": nloc}),
+            "config": workload_config(s),
+            "engine": {"adjoint": {1: "stored strain snapshots", 2: "checkpoint+recompute"}[info["mode"]],
+                       "ckpt_interval": info.get("ckpt_interval"), "batch": info["batch"], "engine_bytes": info["bytes"],
+                       "fd_variant": {k: info[k] for k in ("fd_schedule", "warps", "cells", "ring_fwd", "ring_adj",
+                                                           "chunk_rows")} | {"autotuned": tune},
+                       "image_sums": args.image_precision,
+                       "parallelism": f"{s.ns} shots split round-robin over {world} GPU(s), one FP64 all-reduce "
+                                      f"of the shot sums per step", "shots_this_rank": nloc},
             "e2e": {"value": s.ns / e2e_s, "unit": UNIT, "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,

@@ -143,7 +143,8 @@ int swd_pick(const double* ml, int np, int npair, double vmin, const double* cr_
  * default stream); the call synchronises it to read the pick status.  The scratch lives in one
  * static device array of libswd.so (16 KiB, held by every GPU that loads the library until the
  * process exits), which limits npair to SWD_PICK_NOALLOC_MAX_NPAIR.  The first call on a device
- * looks up the array's device address; make that call before any stream capture.  Every call
+ * looks up the array's device address; make that call before any stream capture.  Later calls
+ * outside a capture look it up again, so a cudaDeviceReset leaves no stale address.  Every call
  * shares the array: calls that overlap on the GPU race. */
 #define SWD_PICK_NOALLOC_MAX_NPAIR 2047
 int swd_pick_noalloc(const double* d_ml, int np, int npair, double vmin, const double* d_cr_0, int method,

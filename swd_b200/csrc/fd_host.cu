@@ -533,7 +533,7 @@ int staggerfd_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl
   for (int it = 0; it < p.nt; ++it) {
     a.in = bufs[it & 1];
     a.out = bufs[(it + 1) & 1];
-    launch_fwd_step<T, 4>(a, it, st);
+    SWD_TRY(launch_fwd_step<T, 4>(a, it, st));  // a dispatch or geometry error ends the call
   }
   SWD_CUDA(cudaGetLastError());
   // seismograms: [2][nt][ng] -> MATLAB nt x ng (column-major) each
@@ -615,7 +615,7 @@ int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, c
   for (int it = nt - 2; it >= 0; --it) {  // core/eigen_e2drtm_single.cpp:181
     a.in = bufs[cur];
     a.out = bufs[cur ^ 1];
-    launch_adj_step<T, 4>(a, it, st);
+    SWD_TRY(launch_adj_step<T, 4>(a, it, st));
     cur ^= 1;
   }
   SWD_CUDA(cudaGetLastError());

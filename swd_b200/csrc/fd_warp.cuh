@@ -280,6 +280,18 @@ __host__ __device__ __forceinline__ unsigned long long row_span(int base, int lo
   return lo > hi ? 0ull : (~0ull >> (63 - (hi - lo))) << (lo - base);
 }
 
+// The checked rows of a two-step chunk that starts at row zs, as a mask over rows zs-2 ..
+// zs+61: rows <= 1 and >= NZ-2, the free surface, the receiver row and the rows sx-2 .. sx
+// above and at each source row sx in {src0, src1} (kNoSourceRow: none; the adjoint has none,
+// the two-shots-per-warp forward kernels have two).
+constexpr int kNoSourceRow = -1000000;
+__host__ __device__ __forceinline__ unsigned long long slow_rows(int NZ, int pad_top, int gz, int zs,
+                                                                int src0 = kNoSourceRow, int src1 = kNoSourceRow) {
+  const int mb = zs - 2;
+  return row_span(mb, mb, 1) | row_span(mb, NZ - 2, mb + 63) | row_span(mb, pad_top, pad_top) |
+         row_span(mb, gz, gz) | row_span(mb, src0 - 2, src0) | row_span(mb, src1 - 2, src1);
+}
+
 // Steps it and it+1 in one sweep: the state after step it (S1) is formed row by row as in
 // fd_fwd_warp and kept in registers, and step it+1 runs one row behind it on S1, so S1 never
 // goes to memory and a launch moves the state once for two steps.  Lanes x = 28*strip-1 ..
@@ -458,9 +470,7 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it
   };
   // rows with checks: k <= 1, k >= NZ-2, the free surface, the receiver row, the source rows
   const int mb = zs - 2;
-  const unsigned long long slowm = row_span(mb, mb, 1) | row_span(mb, g.NZ - 2, mb + 63) |
-                                   row_span(mb, g.pad_top, g.pad_top) | row_span(mb, g.gz, g.gz) |
-                                   row_span(mb, sp.x - 2, sp.x);
+  const unsigned long long slowm = slow_rows(g.NZ, g.pad_top, g.gz, zs, sp.x);
   // peeled: S1 rows zs-1 and zs, then the second step's prologue (new ww of row zs-1, new uu of row zs)
   first(std::true_type{}, 1, 2 % NS, 0, 0, zs - 1);
   first(std::true_type{}, 0, 3 % NS, 1, 1, zs);
@@ -834,8 +844,7 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
   };
   // rows with checks: k <= 1, k >= NZ-2, the free surface, the receiver row
   const int mb = zs - 2;
-  const unsigned long long slowm = row_span(mb, mb, 1) | row_span(mb, g.NZ - 2, mb + 63) |
-                                   row_span(mb, g.pad_top, g.pad_top) | row_span(mb, g.gz, g.gz);
+  const unsigned long long slowm = slow_rows(g.NZ, g.pad_top, g.gz, zs);
   first(std::true_type{}, 1, 1, 2 % NS, 0, 0, zs - 1);
   first(std::true_type{}, 0, 2 % NS, 3 % NS, 1, 1, zs);
   {

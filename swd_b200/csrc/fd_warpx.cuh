@@ -313,9 +313,7 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2x(FwdArgs<float> a, int i
     if (SNAPSUB == 1 && snapc && j >= z_img0 && j < z_img1) snap_write(sn, j);
   };
   const int mb = zs - 2;  // rows with checks, as in fd_fwd_warp2, for both shots' sources
-  const unsigned long long slowm = row_span(mb, mb, 1) | row_span(mb, g.NZ - 2, mb + 63) |
-                                   row_span(mb, g.pad_top, g.pad_top) | row_span(mb, g.gz, g.gz) |
-                                   row_span(mb, sp[0].x - 2, sp[0].x) | row_span(mb, sp[1].x - 2, sp[1].x);
+  const unsigned long long slowm = slow_rows(g.NZ, g.pad_top, g.gz, zs, sp[0].x, sp[1].x);
   first(std::true_type{}, 1, 2 % NS, 0, 0, zs - 1);
   first(std::true_type{}, 0, 3 % NS, 1, 1, zs);
   {
@@ -558,8 +556,7 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2x(AdjArgs<float> a, int i
     if (IMGSUB == 1) image(IMp, r, j);
   };
   const int mb = zs - 2;  // rows with checks, as in fd_adj_warp2
-  const unsigned long long slowm = row_span(mb, mb, 1) | row_span(mb, g.NZ - 2, mb + 63) |
-                                   row_span(mb, g.pad_top, g.pad_top) | row_span(mb, g.gz, g.gz);
+  const unsigned long long slowm = slow_rows(g.NZ, g.pad_top, g.gz, zs);
   first(std::true_type{}, 1, 1, 2 % NS, 0, 0, zs - 1);
   first(std::true_type{}, 0, 2 % NS, 3 % NS, 1, 1, zs);
   {

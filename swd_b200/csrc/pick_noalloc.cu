@@ -8,11 +8,15 @@
 //
 // g_pick_scratch is per device: every GPU that loads libswd.so holds its 16 KiB until the process
 // exits.  In host code the name g_pick_scratch is only a stand-in for the device symbol; its
-// device address comes from cudaGetSymbolAddress, looked up once per device (with that device
-// current) on the first call there, and passed to the kernel as a plain pointer.  Every call
-// shares the array and it keeps the last call's contents: the status word is cleared on the
-// stream before each launch, and the differences are written before anything reads them.  Calls
-// that overlap on the GPU (two streams, two host threads) race on the array.
+// device address comes from cudaGetSymbolAddress (with the device current; return code checked)
+// and is passed to the kernel as a plain pointer.  The first call on a device does that set-up,
+// so it must come before any stream capture on that device.  Outside a capture every call looks
+// the address up again (a cheap runtime lookup), so a cudaDeviceReset, which unloads the module
+// and may place the array elsewhere when it is loaded again, never leaves a stale address
+// behind; inside a capture the address found by the last uncaptured call on the device is used.
+// Every call shares the array and it keeps the last call's contents: the status word is cleared
+// on the stream before each launch, and the differences are written before anything reads them.
+// Calls that overlap on the GPU (two streams, two host threads) race on the array.
 #include <mutex>
 
 #include "fd_host.cuh"
@@ -32,18 +36,23 @@ constexpr int kMaxDevices = 64;
 std::mutex g_scratch_mu;
 double* g_scratch_addr[kMaxDevices] = {};
 
-// Device address of g_pick_scratch on the current device (looked up on first use).
-int scratch_on_current_device(double** out) {
+// Device address of g_pick_scratch on the current device: looked up now unless `st` is being
+// captured, else the address of the last lookup on this device.
+int scratch_on_current_device(cudaStream_t st, double** out) {
   int dev = -1;
   SWD_CUDA(cudaGetDevice(&dev));
   SWD_CHECK(dev >= 0 && dev < kMaxDevices, "device %d is beyond the %d devices this entry point tracks", dev,
             kMaxDevices);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  SWD_CUDA(cudaStreamIsCapturing(st, &cap));
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     SWD_CUDA(cudaGetSymbolAddress(&p, g_pick_scratch));
     g_scratch_addr[dev] = static_cast<double*>(p);
   }
+  SWD_CHECK(g_scratch_addr[dev] != nullptr,
+            "the first swd_pick_noalloc call on device %d must come before any stream capture", dev);
   *out = g_scratch_addr[dev];
   return SWD_OK;
 }
@@ -60,12 +69,12 @@ extern "C" int swd_pick_noalloc(const double* d_ml, int np_, int npair, double v
             "npair %d exceeds the %d columns of the allocation-free picker's static scratch (swd_pick has no "
             "such limit on the scratch)",
             npair, kMaxNpair);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
   double* scratch = nullptr;
-  SWD_TRY(scratch_on_current_device(&scratch));
+  SWD_TRY(scratch_on_current_device(st, &scratch));
   double* d_dc = scratch;
   double* d_res_scratch = scratch + kMaxNpair;
   int* d_status = reinterpret_cast<int*>(scratch + kMaxNpair + 1);
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   // pick_batch clears the status word on st before it launches the picker
   SWD_TRY(pick_batch(np_, npair, 1, ini, method, vmin, nullptr, d_ml, d_cr_0, d_cr_pre, d_dc,
                      d_res ? d_res : d_res_scratch, d_status, st));

@@ -184,10 +184,15 @@ __global__ void __launch_bounds__(kThreads) tc_contract_kernel(TcArgs a) {
     if (s < nk) load_stage(s);
     cp_commit();
   }
-  for (int kt = 0; kt < nk; ++kt) {
+  // A wait that times out sets `failed`.  Every write to it comes before the barrier at the top of
+  // the next stage, so all threads read the same value there and leave the loop together: no
+  // further copies into slots that MMAs may still read, and no further MMAs.
+  int kt = 0;
+  for (; kt < nk; ++kt) {
     cp_wait<STAGES - 2>();  // this thread's copies of stage kt have landed
     fence_proxy_async();
     __syncthreads();
+    if (failed) break;
     const int slot = kt % STAGES;
     if (tid == 0) {
       fence_after_sync();
@@ -213,21 +218,27 @@ __global__ void __launch_bounds__(kThreads) tc_contract_kernel(TcArgs a) {
       }
       mma_commit(smem_u32(&mbar[slot]));
     }
-    // refill the slot consumed by the previous stage once its MMAs are done
+    // refill the slot consumed by the previous stage once its MMAs are done; a thread whose
+    // wait gave up copies nothing into it
     const int kn = kt + STAGES - 1;
     if (kn < nk) {
+      bool free_slot = true;
       if (kn >= STAGES) {
         const int ps = kn % STAGES;  // == (kt - 1) % STAGES
-        if (!mbar_wait(smem_u32(&mbar[ps]), (uint32_t)((kn / STAGES - 1) & 1))) failed = 1;
+        free_slot = mbar_wait(smem_u32(&mbar[ps]), (uint32_t)((kn / STAGES - 1) & 1));
+        if (!free_slot) failed = 1;
       }
-      load_stage(kn);
+      if (free_slot) load_stage(kn);
     }
     cp_commit();
   }
-  cp_wait<0>();
-  // all MMAs: the last commit covers every earlier tcgen05 operation of thread 0
-  const int last = (nk - 1) % STAGES;
-  if (!mbar_wait(smem_u32(&mbar[last]), (uint32_t)(((nk - 1) / STAGES) & 1))) failed = 1;
+  cp_wait<0>();  // this thread's copies in flight
+  // the MMAs: the last commit (stage kt-1) covers every earlier tcgen05 operation of thread 0;
+  // after a failure this one more wait is bounded too, and TMEM is released either way
+  if (kt > 0) {
+    const int last = kt - 1;
+    if (!mbar_wait(smem_u32(&mbar[last % STAGES]), (uint32_t)((last / STAGES) & 1))) failed = 1;
+  }
   fence_after_sync();
   __syncthreads();
 

@@ -1,11 +1,13 @@
 """The checked-row masks of the two-step FD kernels, on the host.
 
-fd_fwd_warp2 / fd_adj_warp2 (swd_b200/csrc/fd_warp.cuh) decide per row whether row k or k-1
-needs the checked path (rows <= 1, >= NZ-2, the free surface, the receiver row and, forward,
-the source rows sp.x-2 .. sp.x) with one bit test on a 64-bit mask built by row_span over the
-rows zs-2 .. zs+61 of a chunk.  This compiles row_span for the host and checks, for every
-chunk of up to 60 rows (the cap of the warp schedules) and ring depths 4, 6 and 8, that the
-bit test the kernels' main loop makes equals the chain of compares it replaced.
+fd_fwd_warp2 / fd_adj_warp2 (swd_b200/csrc/fd_warp.cuh) and the two-shots-per-warp kernels
+(fd_warpx.cuh) decide per row whether row k or k-1 needs the checked path (rows <= 1, >= NZ-2,
+the free surface, the receiver row and, forward, the source rows sx-2 .. sx of each shot of the
+warp) with one bit test on a 64-bit mask that slow_rows builds over the rows zs-2 .. zs+61 of a
+chunk.  This compiles slow_rows (the same function the kernels call) for the host and checks, for
+every chunk of up to 60 rows (the cap of the warp schedules), ring depths 4, 6 and 8, no source
+(adjoint), one source and two sources, that the bit test of the kernels' main loop equals the
+chain of compares it replaced.
 """
 import os
 import shutil
@@ -19,7 +21,8 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 SRC = r"""
 #include <cstdio>
 #include "fd_warp.cuh"
-using swd::row_span;
+using swd::slow_rows;
+using swd::kNoSourceRow;
 using swd::kWarpChunkMax;
 
 int main() {
@@ -30,15 +33,17 @@ int main() {
         for (int spx = pad_top; spx <= NZ - 3; spx += 7)
           for (int chunk = 1; chunk <= kWarpChunkMax; ++chunk)
             for (int zs = 1; zs <= NZ - 2; zs += chunk)
-              for (int fwd = 0; fwd <= 1; ++fwd)
+              for (int nsrc = 0; nsrc <= 2; ++nsrc)
                 for (int NS = 4; NS <= 8; NS += 2) {
                   const int ze = zs + chunk < NZ - 1 ? zs + chunk : NZ - 1;
                   const int mb = zs - 2;
-                  unsigned long long m = row_span(mb, mb, 1) | row_span(mb, NZ - 2, mb + 63) |
-                                         row_span(mb, pad_top, pad_top) | row_span(mb, gz, gz);
-                  if (fwd) m |= row_span(mb, spx - 2, spx);
+                  // the second shot of a two-shot warp sits a few rows lower (or at the same row)
+                  const int s0 = nsrc >= 1 ? spx : kNoSourceRow;
+                  const int s1 = nsrc >= 2 ? pad_top + (spx * 5) % (NZ - 2 - pad_top) : kNoSourceRow;
+                  const unsigned long long m = slow_rows(NZ, pad_top, gz, zs, s0, s1);
+                  auto src = [&](int k, int s) { return s != kNoSourceRow && k >= s - 2 && k <= s; };
                   auto slow1 = [&](int k) {
-                    return k <= 1 || k >= NZ - 2 || k == pad_top || k == gz || (fwd && k >= spx - 2 && k <= spx);
+                    return k <= 1 || k >= NZ - 2 || k == pad_top || k == gz || src(k, s0) || src(k, s1);
                   };
                   // the main loop of the kernels: k1 = zs+1, zs+1+NS, ... while k1 + NS <= ze + 1
                   for (int k1 = zs + 1; k1 + NS <= ze + 1; k1 += NS) {
@@ -48,8 +53,8 @@ int main() {
                       const bool chain = slow1(k1 + u) || slow1(k1 + u - 1);
                       ++checked;
                       if (mask != chain) {
-                        if (bad < 5) printf("NZ %d pad %d gz %d sp %d chunk %d zs %d fwd %d NS %d k %d\n", NZ, pad_top,
-                                            gz, spx, chunk, zs, fwd, NS, k1 + u);
+                        if (bad < 5) printf("NZ %d pad %d gz %d sp %d chunk %d zs %d nsrc %d NS %d k %d\n", NZ,
+                                            pad_top, gz, spx, chunk, zs, nsrc, NS, k1 + u);
                         ++bad;
                       }
                     }

@@ -1,8 +1,10 @@
-"""swd_pick_noalloc (device pointers, static scratch) against swd_pick (host pointers, cudaMalloc'd scratch).
+"""swd_pick_noalloc (device pointers, static scratch) against swd_pick (host pointers, cudaMalloc'd
+scratch) and against the oracle's LHDispPick restatement.
 
-The picker's results are integers plus vmin, so the two entry points must agree exactly; the
+The picker's results are integers plus vmin, so the entry points must agree exactly; the
 misfit is compared with the rel 1e-12 the other picker tests use.  Two calls in a row on
 different spectra check that the shared scratch carries nothing from one call into the next.
+The device's free memory must not move across a call.
 """
 import ctypes
 
@@ -81,3 +83,29 @@ def test_noalloc_pick_rejects_npair_beyond_its_scratch():
     with pytest.raises(_lib.SwdError) as e:
         _lib.call("swd_pick_noalloc", _vp(d_ml), 4, npair, 100.0, _vp(d_v), 1, 1, None, _vp(d_v), None)
     assert e.value.status == 1 and "2047" in str(e.value)
+
+
+@pytest.mark.gpu
+def test_noalloc_pick_matches_the_oracle_and_leaves_free_memory_unchanged():
+    import torch
+
+    from oracle import swd_oracle as O
+    rng = np.random.default_rng(77)
+    ml = _spectrum(rng, 351, 56)
+    cr0 = rng.integers(1, 351, 56).astype(float) + 100
+    ref_res, ref_cr = O.LHDispPick(ml, 100, cr0, 1, 10)
+    np_, npair = ml.shape
+    d_ml, d_cr0 = _dev(ml), _dev(cr0)
+    d_cr = torch.zeros(npair, dtype=torch.float64, device="cuda")
+    d_res = torch.zeros(1, dtype=torch.float64, device="cuda")
+    args = (_vp(d_ml), np_, npair, 100.0, _vp(d_cr0), 1, 10, _vp(d_res), _vp(d_cr), None)
+    _lib.call("swd_pick_noalloc", *args)  # the first call on a device may load the module
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for _ in range(2):
+        _lib.call("swd_pick_noalloc", *args)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    assert np.array_equal(d_cr.cpu().numpy(), ref_cr)
+    assert float(d_res.cpu()[0]) == pytest.approx(ref_res, rel=1e-12, abs=1e-12)
