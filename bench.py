@@ -71,8 +71,8 @@ def parse():
                    help="per-shot imaging sums: fp32 as the reference accumulates them (default) or fp64")
     p.add_argument("--sched", type=int, default=-1,
                    help="FD schedule: 0 or 3 warp streaming, two steps per launch; 1 one barrier per row; "
-                        "2 warp streaming, one step; 4 two barriers per row; 5 as 3 with two shots per warp "
-                        "(-1: autotuned)")
+                        "2 warp streaming, one step; 4 two barriers per row; 5 as 3 with two shots per warp; "
+                        "6 as 3 with two columns per lane (-1: autotuned)")
     p.add_argument("--serve", type=int, default=0,
                    help="served request stream: number of requests (0: run the gradient bench instead)")
     p.add_argument("--rate", type=float, default=2.0, help="served stream: Poisson arrival rate, requests/s")
@@ -601,7 +601,7 @@ def main():
     # the reference's two-phase schedule per time step of every shot: 84 B per padded cell-step,
     # plus 16 B snapshot write (forward) or 16 B snapshot read + 24 B FP32 image update
     # (adjoint) per interior cell every nt_wf steps; times the steps per launch
-    spl = 2 if info["fd_schedule"] in (3, 5) else 1  # time steps per launch
+    spl = 2 if info["fd_schedule"] in (3, 5, 6) else 1  # time steps per launch
     fwd_bytes = spl * (cells * 84 + inner * 16 / s.nt_wf)
     img_rmw = 24 if args.image_precision == "fp32" else 48  # 3 image sums read and written
     adj_bytes = spl * (cells * 84 + inner * (16 + 24) / s.nt_wf)  # the reference's FP32 image sums

@@ -24,7 +24,7 @@ enum {
   SWD_ERR_UNSUPPORTED = 2,  /* accepted by the reference, not built here (fd_order 24/26/28) */
   SWD_ERR_CUDA = 3,         /* CUDA runtime error */
   SWD_ERR_OOM = 4,          /* device allocation failed or over the HBM budget */
-  SWD_ERR_CANCELLED = 5,    /* a served request was cancelled */
+  SWD_ERR_CANCELLED = 5,    /* a served request or an engine call was cancelled */
   SWD_ERR_NUMERIC = 6,      /* NaN spectrum column, or interp1 with fewer than two picks */
   SWD_ERR_TIMEOUT = 7       /* swd_server_wait: the request has not finished yet */
 };
@@ -171,6 +171,32 @@ int swd_adwdgrad_limband(const swd_radon_params* p, int ns, int is, int w, doubl
                          const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
                          double* a_data_res);
 
+/* ---- field-data variants (fieldexamples/outcrop, fieldexamples/QadimahFault) ---- */
+
+/* Replaces the field-data LHDispPick variants, which start the guided pick at the global
+ * maximum of the unnormalised spectrum ml_raw (saveForBackward.mlr / .mll):
+ *   variant 1: fieldexamples/outcrop/core/LHDispPick.m:2-25 -> pickFDCValue(ml,ini,iniP,2,4)
+ *              (fieldexamples/outcrop/core/pickFDCValue.m:1-131) for method 1, argmax picks
+ *              otherwise; misfit over rows 15..npair-15;
+ *   variant 2: fieldexamples/QadimahFault/core/LHDispPick.m:2-41 (its mode 1) -> pickFDC1(ml,ini,
+ *              2,4) for any method; misfit over rows 50..npair-30 (NaN when that range is empty).
+ * ini = the first column holding the maximum of ml_raw, iniP = its first row of that value.
+ * ml, ml_raw: np x npair; cr_0, cr_pre: npair; res: scalar (may be NULL). */
+int swd_pick_field(const double* ml, const double* ml_raw, int np, int npair, double vmin, const double* cr_0,
+                   int method, int variant, double* res, double* cr_pre);
+
+/* Replaces fieldexamples/outcrop/core/ADWDgrad_1.m:1-81 (same arguments as ADWDgrad_1): the
+ * adjoint source divided by its largest magnitude (:79). */
+int swd_adwdgrad_maxnorm(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
+                         const double* grad_output_r, const double* grad_output_l, const double* space_m,
+                         const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
+                         double* a_data_res);
+
+/* Replaces norm_trace(data_in) (core/norm_trace.m:1-22; fieldexamples/outcrop/outcrop.m:174 applies
+ * it to every predicted gather): each column of the nt x ng array divided by its largest
+ * magnitude (an all-zero trace becomes NaN, 0/0, as in the reference). */
+int swd_norm_trace(const double* data_in, int nt, int ng, double* data_out);
+
 /* Replaces ADWDgrad_norm(...) (core/ADWDgrad_norm.m:1-102, same arguments as ADWDgrad_1):
  * the SoftMax weights are replaced by normpdf(1:np, cr, 16) around the picks
  * (core/paddingMl_norm.m:1-9).  cr_r / cr_l: npair, saveForBackward.cr_r / cr_l = cr_pre - vmin
@@ -298,6 +324,21 @@ int swd_engine_gradient(swd_engine* e, const double* vp, const double* vs, swd_g
 int swd_engine_gradient_device(swd_engine* e, const double* d_vp, const double* d_vs, double* d_dk_vs,
                                double* residual);
 /* The engine's CUDA stream (a cudaStream_t). */
+/* Cancel the engine's call in flight (callable from any host thread; returns at once).  The
+ * call's remaining FD launches return as soon as they start, and the call returns
+ * SWD_ERR_CANCELLED without results; the engine is ready for the next call.  A cancel raised
+ * while no call runs cancels the next call.  No counterpart in the reference (its parfor has no
+ * cancellation). */
+int swd_engine_cancel(swd_engine* e);
+/* Withdraw a cancel that no call has taken yet (e.g. one that arrived after its call finished),
+ * so that it does not cancel the next call.  No counterpart in the reference. */
+int swd_engine_cancel_clear(swd_engine* e);
+/* With radon_precision SWD_PREC_BF16X2 / _BF16X3 the spectra come from the tensor cores and the
+ * picker certifies each gather: a gather with any pick decision whose compared spectrum values
+ * differ by less than 1e-4 (of the column maximum) is recomputed in FP64 and picked again, so the
+ * picks are those of the FP64 spectrum.  gathers: gathers picked so far; recomputed: how many of
+ * them were recomputed.  No counterpart in the reference. */
+int swd_engine_radon_stats(swd_engine* e, uint64_t* gathers, uint64_t* recomputed);
 int swd_engine_stream(const swd_engine* e, void** stream);
 /* Split form of the gradient for several GPUs (shots sharded across ranks; the
  * parfor sum of SWD.m:193 becomes one all-reduce): the shot sums g_cl, g_cm,
@@ -391,7 +432,9 @@ int swd_server_submit(swd_server* s, const swd_request* req, uint64_t* id);
 /* Wait up to timeout_ms (< 0: forever) for request id; copies its outputs into out's buffers
  * and releases it.  SWD_ERR_TIMEOUT leaves it pending; otherwise returns its status. */
 int swd_server_wait(swd_server* s, uint64_t id, int timeout_ms, swd_request_result* out);
-/* Cancel a request that has not started (its wait returns SWD_ERR_CANCELLED). */
+/* Cancel a request: one still queued never starts; one already running has its engine's call
+ * cancelled (swd_engine_cancel).  Either way its wait returns SWD_ERR_CANCELLED.  A request that
+ * has finished cannot be cancelled (SWD_ERR_INVALID). */
 int swd_server_cancel(swd_server* s, uint64_t id);
 int swd_server_stats(swd_server* s, swd_server_stats_t* out);
 /* Cancel queued requests, wait for running ones, free every engine. */

@@ -7,7 +7,8 @@
  * (ADWDgrad_1.m:13, :46) is not read, as in the reference.  With SWD_ADWD_NORM set, the
  * structs also carry cr_r / cr_l (the picks minus vmin, SWD.m:178, :184), around which
  * ADWDgrad_norm.m weights the spectrum with normpdf(1:np, cr, 16).  With SWD_ADWD_LIMBAND set,
- * the call is ADWDgradlimband (core/ADWDgradlimband.m).
+ * the call is ADWDgradlimband (core/ADWDgradlimband.m); with SWD_ADWD_MAXNORM set, the field
+ * drivers' ADWDgrad_1 (the adjoint source over its largest magnitude).
  */
 #include <math.h>
 #include <string.h>
@@ -81,8 +82,13 @@ void mexFunction(int nlhs, mxArray* plhs[], int nrhs, const mxArray* prhs[]) {
 #ifndef SWD_ADWD_LIMBAND
 #define SWD_ADWD_LIMBAND 0
 #endif
+#ifndef SWD_ADWD_MAXNORM
+#define SWD_ADWD_MAXNORM 0
+#endif
   const int rc = SWD_ADWD_NORM ? swd_adwdgrad_norm(&p, ns, is, w, beta, go[0], go[1], space, mm[0], raw[0], cr[0],
                                                   mm[1], raw[1], cr[1], mxGetPr(plhs[0]))
+                 : SWD_ADWD_MAXNORM ? swd_adwdgrad_maxnorm(&p, ns, is, w, beta, go[0], go[1], space, mm[0], raw[0],
+                                                           mm[1], raw[1], mxGetPr(plhs[0]))
                  : SWD_ADWD_LIMBAND ? swd_adwdgrad_limband(&p, ns, is, w, beta, go[0], go[1], space, mm[0], raw[0],
                                                            mm[1], raw[1], mxGetPr(plhs[0]))
                                     : swd_adwdgrad(&p, ns, is, w, beta, go[0], go[1], space, mm[0], raw[0], mm[1],

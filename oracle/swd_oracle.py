@@ -448,8 +448,10 @@ def _argmax1(v):
     return int(np.argmax(v)) + 1  # first index of the max, 1-based
 
 
-def pickFDC1(ml, lp, fg, lfg):
-    """core/pickFDC1.m:1-131; returns (cr_0 after interpolation, dvmin, dvmax, raw idx, chazhi)."""
+def pickFDC1(ml, lp, fg, lfg, lpvalue=None):
+    """core/pickFDC1.m:1-131; returns (cr_0 after interpolation, dvmin, dvmax, raw idx, chazhi).
+    lpvalue: the seed pick of column lp given by the caller instead of the argmax of that column,
+    which is all that fieldexamples/outcrop/core/pickFDCValue.m:1-131 changes (its :20)."""
     ml = np.asarray(ml, np.float64)
     if np.isnan(ml).any():
         raise ValueError("pickFDC1: NaN in the spectrum is not supported")
@@ -460,7 +462,7 @@ def pickFDC1(ml, lp, fg, lfg):
     qujian = np.full(b + 1, np.nan)
     chazhi = np.ones(b + 1, np.int64)
     col = lambda i: ml[:, i - 1]
-    idx[lp] = _argmax1(col(lp))                                  # :19
+    idx[lp] = _argmax1(col(lp)) if lpvalue is None else int(lpvalue)  # :19
     for i in range(lp - 1, 0, -1):                               # :21-77
         if idx[i + 1] == a:
             idx[i] = a
@@ -547,6 +549,51 @@ def LHDispPick(ml, vmin, cr_0, method=1, ini=10):
         cr_pre = np.argmax(ml, axis=0) + 1 + vmin
     res = float(np.mean((cr_pre - np.asarray(cr_0, np.float64)) ** 2))
     return res, cr_pre
+
+
+def pickFDCValue(ml, lp, lpvalue, fg, lfg):
+    """fieldexamples/outcrop/core/pickFDCValue.m:1-131: pickFDC1 seeded with idx(lp) = lpvalue."""
+    return pickFDC1(ml, lp, fg, lfg, lpvalue=lpvalue)
+
+
+def LHDispPick_field(ml, ml_raw, vmin, cr_0, method=1, variant=1):
+    """The field-data LHDispPick variants, seeded at the global maximum of the unnormalised
+    spectrum ml_raw (saveForBackward.mlr / .mll, RTrAD.m:34): [~,ini] = max(max(mlr)) is the first
+    column holding the largest value, [~,iniP] = max(mlr(:,ini)) its first row of that value.
+
+    variant 1: fieldexamples/outcrop/core/LHDispPick.m:2-25, pickFDCValue(ml, ini, iniP, 2, 4)
+               for method 1, misfit over rows 15..end-15 (:24);
+    variant 2: fieldexamples/QadimahFault/core/LHDispPick.m:2-41 with its mode 1, pickFDC1(ml,
+               ini, 2, 4) whatever the method, misfit over rows 50..end-30 (:25).  That file also
+               calls pickdisp_xl / CEDC when the window holds more than 100 traces; mode 1 does not
+               use their results (and CEDC is not in the reference tree)."""
+    raw = np.asarray(ml_raw, np.float64)
+    ini = _argmax1(raw.max(axis=0))
+    b = np.asarray(ml).shape[1]
+    if variant == 1:
+        if method == 1:
+            cr, *_ = pickFDCValue(ml, ini, _argmax1(raw[:, ini - 1]), 2, 4)
+            cr_pre = cr + vmin
+        else:
+            cr_pre = np.argmax(ml, axis=0) + 1 + vmin
+        lo, hi = 15, b - 15
+    elif variant == 2:
+        cr, *_ = pickFDC1(ml, ini, 2, 4)
+        cr_pre = cr + vmin
+        lo, hi = 50, b - 30
+    else:
+        raise ValueError("variant must be 1 (outcrop) or 2 (QadimahFault)")
+    d = cr_pre - np.asarray(cr_0, np.float64)
+    res = float(np.mean(d[lo - 1:hi] ** 2)) if hi >= lo else float("nan")  # mean([]) is NaN
+    return res, cr_pre
+
+
+def norm_trace(data_in):
+    """core/norm_trace.m:1-22: each trace (column) divided by its largest magnitude; the guard for
+    an all-zero trace is commented out there, so such a trace becomes 0/0 = NaN."""
+    d = np.asarray(data_in, np.float64)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return d / np.nanmax(np.abs(d), axis=0, keepdims=True)  # MATLAB's max skips NaN
 
 
 # --------------------------------------------------------------------------------------
@@ -741,6 +788,14 @@ def ADWDgrad_1(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_
 # Gradient assembly
 # --------------------------------------------------------------------------------------
 
+def ADWDgrad_1_maxnorm(*args):
+    """fieldexamples/outcrop/core/ADWDgrad_1.m:1-81: ADWDgrad_1 with the adjoint source divided by
+    its largest magnitude at the end (:79), same arguments."""
+    a = ADWDgrad_1(*args)
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return a / np.nanmax(np.abs(a))
+
+
 def smooth2a(A, Nr, Nc):
     """core/smooth2a.m:38-76: (2Nr+1)x(2Nc+1) box mean with shrinking edges; NaNs are left out of
     the sums and counts and stay NaN in the output."""
@@ -773,8 +828,27 @@ def _survey_fd(s, is_, vs, single=True, adjoint=False, vp=None):
                      vp, vs, s.isfs, s.fd_order, s.source_type, s.nt_wf, single, adjoint)
 
 
+def _gno(s, is_):
+    """Shot number of the is_-th shot of s in its whole survey (a subset keeps them, shot_no)."""
+    no = getattr(s, "shot_no", None)
+    return int(no[is_ - 1]) if no is not None else is_
+
+
+def _ns(s):
+    """Shots of the whole survey (a subset keeps the count, ns_total)."""
+    return int(getattr(s, "ns_total", None) or s.ns)
+
+
+def _refsx(s, dgc):
+    """refsx of SWD.m:96 (receiver index of each source) over the whole survey's shot numbers."""
+    r = np.zeros(_ns(s))
+    r[[_gno(s, i) - 1 for i in range(1, s.ns + 1)]] = np.floor(np.asarray(s.sx) / dgc) + 1
+    return r
+
+
 def _sides(s, is_):
-    return has_right(is_, s.ns, s.m, s.M, s.w), has_left(is_, s.m, s.M, s.w)
+    g = _gno(s, is_)
+    return has_right(g, _ns(s), s.m, s.M, s.w), has_left(g, s.m, s.M, s.w)
 
 
 def _spectra(s, seis, is_):
@@ -782,8 +856,8 @@ def _spectra(s, seis, is_):
     r_on, l_on = _sides(s, is_)
     for side, on in (("r", r_on), ("l", l_on)):
         if on:
-            out[side] = radon(seis, is_, s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.ng, s.ds, s.offset, s.m,
-                              s.M, side, s.dv)
+            out[side] = radon(seis, _gno(s, is_), s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.ng, s.ds, s.offset,
+                              s.m, s.M, side, s.dv)
     return out
 
 
@@ -815,35 +889,48 @@ def _fd_pair(fd, single, accum_fp64):
 
 
 def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=False, single=True, vp=None, weight="softmax",
-                  fd="oracle"):
+                  fd="oracle", field=0):
     """SWD_single.m:172-193 for one shot: forward (FP32), spectra, picks, ADWDgrad_1, adjoint.
     single=False: SWD.m's double path (FP64 FD, adjoint source kept in double).  accum_fp64=False
     (default) sums the single path's images in FP32, as the reference's single MEX does.
-    fd="reference" runs the FD steps on the reference's own MEX sources (oracle/_ref)."""
+    fd="reference" runs the FD steps on the reference's own MEX sources (oracle/_ref).
+    field=1 / 2: the field-data flow (fieldexamples/outcrop/outcrop.m:168-196): norm_trace of the
+    predicted gather (in the data's precision), the field picker variant, the max-normalised
+    ADWDgrad_1 (fieldexamples/outcrop/core/ADWDgrad_1.m:79)."""
     fwd, adj = _fd_pair(fd, single, accum_fp64)
     inp = _survey_fd(s, is_, vs, single, vp=vp)
     _, sw, wf = fwd(inp, s.source())
+    if field:
+        sw_n = norm_trace(sw.astype(np.float64))
+        sw = sw_n.astype(np.float32) if single else sw_n
     sp = _spectra(s, sw.astype(np.float64), is_)
     npair = s.npair
     out = {"res_r": np.nan, "res_l": np.nan, "crp_r": np.ones(npair), "crp_l": np.ones(npair)}
+    def pick(sd, cr0):
+        if field:  # sd = (ml, noff, saved state) as radon() returns it
+            return LHDispPick_field(sd[0], sd[2]["ml_raw"], s.vmin, cr0, 1, field)
+        return LHDispPick(sd[0], s.vmin, cr0, 1, s.ini)
+
     if "r" in sp:
-        out["res_r"], out["crp_r"] = LHDispPick(sp["r"][0], s.vmin, cr0_r[:, is_ - 1], 1, s.ini)
+        out["res_r"], out["crp_r"] = pick(sp["r"], cr0_r[:, is_ - 1])
     if "l" in sp:
-        out["res_l"], out["crp_l"] = LHDispPick(sp["l"][0], s.vmin, cr0_l[:, is_ - 1], 1, s.ini)
+        out["res_l"], out["crp_l"] = pick(sp["l"], cr0_l[:, is_ - 1])
     gr = out["crp_r"] - cr0_r[:, is_ - 1]
     gl = out["crp_l"] - cr0_l[:, is_ - 1]
     if weight == "wd":  # SWD.m:188 (F1 = 0), ind/win of SWD.m:124-127, refsx of SWD.m:96
         dgc = int(s.gx[1] - s.gx[0])
         ind = s.fmin / s.df + 1
-        a = weight_data_muti3(sw, sw.astype(np.float64), is_, s.dt, s.df, s.offset, s.ds, 0, s.w, s.M, s.m, s.ns,
-                              np.floor(np.asarray(s.sx) / dgc) + 1, npair + 2 * ind, s.fmin, s.fmax,
+        a = weight_data_muti3(sw, sw.astype(np.float64), _gno(s, is_), s.dt, s.df, s.offset, s.ds, 0, s.w, s.M, s.m,
+                              _ns(s),
+                              _refsx(s, dgc), npair + 2 * ind, s.fmin, s.fmax,
                               cr0_r[:, is_ - 1], cr0_l[:, is_ - 1], out["crp_r"], out["crp_l"], ind)
     elif weight == "gauss":  # SWD.m:178,184 keep cr_pre - vmin in saveForBackward
-        a = ADWDgrad_norm(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl,
+        a = ADWDgrad_norm(s.nt, s.ng, _ns(s), npair, _gno(s, is_), s.w, s.m, s.M, s.soft_arg_norm, gr, gl,
                           sp.get("r", (0, 0, None))[2], sp.get("l", (0, 0, None))[2], out["crp_r"] - s.vmin,
                           out["crp_l"] - s.vmin)
     else:
-        a = ADWDgrad_1(s.nt, s.ng, s.ns, npair, is_, s.w, s.m, s.M, s.soft_arg_norm, gr, gl,
+        a = (ADWDgrad_1_maxnorm if field else ADWDgrad_1)(s.nt, s.ng, _ns(s), npair, _gno(s, is_), s.w, s.m, s.M,
+                                                          s.soft_arg_norm, gr, gl,
                        sp.get("r", (0, 0, None))[2], sp.get("l", (0, 0, None))[2])
     out["adj_src"] = a.astype(np.float32) if single else a
     ainp = _survey_fd(s, is_, vs, single, adjoint=True, vp=vp)
@@ -852,17 +939,17 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=False, single=True, vp=No
 
 
 def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=False, single=True, vp=None, weight="softmax",
-             fd="oracle"):
+             fd="oracle", field=0):
     """SWD_single.m:171-201 (SWD.m with single=False) with the shot sum in FP64 in shot order
     (per-shot images as shot_gradient)."""
     from concurrent.futures import ThreadPoolExecutor
     shots = list(range(1, s.ns + 1))
     if threads > 1:
         with ThreadPoolExecutor(threads) as ex:
-            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight, fd),
-                              shots))
+            per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight, fd,
+                                                      field), shots))
     else:
-        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight, fd) for i in shots]
+        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight, fd, field) for i in shots]
     g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
     for p in per:
         for k in g:
@@ -889,10 +976,10 @@ def misfit(s, vs, cr0_r, cr0_l, single=True, vp=None):
     that have a right side (res_r is only assigned for them, and they come first)."""
     res = []
     for is_ in range(1, s.ns + 1):
-        if not has_right(is_, s.ns, s.m, s.M, s.w):
+        if not _sides(s, is_)[0]:
             continue
         _, sw, _ = mex_staggerfd(_survey_fd(s, is_, vs, single, vp=vp), s.source(), want_wf=False)
-        ml = radon(sw.astype(np.float64), is_, s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.ng, s.ds, s.offset,
+        ml = radon(sw.astype(np.float64), _gno(s, is_), s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.ng, s.ds, s.offset,
                    s.m, s.M, "r", s.dv)[0]
         res.append(LHDispPick(ml, s.vmin, cr0_r[:, is_ - 1], 1, s.ini)[0])
     return float(np.mean(res))

@@ -51,6 +51,9 @@ _SIGS = {
     "swd_adwdgrad": [_rpp, _c_int, _c_int, _c_int, _c_dbl] + [_f64p] * 8,
     "swd_adwdgrad_norm": [_rpp, _c_int, _c_int, _c_int, _c_dbl] + [_f64p] * 10,
     "swd_adwdgrad_limband": [_rpp, _c_int, _c_int, _c_int, _c_dbl] + [_f64p] * 8,
+    "swd_adwdgrad_maxnorm": [_rpp, _c_int, _c_int, _c_int, _c_dbl] + [_f64p] * 8,
+    "swd_pick_field": [_f64p, _f64p, _c_int, _c_int, _c_dbl, _f64p, _c_int, _c_int, _f64p, _f64p],
+    "swd_norm_trace": [_f64p, _c_int, _c_int, _f64p],
     "swd_wd_residual": [_c_int, _c_int, _f64p, _f64p, _c_int, _c_dbl, _c_dbl, _c_int, _c_dbl, _c_int, _c_int,
                         _c_dbl, _c_int, _c_int, _f64p, _c_int, _c_dbl, _c_dbl] + [_f64p] * 4 + [_c_int, _f64p],
 }

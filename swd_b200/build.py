@@ -27,6 +27,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", os.path
 SOURCES = {
     "fd_host.cu": ["-fmad=false"],
     "fd_warpx.cu": ["-fmad=false"],
+    "fd_col2.cu": ["-fmad=false"],
     "model_prep.cu": ["-fmad=false"],
     "radon.cu": [],
     "engine.cu": ["-fmad=false"],

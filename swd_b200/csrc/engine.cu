@@ -13,7 +13,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <atomic>
 #include <map>
+#include <mutex>
 #include <memory>
 #include <vector>
 
@@ -92,6 +94,7 @@ struct swd_engine {
   // device memory
   DevBuf model;        // vp, vs (nz*nx each) + vmin
   DevBuf mat;          // packed materials {temp, ca, cl, cm1}
+  DevBuf mat2;         // the same per column pair, for the column-pair FD kernels (fd_col2.cuh)
   DevBuf fstate;       // forward state ping-pong [2][B][5][field]
   DevBuf astate;       // adjoint state ping-pong (checkpoint mode)
   DevBuf ckbuf;        // checkpoints [nseg][B][5][field]
@@ -108,16 +111,28 @@ struct swd_engine {
   bool have_source = false, have_observed = false;
   double tuned_fwd_us = 0, tuned_adj_us = 0;  // autotune: chosen variants' step times
   swd_contract* tc = nullptr;                  // split-BF16 forward contraction (radon_precision)
+  DevBuf cflag, ccount;                        // split-BF16 picks: gathers to recompute in FP64, their count
+  std::vector<int> valid_gathers;              // per batch: gathers with a window (picked)
+  uint64_t radon_gathers = 0;                  // gathers picked on split-BF16 spectra so far
   std::map<long, cudaGraphExec_t> graphs;
   std::vector<double> h_gres, h_crp;
   // optional per-phase timing of the last call (events on the engine stream)
   bool timing = false;
   std::vector<cudaEvent_t> ev;  // 4 per batch: before forward, after forward, after spectra, after adjoint
   double phase_ms[3] = {0, 0, 0};
+  // cancellation of a call in flight: swd_engine_cancel (any host thread) raises cancel_req and
+  // copies 1 into the device word cancelw on its own stream, which the FD kernels read
+  DevBuf cancelw;
+  std::atomic<int> cancel_req{0};
+  std::mutex cancel_mu;
+  cudaStream_t cst = nullptr;
+  int* h_one = nullptr;  // pinned 1, the source of that copy
   ~swd_engine() {
     if (tc) swd_contract_destroy(tc);
     for (auto& kv : graphs) cudaGraphExecDestroy(kv.second);
     for (auto x : ev) cudaEventDestroy(x);
+    if (cst) cudaStreamSynchronize(cst), cudaStreamDestroy(cst);
+    if (h_one) cudaFreeHost(h_one);
     if (st) cudaStreamDestroy(st);
   }
 };
@@ -189,6 +204,7 @@ static int alloc_all(swd_engine* e) {
   const size_t fieldB = (size_t)B * 5 * g.field;
   SWD_TRY(e->model.alloc((2 * n + 1) * sizeof(double)));
   SWD_TRY(e->mat.alloc(g.field * sizeof(float4)));
+  if (fd_col2_fits(g)) SWD_TRY(e->mat2.alloc(g.field * sizeof(float4)));
   SWD_TRY(e->fstate.alloc(2 * fieldB * sizeof(float)));
   if (e->mode == 2) {
     SWD_TRY(e->astate.alloc(2 * fieldB * sizeof(float)));
@@ -257,20 +273,21 @@ static int run_seq(swd_engine* e, long key, uint64_t nkernels, F&& body) {
 static FwdArgs<float> fwd_args(swd_engine* e, const FdGeom& g, int s0, int nb) {
   FwdArgs<float> a{};
   a.g = g;
-  a.mat = e->mat.as<float4>();
+  a.mat = g.sched == 3 ? e->mat2.as<float4>() : e->mat.as<float4>();  // pair-interleaved for schedule 3
   a.mb = nullptr;
   a.src = e->src.as<int2>() + s0;
   a.src_type = e->sv.source_type;
   a.s = e->wav.as<float>();
   a.dtx = (float)(e->sv.dt / e->sv.dx);
   a.n_shots = nb;
+  a.cancel = e->cancelw.as<int>();
   return a;
 }
 
 static AdjArgs<float> adj_args(swd_engine* e, const FdGeom& g, int nb) {
   AdjArgs<float> a{};
   a.g = g;
-  a.mat = e->mat.as<float4>();
+  a.mat = g.sched == 3 ? e->mat2.as<float4>() : e->mat.as<float4>();
   a.mb = nullptr;
   a.res = e->res.as<float>();
   a.img = e->img.as<double>();
@@ -278,6 +295,7 @@ static AdjArgs<float> adj_args(swd_engine* e, const FdGeom& g, int nb) {
   a.dtx = (float)(e->sv.dt / e->sv.dx);
   a.dt = (float)e->sv.dt;
   a.n_shots = nb;
+  a.cancel = e->cancelw.as<int>();
   return a;
 }
 
@@ -538,6 +556,50 @@ static int autotune(swd_engine* e) {
       if (rc != SWD_OK) break;
     }
   }
+  // column pairs (two steps per launch): warps per CTA, row slots and chunk height
+  if (rc == SWD_OK && fd_col2_fits(base) && e->mat2.p) {
+    FdGeom hc = base;
+    hc.sched = 3;
+    hc.warps = 4;
+    plan_decomposition(hc, e->B, 0);
+    std::vector<int> cch = {hc.chunk, std::max(8, hc.chunk * 2 / 3), std::min(rows, hc.chunk * 3 / 2),
+                            std::min(rows, hc.chunk * 2)};
+    std::sort(cch.begin(), cch.end());
+    cch.erase(std::unique(cch.begin(), cch.end()), cch.end());
+    for (int nw : {4, 2, 8}) {
+      for (int ch : cch) {
+        double bf = 1e30, ba = 1e30;
+        int rf = 4, ra = 4;
+        for (int slots : {4, 6}) {
+          if (!fd_col2_built(nw, slots)) continue;
+          FdGeom gc = base;
+          gc.nrec = snap_nrec;
+          gc.sched = 3;
+          gc.warps = nw;
+          gc.ring_fwd = gc.ring_adj = slots;
+          plan_decomposition(gc, e->B, ch);
+          float mf = 0, ma = 0;
+          if ((rc = time_steps(gc, true, &mf)) != SWD_OK) break;
+          if ((rc = time_steps(gc, false, &ma)) != SWD_OK) break;
+          if (mf < bf) { bf = mf; rf = slots; }
+          if (ma < ba) { ba = ma; ra = slots; }
+        }
+        if (rc != SWD_OK) break;
+        if (bf + ba < best) {
+          best = bf + ba;
+          pick = base;
+          pick.sched = 3;
+          pick.warps = nw;
+          pick.ring_fwd = rf;
+          pick.ring_adj = ra;
+          plan_decomposition(pick, e->B, ch);
+          e->tuned_fwd_us = bf * 1e3 / n;
+          e->tuned_adj_us = ba * 1e3 / n;
+        }
+      }
+      if (rc != SWD_OK) break;
+    }
+  }
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   if (rc != SWD_OK) return rc;
@@ -549,6 +611,12 @@ static int autotune(swd_engine* e) {
 }
 
 // Spectra, picks, misfits (+ adjoint sources when `grad`) for the gathers of one batch.
+// A split-BF16 spectrum column (normalised to 1) is within ~1e-5 of the FP64 one (measured:
+// 3.4e-6 relative L2 over the 100 x 600 survey's spectra); a pick decision whose two compared
+// values differ by more than ten times that cannot flip, so only gathers with a closer decision
+// are recomputed in FP64.
+constexpr double kBf16PickMargin = 1e-4;
+
 static int spectrum_batch(swd_engine* e, int bi, int s0, int nb, bool grad) {
   const RadonGeom& rg = e->rg;
   const int G = 2 * e->B;
@@ -558,17 +626,36 @@ static int spectrum_batch(swd_engine* e, int bi, int s0, int nb, bool grad) {
     SWD_CUDA(cudaMemsetAsync(e->D.p, 0, (size_t)G * rg.npair * rg.offset * sizeof(double2), e->st));
   }
   SWD_TRY(radon_dft<float>(rg, gs, G, e->seis.as<float>(), sstride, e->W.as<double2>(), e->D.as<double2>(), e->st));
+  const size_t go = (size_t)2 * s0;
+  auto pick = [&](PickSeed ps) {
+    return pick_batch(rg.np, rg.npair, G, e->sv.ini, e->sv.pick_method, e->sv.vmin, gs, e->ml.as<double>(),
+                      e->cr0.as<double>() + go * rg.npair, e->crp.as<double>() + go * rg.npair,
+                      e->dc.as<double>() + go * rg.npair, e->gres.as<double>() + go, e->status.as<int>() + go, e->st,
+                      ps);
+  };
   if (e->tc) {
+    // split-BF16 spectra on the tensor cores; the picker certifies each gather's decisions and
+    // the gathers with a decision inside kBf16PickMargin are recomputed in FP64 and picked again,
+    // so that the picks are the FP64 picks
     SWD_TRY(swd_contract_run(e->tc, e->D.as<double>(), e->MM.as<double>(), e->st));
     SWD_TRY(radon_amplitudes(rg, gs, G, e->MM.as<double2>(), e->mlraw.as<double>(), e->ml.as<double>(), e->st));
+    SWD_CUDA(cudaMemsetAsync(e->cflag.p, 0, G * sizeof(int), e->st));
+    PickSeed cert;
+    cert.cert = e->cflag.as<int>();
+    cert.delta = kBf16PickMargin;
+    cert.cert_count = e->ccount.as<unsigned long long>();
+    SWD_TRY(pick(cert));
+    SWD_TRY(radon_contract(rg, gs, G, e->K.as<double2>(), e->D.as<double2>(), e->MM.as<double2>(),
+                           e->mlraw.as<double>(), e->ml.as<double>(), e->st, e->cflag.as<int>()));
+    PickSeed again;
+    again.only = e->cflag.as<int>();
+    SWD_TRY(pick(again));
+    e->radon_gathers += (uint64_t)e->valid_gathers[bi];
   } else {
     SWD_TRY(radon_contract(rg, gs, G, e->K.as<double2>(), e->D.as<double2>(), e->MM.as<double2>(),
                            e->mlraw.as<double>(), e->ml.as<double>(), e->st));
+    SWD_TRY(pick(PickSeed{}));
   }
-  const size_t go = (size_t)2 * s0;
-  SWD_TRY(pick_batch(rg.np, rg.npair, G, e->sv.ini, e->sv.pick_method, e->sv.vmin, gs, e->ml.as<double>(),
-                     e->cr0.as<double>() + go * rg.npair, e->crp.as<double>() + go * rg.npair,
-                     e->dc.as<double>() + go * rg.npair, e->gres.as<double>() + go, e->status.as<int>() + go, e->st));
   if (!grad) return SWD_OK;
   if (e->opt.adjoint_weight == 2) {  // WD residual of the predicted data (SWD.m:188, F1 = 0)
     SWD_CUDA(cudaMemsetAsync(e->res.p, 0, (size_t)e->B * sstride * sizeof(float), e->st));
@@ -596,10 +683,25 @@ static int load_model(swd_engine* e, const double* vp, const double* vs, bool de
   SWD_CUDA(cudaMemcpyAsync(d + n, vs, n * sizeof(double), kind, e->st));
   SWD_TRY(vmin_device(d, d + n, n, d + 2 * n, e->st));
   SWD_TRY(prep_packed<float>(e->pp, d, d + n, d + 2 * n, e->mat.as<float4>(), e->g.pitch, e->st));
+  if (e->mat2.p) SWD_TRY(col2_material_pairs(e->mat.as<float4>(), e->mat2.as<float4>(), e->g.NZ, e->g.pitch, e->st));
   return SWD_OK;
 }
 
+// A cancel raised during (or before) this call: wait for its copy, clear the device word for the
+// next call, and report the call as cancelled (its results are partial and are not returned).
+static int take_cancel(swd_engine* e) {
+  if (!e->cancel_req.load()) return SWD_OK;
+  std::lock_guard<std::mutex> lk(e->cancel_mu);
+  SWD_CUDA(cudaStreamSynchronize(e->cst));
+  SWD_CUDA(cudaMemsetAsync(e->cancelw.p, 0, sizeof(int), e->st));
+  SWD_CUDA(cudaStreamSynchronize(e->st));
+  e->cancel_req.store(0);
+  set_error("the call was cancelled (swd_engine_cancel)");
+  return SWD_ERR_CANCELLED;
+}
+
 static int check_status(swd_engine* e) {
+  SWD_TRY(take_cancel(e));  // a cancelled call's picks are meaningless: report the cancel first
   std::vector<int> stv(2 * e->ns);
   SWD_CUDA(cudaMemcpyAsync(stv.data(), e->status.p, stv.size() * sizeof(int), cudaMemcpyDeviceToHost, e->st));
   SWD_CUDA(cudaStreamSynchronize(e->st));
@@ -724,7 +826,7 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   e->sv.sz = nullptr;
   e->sv.shot_no = nullptr;
   // option ranges: checked before the first CUDA call, so that they are reported on any host
-  SWD_CHECK(e->opt.fd_schedule >= 0 && e->opt.fd_schedule <= 5, "fd_schedule must lie in 0..5 (got %d)",
+  SWD_CHECK(e->opt.fd_schedule >= 0 && e->opt.fd_schedule <= 6, "fd_schedule must lie in 0..6 (got %d)",
             e->opt.fd_schedule);
   SWD_CHECK(e->opt.image_precision == 0 || e->opt.image_precision == 1, "image_precision must be 0 (FP32) or 1 (FP64)");
   SWD_CHECK(e->opt.adjoint_weight >= 0 && e->opt.adjoint_weight <= 2,
@@ -763,10 +865,12 @@ static int engine_setup(const swd_survey* s, const swd_engine_opts* o, swd_engin
   g.ring_adj = e->opt.ring_adj;
   // fd_schedule: 0 (default) and 3 warp streaming with two steps per launch, 1 one barrier per
   // row, 2 warp streaming one step per launch, 4 two barriers per row, 5 as 3 with two shots
-  // per warp in packed FP32 pairs
+  // per warp in packed FP32 pairs, 6 as 3 with two columns per lane in packed FP32 pairs
   const int fs = e->opt.fd_schedule;
-  g.sched = fs == 1 ? 1 : fs == 4 ? 0 : 2;
+  g.sched = fs == 1 ? 1 : fs == 4 ? 0 : fs == 6 ? 3 : 2;
   g.pairs = (fs == 0 || fs == 3) ? 1 : fs == 5 ? 2 : 0;
+  SWD_CHECK(fs != 6 || fd_col2_fits(g), "fd_schedule 6 (column pairs) needs even nbc and nx (got nbc %d, nx %d)",
+            g.nbc, g.nx);
   plan_decomposition(g, std::max(1, std::min(e->opt.max_batch > 0 ? e->opt.max_batch : e->ns, e->ns)),
                      e->opt.chunk_rows);
   // Radon geometry
@@ -807,7 +911,12 @@ static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engi
   for (int i = 0; i < e->ns; ++i)
     hsrc[i] = make_int2(e->sz[i] + e->pp.pad_top - 1, e->sx[i] + s->nbc - 1);
   SWD_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+  SWD_CUDA(cudaStreamCreateWithFlags(&e->cst, cudaStreamNonBlocking));
+  SWD_CUDA(cudaHostAlloc((void**)&e->h_one, sizeof(int), cudaHostAllocDefault));
+  *e->h_one = 1;
   SWD_TRY(alloc_all(e));
+  SWD_TRY(e->cancelw.alloc(sizeof(int)));
+  SWD_CUDA(cudaMemsetAsync(e->cancelw.p, 0, sizeof(int), e->st));
   SWD_CUDA(cudaMemcpyAsync(e->src.p, hsrc.data(), e->ns * sizeof(int2), cudaMemcpyHostToDevice, e->st));
   // gathers per batch (local shot index), validated against the reference's window rules
   std::vector<Gather> hg((size_t)e->nbatch * 2 * e->B);
@@ -825,6 +934,8 @@ static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engi
       }
     }
   SWD_CUDA(cudaMemcpyAsync(e->gath.p, hg.data(), hg.size() * sizeof(Gather), cudaMemcpyHostToDevice, e->st));
+  e->valid_gathers.assign(e->nbatch, 0);
+  for (size_t i = 0; i < hg.size(); ++i) e->valid_gathers[i / (2 * (size_t)e->B)] += hg[i].valid > 0 ? 1 : 0;
   SWD_TRY(radon_tables(e->rg, e->W.as<double2>(), e->K.as<double2>(), e->st));
   std::vector<Gather> hw;
   std::vector<double> hfre;
@@ -860,6 +971,9 @@ static int engine_create(const swd_survey* s, const swd_engine_opts* o, swd_engi
     for (int x = 0; x < rg.offset; ++x) off[x] = (rg.m + x) * rg.ds;
     SWD_TRY(swd_contract_create(rg.npair, fr.data(), rg.np, vel.data(), rg.offset, off.data(), 2 * e->B,
                                 e->opt.radon_precision, e->device, &e->tc));
+    SWD_TRY(e->cflag.alloc(2 * (size_t)e->B * sizeof(int)));
+    SWD_TRY(e->ccount.alloc(sizeof(unsigned long long)));
+    SWD_CUDA(cudaMemsetAsync(e->ccount.p, 0, sizeof(unsigned long long), e->st));
   } else {
     SWD_CHECK(e->opt.radon_precision == SWD_PREC_FP64, "radon_precision must be SWD_PREC_FP64, _BF16X2 or _BF16X3");
   }
@@ -902,7 +1016,7 @@ static void fill_info(const swd_engine* e, swd_engine_info_t* info) {
   info->ring_adj = e->g.ring_adj;
   info->tuned_fwd_us = e->tuned_fwd_us;
   info->tuned_adj_us = e->tuned_adj_us;
-  info->fd_schedule = fd_pairs(e->g) ? (e->g.pairs == 2 ? 5 : 3) : e->g.sched == 0 ? 4 : e->g.sched;
+  info->fd_schedule = e->g.sched == 3 ? 6 : fd_pairs(e->g) ? (e->g.pairs == 2 ? 5 : 3) : e->g.sched == 0 ? 4 : e->g.sched;
 }
 
 int swd_engine_info(const swd_engine* e, swd_engine_info_t* info) {
@@ -986,6 +1100,42 @@ int swd_engine_gradient_device(swd_engine* e, const double* d_vp, const double* 
     SWD_CUDA(cudaStreamSynchronize(e->st));
   }
   if (residual) SWD_TRY(copy_picks(e, nullptr, nullptr, nullptr, nullptr, residual));
+  return SWD_OK;
+}
+
+int swd_engine_cancel(swd_engine* e) {
+  clear_error();
+  SWD_CHECK(e, "null engine");
+  std::lock_guard<std::mutex> lk(e->cancel_mu);
+  SWD_CUDA(cudaSetDevice(e->device));
+  e->cancel_req.store(1);
+  SWD_CUDA(cudaMemcpyAsync(e->cancelw.p, e->h_one, sizeof(int), cudaMemcpyHostToDevice, e->cst));
+  return SWD_OK;
+}
+
+int swd_engine_cancel_clear(swd_engine* e) {
+  clear_error();
+  SWD_CHECK(e, "null engine");
+  if (!e->cancel_req.load()) return SWD_OK;
+  SWD_CUDA(cudaSetDevice(e->device));
+  std::lock_guard<std::mutex> lk(e->cancel_mu);
+  SWD_CUDA(cudaStreamSynchronize(e->cst));
+  SWD_CUDA(cudaMemsetAsync(e->cancelw.p, 0, sizeof(int), e->st));
+  SWD_CUDA(cudaStreamSynchronize(e->st));
+  e->cancel_req.store(0);
+  return SWD_OK;
+}
+
+int swd_engine_radon_stats(swd_engine* e, uint64_t* gathers, uint64_t* recomputed) {
+  clear_error();
+  SWD_CHECK(e && gathers && recomputed, "null argument");
+  *gathers = e->radon_gathers;
+  unsigned long long c = 0;
+  if (e->ccount.p) {
+    SWD_CUDA(cudaMemcpyAsync(&c, e->ccount.p, sizeof(c), cudaMemcpyDeviceToHost, e->st));
+    SWD_CUDA(cudaStreamSynchronize(e->st));
+  }
+  *recomputed = c;
   return SWD_OK;
 }
 

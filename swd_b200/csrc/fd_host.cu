@@ -123,6 +123,25 @@ bool fd_lead_built(int w, int c, int d) {
 
 void plan_decomposition(FdGeom& g, int n_shots, int chunk_rows) {
   const int rows = g.NZ - 2;
+  if (g.sched == 3) {  // column pairs (fd_col2.cuh): 60 output columns per warp, 2, 4 or 8 warps per CTA
+    if (g.warps != 2 && g.warps != 8) g.warps = 4;
+    g.cells = 2;
+    if (!fd_col2_built(g.warps, g.ring_fwd)) g.ring_fwd = 4;
+    if (!fd_col2_built(g.warps, g.ring_adj)) g.ring_adj = 4;
+    g.pairs = 0;
+    g.n_strips = (g.NX / 2 + kCol2Pairs - 1) / kCol2Pairs;
+    if (chunk_rows <= 0) {
+      // about 2.5 waves of warps (148 SMs x ~16 resident): 96 shots of 132 x 660 -> 22 rows
+      const long target = 148L * 16 * 5 / 2;
+      const long per = (long)g.n_strips * n_shots;
+      int nch = (int)((target + per - 1) / per);
+      nch = std::max(1, std::min(nch, std::max(1, rows / 8)));
+      chunk_rows = (rows + nch - 1) / nch;
+    }
+    g.chunk = std::max(1, std::min({chunk_rows, rows, kWarpChunkMax}));
+    g.n_chunks = (rows + g.chunk - 1) / g.chunk;
+    return;
+  }
   if (g.sched == 2) {  // warp streaming (fd_warp.cuh): 30 output columns per warp, warps per CTA 2, 4 or 8,
                        // 4, 6 or 8 register row slots (ring_fwd / ring_adj)
     if (g.warps != 2 && g.warps != 8) g.warps = 4;
@@ -302,6 +321,7 @@ template <typename T, int NF>
 int launch_fwd_step(const FwdArgs<T>& a, int it, cudaStream_t st) {
   if (a.mb) return fwd_impl<T, NF, 4, 1, 4, true>(a, it, st);
   if constexpr (NF == 3 && sizeof(T) == 4) {
+    if (a.g.sched == 3) return launch_fwd_step_c2(a, it, st);
     if (a.g.sched == 2) {
       switch (a.g.warps * 10 + a.g.ring_fwd) {
 #define X(w, s) case w * 10 + s: return fwd_warp_impl<w, s>(a, it, st);
@@ -338,6 +358,7 @@ template <typename T, int NF, bool IMG>
 static int adj_dispatch(const AdjArgs<T>& a, int it, cudaStream_t st) {
   if (a.mb) return adj_impl<T, NF, 4, 1, 4, true, IMG>(a, it, st);
   if constexpr (NF == 3 && sizeof(T) == 4) {
+    if (a.g.sched == 3) return launch_adj_step_c2(a, it, st);
     if (a.g.sched == 2) {
       switch (a.g.warps * 10 + a.g.ring_adj) {
 #define X(w, s) case w * 10 + s: return adj_warp_impl<w, s, IMG>(a, it, st);
@@ -378,6 +399,7 @@ int launch_adj_step(const AdjArgs<T>& a, int it, cudaStream_t st) {
   return adj_dispatch<T, NF, false>(a, it, st);
 }
 int launch_fwd_pair(const FwdArgs<float>& a, int it, cudaStream_t st) {
+  if (a.g.sched == 3) return launch_fwd_pair_c2(a, it, st);
   if (!fd_pairs(a.g) || a.mb || it + 1 >= a.g.nt) {
     set_error("internal: two-step forward launch outside the warp-streaming schedule");
     return SWD_ERR_INVALID;
@@ -394,6 +416,7 @@ int launch_fwd_pair(const FwdArgs<float>& a, int it, cudaStream_t st) {
 }
 
 int launch_adj_pair(const AdjArgs<float>& a, int it, cudaStream_t st) {
+  if (a.g.sched == 3) return launch_adj_pair_c2(a, it, st);
   if (!fd_pairs(a.g) || a.mb || it < 1) {
     set_error("internal: two-step adjoint launch outside the warp-streaming schedule");
     return SWD_ERR_INVALID;

@@ -14,6 +14,7 @@
 namespace swd {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kCol2Pairs = 30;  // column pairs written per warp by the column-pair kernels (fd_col2.cuh)
 
 template <typename T> struct Vec4;
 template <> struct Vec4<float> { using type = float4; };
@@ -34,7 +35,8 @@ struct FdGeom {
   int cells;                 // output columns per thread; a CTA owns 32*warps*cells columns
   int ring_fwd, ring_adj;    // rows in the shared-memory ring of the forward / adjoint kernels (4, 6, 8)
   int sched;                 // 0: two barriers per row (fd_smem.cuh); 1: one, velocities a row ahead (fd_lead.cuh);
-                             // 2: warp streaming (fd_warp.cuh; warps = warps per CTA)
+                             // 2: warp streaming (fd_warp.cuh; warps = warps per CTA); 3: warp streaming over
+                             // column pairs, two steps per launch (fd_col2.cuh; pair-interleaved state)
   int pairs;                 // schedule 2: 1 = forward and adjoint advance two steps per launch; 2 = the same
                              // with two shots per warp in packed FP32 pairs (fd_warpx.cuh)
   size_t field;              // NZ * pitch
@@ -59,6 +61,7 @@ struct FwdArgs {
   T* snap;                            // [shot][nrec][NF][nz][nx] (may be null)
   int rec0;                           // snapshot it/nt_wf is stored at index it/nt_wf - rec0
   int n_shots;
+  const int* cancel;                  // engine's cancel word (null: never cancelled)
 };
 
 template <typename T>
@@ -75,7 +78,16 @@ struct AdjArgs {
   T dtx, dt;
   int rec0;                           // snapshot it/nt_wf is read from index it/nt_wf - rec0
   int n_shots;
+  const int* cancel;                  // engine's cancel word (null: never cancelled)
 };
+
+// Cancellation of a call in flight: swd_engine_cancel sets a device word while the engine's time
+// loops run, and every FD launch of the engine returns as soon as it finds it set, so the rest
+// of a captured time loop drains as empty launches.  The decision is made once per warp (warp
+// kernels, before their first wait) or once per CTA (kernels with barriers), never per thread.
+__device__ __forceinline__ int cancel_word(const int* c) { return c ? *reinterpret_cast<const volatile int*>(c) : 0; }
+__device__ __forceinline__ bool warp_cancelled(const int* c) { return __any_sync(kFull, cancel_word(c) != 0); }
+__device__ __forceinline__ bool cta_cancelled(const int* c) { return __syncthreads_or(cancel_word(c) != 0) != 0; }
 
 // ---------------------------------------------------------------- forward
 

@@ -32,6 +32,7 @@ constexpr size_t lead_smem_bytes() {
 template <typename T, int NF, int W, int C, int D, bool GB, bool SNAP>
 __global__ void __launch_bounds__(32 * W)
 fd_fwd_lead(FwdArgs<T> a, int it) {
+  if (cta_cancelled(a.cancel)) return;  // every thread of the CTA reaches this first
   static_assert(D >= 4 && D % 2 == 0, "rows k+1, k+2 in use, rows in flight, even depth for static slots");
   constexpr int NT = 32 * W;
   using R = SRow<T, NT * C, GB>;
@@ -272,6 +273,7 @@ fd_fwd_lead(FwdArgs<T> a, int it) {
 template <typename T, int NF, int W, int C, int D, bool GB, bool IMG>
 __global__ void __launch_bounds__(32 * W)
 fd_adj_lead(AdjArgs<T> a, int it) {
+  if (cta_cancelled(a.cancel)) return;  // every thread of the CTA reaches this first
   static_assert(D >= 4 && D % 2 == 0, "rows k+1, k+2 in use, rows in flight, even depth for static slots");
   constexpr int NT = 32 * W;
   using R = SRow<T, NT * C, GB>;

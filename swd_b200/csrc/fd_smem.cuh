@@ -140,6 +140,7 @@ constexpr size_t smem_bytes() {
 template <typename T, int NF, int W, int C, int D, bool GB, bool SNAP>
 __global__ void __launch_bounds__(32 * W)
 fd_fwd_smem(FwdArgs<T> a, int it) {
+  if (cta_cancelled(a.cancel)) return;  // every thread of the CTA reaches this first
   static_assert(D >= 4 && D % 2 == 0, "rows k, k+1 in use, rows in flight, even depth for static slots");
   constexpr int NT = 32 * W;
   using R = SRow<T, NT * C, GB>;
@@ -369,6 +370,7 @@ __device__ __forceinline__ T adj_vel_w(bool inner, T ww, T Q1d, T Q1, T Q2d, T Q
 template <typename T, int NF, int W, int C, int D, bool GB, bool IMG>
 __global__ void __launch_bounds__(32 * W)
 fd_adj_smem(AdjArgs<T> a, int it) {
+  if (cta_cancelled(a.cancel)) return;  // every thread of the CTA reaches this first
   static_assert(D >= 4 && D % 2 == 0, "rows k, k+1 in use, rows in flight, even depth for static slots");
   constexpr int NT = 32 * W;
   using R = SRow<T, NT * C, GB>;

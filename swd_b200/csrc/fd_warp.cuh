@@ -178,6 +178,10 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp(FwdArgs<float> a, int it)
   // without moves.
 #pragma unroll
   for (int u = 0; u < NS; ++u) ld.issue(u, zs - 1 + u);
+  if (warp_cancelled(a.cancel)) {  // the flag load overlaps the rows in flight
+    wcp_wait<0>();
+    return;
+  }
   wcp_wait<NS - 2>();
   WRow RR[2];
   ld.read(RR[0], 0);
@@ -410,6 +414,10 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2(FwdArgs<float> a, int it
   // T1[(r - zs + 1) & 1].
 #pragma unroll
   for (int u = 0; u < NS; ++u) ld.issue(u, zs - 2 + u);
+  if (warp_cancelled(a.cancel)) {  // the flag load overlaps the rows in flight
+    wcp_wait<0>();
+    return;
+  }
   wcp_wait<NS - 2>();
   WRow RR[2];
   ld.read(RR[0], 0);
@@ -564,6 +572,10 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp(AdjArgs<float> a, int it)
 
 #pragma unroll
   for (int u = 0; u < NS; ++u) ld.issue(u, zs - 1 + u);
+  if (warp_cancelled(a.cancel)) {  // the flag load overlaps the rows in flight
+    wcp_wait<0>();
+    return;
+  }
   wcp_wait<NS - 2>();
   WRow RR[2];
   ld.read(RR[0], 0);
@@ -789,6 +801,10 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2(AdjArgs<float> a, int it
   for (int u = 0; u < NS; ++u) {
     issue_img(u, zs - 2 + u);
     ld.issue(u, zs - 2 + u);
+  }
+  if (warp_cancelled(a.cancel)) {  // the flag load overlaps the rows in flight
+    wcp_wait<0>();
+    return;
   }
   wcp_wait<NS - 2>();
   WRow RR[2];

@@ -273,6 +273,10 @@ __global__ void __launch_bounds__(32 * NW) fd_fwd_warp2x(FwdArgs<float> a, int i
   // slots and registers as in fd_fwd_warp2
 #pragma unroll
   for (int u = 0; u < NS; ++u) ld.issue(u, zs - 2 + u);
+  if (warp_cancelled(a.cancel)) {  // the flag load overlaps the rows in flight
+    wcp_wait<0>();
+    return;
+  }
   wcp_wait<NS - 2>();
   WRowX RR[2];
   ld.read(RR[0], 0);
@@ -503,6 +507,10 @@ __global__ void __launch_bounds__(32 * NW) fd_adj_warp2x(AdjArgs<float> a, int i
   for (int u = 0; u < NS; ++u) {
     issue_img(u, zs - 2 + u);
     ld.issue(u, zs - 2 + u);
+  }
+  if (warp_cancelled(a.cancel)) {  // the flag load overlaps the rows in flight
+    wcp_wait<0>();
+    return;
   }
   wcp_wait<NS - 2>();
   WRowX RR[2];

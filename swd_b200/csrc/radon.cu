@@ -204,12 +204,12 @@ __device__ double block_sum(double v, double* sm) {
 
 __global__ void __launch_bounds__(256) contract_kernel(RadonGeom g, const Gather* gs, const double2* __restrict__ K,
                                                        const double2* __restrict__ D, double2* MM, double* mlraw,
-                                                       double* ml) {
+                                                       double* ml, const int* only) {
   extern __shared__ double2 sd[];
   __shared__ double red[33];
   const int f = blockIdx.x, gi = blockIdx.y;
   const Gather gg = gs[gi];
-  if (gg.valid <= 0) return;
+  if (gg.valid <= 0 || (only && !only[gi])) return;  // the whole block returns
   const size_t col = ((size_t)gi * g.npair + f);
   for (int x = threadIdx.x; x < gg.noff; x += blockDim.x) sd[x] = D[col * g.offset + x];
   __syncthreads();
@@ -260,11 +260,11 @@ int radon_amplitudes(const RadonGeom& g, const Gather* d_gath, int G, const doub
 }
 
 int radon_contract(const RadonGeom& g, const Gather* d_gath, int G, const double2* K, const double2* D, double2* MM,
-                   double* mlraw, double* ml, cudaStream_t st) {
+                   double* mlraw, double* ml, cudaStream_t st, const int* only) {
   dim3 grid(g.npair, G);
   const size_t smem = (size_t)g.offset * sizeof(double2);
   if (smem > 48 * 1024) SWD_CUDA(cudaFuncSetAttribute(contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  contract_kernel<<<grid, 256, smem, st>>>(g, d_gath, K, D, MM, mlraw, ml);
+  contract_kernel<<<grid, 256, smem, st>>>(g, d_gath, K, D, MM, mlraw, ml, only);
   count_launch(1);
   SWD_CUDA(cudaGetLastError());
   return SWD_OK;
@@ -326,16 +326,67 @@ __device__ int warp_argmax(const double* y, int lo, int hi, int lane) {
   return bi;
 }
 
+// Margins of the picker's decisions (certification of a split-BF16 spectrum).
+// Adjacent samples compared by a findpeaks scan over y(lo:hi): min |y(q) - y(q-1)|, q = lo+1..hi.
+__device__ double warp_adjacent_gap(const double* y, int lo, int hi, int lane) {
+  double m = 1.0 / 0.0;
+  for (int q = lo + 1 + lane; q <= hi; q += 32) m = fmin(m, fabs(y[q - 1] - y[q - 2]));
+  for (int o = 16; o > 0; o >>= 1) m = fmin(m, __shfl_xor_sync(0xffffffffu, m, o));
+  return m;
+}
+// An argmax over y(lo:hi): the largest value minus the next largest (0 for a tie, inf for one sample).
+__device__ double warp_top2_gap(const double* y, int lo, int hi, int lane) {
+  double t1 = -1.0 / 0.0, t2 = -1.0 / 0.0;
+  for (int q = lo + lane; q <= hi; q += 32) {
+    const double v = y[q - 1];
+    if (v > t1) { t2 = t1; t1 = v; }
+    else if (v > t2) t2 = v;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double a1 = __shfl_xor_sync(0xffffffffu, t1, o), a2 = __shfl_xor_sync(0xffffffffu, t2, o);
+    const double n1 = fmax(t1, a1), n2 = fmax(fmin(t1, a1), fmax(t2, a2));
+    t1 = n1;
+    t2 = n2;
+  }
+  return t1 - t2;
+}
+
+// MATLAB [~,ini] = max(max(raw)) over a np x npair column-major spectrum: the first column
+// holding the largest value, 1-based (every lane returns it).
+__device__ int warp_colmax_argmax(const double* raw, int np, int npair, int lane) {
+  double bv = -1.0 / 0.0;
+  int bi = 0x7fffffff;
+  for (int i = 1 + lane; i <= npair; i += 32) {
+    const double* c = raw + (size_t)(i - 1) * np;
+    double m = -1.0 / 0.0;
+    for (int q = 0; q < np; ++q) m = fmax(m, c[q]);
+    if (m > bv || (m == bv && i < bi)) { bv = m; bi = i; }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+    if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
+  }
+  return bi;
+}
+
 __global__ void pick_kernel(int np, int npair, int G, int lp, int method, double fg, double lfg, double vmin,
                             const Gather* gs, const double* ml, const double* cr0, double* cr_pre, double* dc,
-                            double* res, int* status) {
+                            double* res, int* status, PickSeed seed) {
   extern __shared__ int psm[];
   const int gi = blockIdx.x;
   const int lane = threadIdx.x;
+  if (seed.only) {  // re-pick pass: only the flagged gathers, whose status starts over
+    if (!seed.only[gi]) return;
+    if (lane == 0) status[gi] = 0;
+    __syncwarp();
+  }
   if (gs && gs[gi].valid <= 0) {  // side not computed for this shot
     if (lane == 0) res[gi] = 0.0 / 0.0;
     return;
   }
+  const bool cert = seed.cert != nullptr;
+  double mg = 1.0 / 0.0;  // smallest decision margin (certification)
   int* idx = psm;                  // 1-based column arrays, entry 0 unused
   int* dvmin = idx + (npair + 1);
   int* dvmax = dvmin + (npair + 1);
@@ -348,20 +399,33 @@ __global__ void pick_kernel(int np, int npair, int G, int lp, int method, double
   bool bad = false;
   for (int i = lane; i < np * npair; i += 32) bad |= isnan(mlg[i]);
   if (__any_sync(0xffffffffu, bad)) {
-    if (lane == 0) status[gi] = 1;
+    if (lane == 0) {
+      status[gi] = 1;
+      if (seed.cert) seed.cert[gi] = 1;  // let the FP64 spectrum decide
+    }
     return;
   }
   double* crp = cr_pre + (size_t)gi * npair;
   if (method != 1) {  // LHDispPick.m:8-9: plain argmax per column
     for (int i = 1; i <= b; ++i) {
       const int q = warp_argmax(col(i), 1, a, lane);
+      if (cert) mg = fmin(mg, warp_top2_gap(col(i), 1, a, lane));
       if (lane == 0) crp[i - 1] = q + vmin;
     }
   } else {
     for (int i = lane; i <= b; i += 32) { idx[i] = 0; dvmin[i] = 0; dvmax[i] = 0; chazhi[i] = 1; qj[i] = 0.0 / 0.0; }
     __syncwarp();
     const double nanv = 0.0 / 0.0;
-    int cur = warp_argmax(col(lp), 1, a, lane);  // pickFDC1.m:19
+    int cur;
+    if (seed.raw) {  // field variants: start at the global maximum of the unnormalised spectrum
+      const double* rg = seed.raw + (size_t)gi * npair * np;
+      lp = warp_colmax_argmax(rg, np, npair, lane);  // [~,ini] = max(max(mlr))
+      cur = seed.value_from_raw ? warp_argmax(rg + (size_t)(lp - 1) * np, 1, a, lane)  // pickFDCValue.m:20
+                                : warp_argmax(col(lp), 1, a, lane);
+    } else {
+      cur = warp_argmax(col(lp), 1, a, lane);  // pickFDC1.m:19
+      if (cert) mg = fmin(mg, warp_top2_gap(col(lp), 1, a, lane));
+    }
     if (lane == 0) idx[lp] = cur;
     for (int i = lp - 1; i >= 1; --i) {          // pickFDC1.m:21-77
       __syncwarp();
@@ -372,9 +436,17 @@ __global__ void pick_kernel(int np, int npair, int G, int lp, int method, double
       }
       int vmx, vmn;
       if (prev > a - 3) vmx = a;
-      else { const int q = first_local_min(col(i), prev, a, lane); vmx = q ? q + 1 : a; }
+      else {
+        const int q = first_local_min(col(i), prev, a, lane);
+        vmx = q ? q + 1 : a;
+        if (cert) mg = fmin(mg, warp_adjacent_gap(col(i), prev, q ? min(q + 1, a) : a, lane));
+      }
       if (prev < 3) vmn = 1;
-      else { const int q = last_local_min(col(i), prev, lane); vmn = q ? q : 1; }
+      else {
+        const int q = last_local_min(col(i), prev, lane);
+        vmn = q ? q : 1;
+        if (cert) mg = fmin(mg, warp_adjacent_gap(col(i), q ? q - 1 : 1, prev, lane));
+      }
       const double qi = (double)(vmx - vmn);
       const double qn = qj[i + 1];
       int newidx;
@@ -385,6 +457,7 @@ __global__ void pick_kernel(int np, int npair, int G, int lp, int method, double
         if (lane == 0) { chazhi[i] = 0; }
       } else {
         newidx = warp_argmax(col(i), vmn, vmx, lane);
+        if (cert) mg = fmin(mg, warp_top2_gap(col(i), vmn, vmx, lane));
       }
       __syncwarp();
       if (lane == 0) { idx[i] = newidx; dvmax[i] = vmx; dvmin[i] = vmn; qj[i] = (double)(vmx - vmn); }
@@ -394,9 +467,17 @@ __global__ void pick_kernel(int np, int npair, int G, int lp, int method, double
       const int prev = idx[i - 1];
       int vmx, vmn;
       if (prev > a - 3) vmx = a;
-      else { const int q = first_local_min(col(i), prev, a, lane); vmx = q ? q + 1 : a; }
+      else {
+        const int q = first_local_min(col(i), prev, a, lane);
+        vmx = q ? q + 1 : a;
+        if (cert) mg = fmin(mg, warp_adjacent_gap(col(i), prev, q ? min(q + 1, a) : a, lane));
+      }
       if (prev < 3) vmn = 1;
-      else { const int q = last_local_min(col(i), prev, lane); vmn = q ? q : 1; }
+      else {
+        const int q = last_local_min(col(i), prev, lane);
+        vmn = q ? q : 1;
+        if (cert) mg = fmin(mg, warp_adjacent_gap(col(i), q ? q - 1 : 1, prev, lane));
+      }
       const double qi = (double)(vmx - vmn);
       const double qp = qj[i - 1];
       int newidx;
@@ -407,6 +488,7 @@ __global__ void pick_kernel(int np, int npair, int G, int lp, int method, double
         if (lane == 0) chazhi[i] = 0;
       } else {
         newidx = warp_argmax(col(i), vmn, vmx, lane);
+        if (cert) mg = fmin(mg, warp_top2_gap(col(i), vmn, vmx, lane));
       }
       __syncwarp();
       if (lane == 0) { idx[i] = newidx; dvmax[i] = vmx; dvmin[i] = vmn; qj[i] = (double)(vmx - vmn); }
@@ -446,23 +528,30 @@ __global__ void pick_kernel(int np, int npair, int G, int lp, int method, double
   }
   __syncwarp();
   if (lane == 0 && status[gi] == 0) {
+    // misfit over rows r0..r1 (1-based; all rows unless a field variant trims them), mean([]) = NaN
+    const int r0 = seed.r0 > 0 ? seed.r0 : 1, r1 = seed.r0 > 0 ? b - seed.r1_from_end : b;
     double s = 0.0;
     for (int i = 0; i < b; ++i) {
       const double d = crp[i] - cr0[(size_t)gi * npair + i];
       dc[(size_t)gi * npair + i] = d;
-      s += d * d;
+      if (i + 1 >= r0 && i + 1 <= r1) s += d * d;
     }
-    res[gi] = s / b;
+    res[gi] = r1 >= r0 ? s / (r1 - r0 + 1) : 0.0 / 0.0;
+  }
+  if (cert && lane == 0 && !(mg >= seed.delta)) {  // a decision within delta (or NaN): recompute in FP64
+    seed.cert[gi] = 1;
+    if (seed.cert_count) atomicAdd(seed.cert_count, 1ull);
   }
 }
 
 int pick_batch(int np, int npair, int G, int ini, int method, double vmin, const Gather* d_gath, const double* ml,
-               const double* cr0, double* cr_pre, double* dc, double* res, int* status, cudaStream_t st) {
-  SWD_CHECK(ini >= 1 && ini <= npair, "ini (%d) must lie in 1..npair (%d)", ini, npair);
+               const double* cr0, double* cr_pre, double* dc, double* res, int* status, cudaStream_t st,
+               PickSeed seed) {
+  SWD_CHECK(seed.raw || (ini >= 1 && ini <= npair), "ini (%d) must lie in 1..npair (%d)", ini, npair);
   const size_t smem = (size_t)(npair + 1) * (4 * sizeof(int) + sizeof(double));
-  SWD_CUDA(cudaMemsetAsync(status, 0, G * sizeof(int), st));
+  if (!seed.only) SWD_CUDA(cudaMemsetAsync(status, 0, G * sizeof(int), st));
   pick_kernel<<<G, 32, smem, st>>>(np, npair, G, ini, method, 2.0, 4.0, vmin, d_gath, ml, cr0, cr_pre, dc, res,
-                                   status);
+                                   status, seed);
   count_launch(1);
   SWD_CUDA(cudaGetLastError());
   return SWD_OK;
@@ -725,13 +814,115 @@ int swd_pick(const double* ml, int np_, int npair, double vmin, const double* cr
   return SWD_OK;
 }
 
+int swd_pick_field(const double* ml, const double* ml_raw, int np_, int npair, double vmin, const double* cr_0,
+                   int method, int variant, double* res, double* cr_pre) {
+  clear_error();
+  SWD_CHECK(ml && ml_raw && cr_0 && cr_pre && np_ >= 1 && npair >= 1, "bad pick arguments");
+  SWD_CHECK(variant == 1 || variant == 2, "variant must be 1 (outcrop) or 2 (QadimahFault)");
+  const size_t spec = (size_t)np_ * npair;
+  DevBuf b;
+  SWD_TRY(b.alloc((2 * spec + 3 * (size_t)npair + 1) * sizeof(double) + sizeof(int)));
+  double* d_ml = b.as<double>();
+  double* d_raw = d_ml + spec;
+  double* d_cr0 = d_raw + spec;
+  double* d_crp = d_cr0 + npair;
+  double* d_dc = d_crp + npair;
+  double* d_res = d_dc + npair;
+  int* d_st = (int*)(d_res + 1);
+  cudaStream_t st = 0;
+  SWD_CUDA(cudaMemcpyAsync(d_ml, ml, spec * sizeof(double), cudaMemcpyHostToDevice, st));
+  SWD_CUDA(cudaMemcpyAsync(d_raw, ml_raw, spec * sizeof(double), cudaMemcpyHostToDevice, st));
+  SWD_CUDA(cudaMemcpyAsync(d_cr0, cr_0, npair * sizeof(double), cudaMemcpyHostToDevice, st));
+  PickSeed seed;
+  seed.raw = d_raw;
+  seed.value_from_raw = variant == 1;  // pickFDCValue seeds from mlr; pickFDC1 from ml
+  seed.r0 = variant == 1 ? 15 : 50;    // misfit rows 15:end-15 / 50:end-30
+  seed.r1_from_end = variant == 1 ? 15 : 30;
+  SWD_TRY(pick_batch(np_, npair, 1, 1, variant == 2 ? 1 : method, vmin, nullptr, d_ml, d_cr0, d_crp, d_dc, d_res,
+                     d_st, st, seed));
+  int status = 0;
+  SWD_CUDA(cudaMemcpyAsync(&status, d_st, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SWD_CUDA(cudaMemcpyAsync(cr_pre, d_crp, npair * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (res) SWD_CUDA(cudaMemcpyAsync(res, d_res, sizeof(double), cudaMemcpyDeviceToHost, st));
+  SWD_CUDA(cudaStreamSynchronize(st));
+  if (status == 1) { set_error("NaN in the dispersion spectrum"); return SWD_ERR_NUMERIC; }
+  if (status == 2) { set_error("interp1 needs at least two retained picks (pickFDC1.m:129)"); return SWD_ERR_NUMERIC; }
+  return SWD_OK;
+}
+
 }  // extern "C"
 
-// ADWDgrad_1 (mode 0), ADWDgrad_norm (mode 1, picks cr_r / cr_l) or ADWDgradlimband (mode 2) of one shot.
+// each trace (a column of the MATLAB nt x ng array, contiguous) divided by its largest magnitude
+__global__ void norm_trace_kernel(const double* __restrict__ in, double* __restrict__ out, int nt) {
+  __shared__ unsigned long long wm[32];
+  const double* c = in + (size_t)blockIdx.x * nt;
+  unsigned long long m = 0;
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+    const double v = fabs(c[t]);
+    if (!isnan(v)) m = max(m, (unsigned long long)__double_as_longlong(v));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = m;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    m = threadIdx.x < (blockDim.x >> 5) ? wm[threadIdx.x] : 0ull;
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if (threadIdx.x == 0) wm[0] = m;
+  }
+  __syncthreads();
+  const double d = __longlong_as_double((long long)wm[0]);
+  for (int t = threadIdx.x; t < nt; t += blockDim.x) out[(size_t)blockIdx.x * nt + t] = c[t] / d;
+}
+
+extern "C" int swd_norm_trace(const double* data_in, int nt, int ng, double* data_out) {
+  clear_error();
+  SWD_CHECK(data_in && data_out && nt >= 1 && ng >= 1, "bad norm_trace arguments");
+  const size_t n = (size_t)nt * ng;
+  DevBuf b;
+  SWD_TRY(b.alloc(2 * n * sizeof(double)));
+  cudaStream_t st = 0;
+  SWD_CUDA(cudaMemcpyAsync(b.p, data_in, n * sizeof(double), cudaMemcpyHostToDevice, st));
+  norm_trace_kernel<<<ng, 256, 0, st>>>(b.as<double>(), b.as<double>() + n, nt);
+  count_launch(1);
+  SWD_CUDA(cudaGetLastError());
+  SWD_CUDA(cudaMemcpyAsync(data_out, b.as<double>() + n, n * sizeof(double), cudaMemcpyDeviceToHost, st));
+  SWD_CUDA(cudaStreamSynchronize(st));
+  return SWD_OK;
+}
+
+// max |x| over n values, NaN skipped as MATLAB's max skips it: non-negative doubles order as their
+// bit patterns, so an atomic max on the bits of |x| finds it (0 when every value is NaN or 0).
+__global__ void maxabs_kernel(const double* __restrict__ x, size_t n, unsigned long long* out) {
+  unsigned long long m = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const double v = fabs(x[i]);
+    if (!isnan(v)) m = max(m, (unsigned long long)__double_as_longlong(v));
+  }
+  for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+__global__ void scale_by_kernel(double* x, size_t n, const unsigned long long* m) {
+  const double d = __longlong_as_double((long long)*m);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    x[i] = x[i] / d;  // 0/0 = NaN when the array is all zero, as in MATLAB
+}
+// x ./ max(abs(x(:))) in place (fieldexamples/outcrop/core/ADWDgrad_1.m:79); m: one device word
+static int divide_by_maxabs(double* x, size_t n, unsigned long long* m, cudaStream_t st) {
+  SWD_CUDA(cudaMemsetAsync(m, 0, sizeof(unsigned long long), st));
+  const unsigned blocks = (unsigned)std::min<size_t>((n + 255) / 256, 1184);
+  maxabs_kernel<<<blocks, 256, 0, st>>>(x, n, m);
+  scale_by_kernel<<<blocks, 256, 0, st>>>(x, n, m);
+  count_launch(2);
+  SWD_CUDA(cudaGetLastError());
+  return SWD_OK;
+}
+
+// ADWDgrad_1 (mode 0), ADWDgrad_norm (mode 1, picks cr_r / cr_l) or ADWDgradlimband (mode 2) of one
+// shot; maxnorm divides the adjoint source by its largest magnitude (the field-data ADWDgrad_1).
 static int adwdgrad_impl(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
                          const double* grad_output_r, const double* grad_output_l, const double* space_m,
                          const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
-                         const double* cr_r, const double* cr_l, int mode, double* a_data_res) {
+                         const double* cr_r, const double* cr_l, int mode, double* a_data_res, bool maxnorm = false) {
   const bool gauss = mode == 1;
   RadonGeom g{};
   SWD_TRY(radon_geom(p, g));
@@ -753,7 +944,8 @@ static int adwdgrad_impl(const swd_radon_params* p, int ns, int is, int w, doubl
     }
   }
   const size_t spec = (size_t)g.npair * g.np, nsz = (size_t)g.nt * g.ng;
-  DevBuf b_W, b_K, b_MM, b_raw, b_dc, b_sm, b_Gx, b_out, b_out_t, b_g, b_cr, b_tab;
+  DevBuf b_W, b_K, b_MM, b_raw, b_dc, b_sm, b_Gx, b_out, b_out_t, b_g, b_cr, b_tab, b_max;
+  if (maxnorm) SWD_TRY(b_max.alloc(sizeof(unsigned long long)));
   if (gauss) SWD_TRY(b_cr.alloc(2 * (size_t)g.npair * sizeof(double)));
   SWD_TRY(b_W.alloc((size_t)g.npair * g.ntd * sizeof(double2)));
   SWD_TRY(b_K.alloc((size_t)g.npair * g.offset * g.np * sizeof(double2)));
@@ -814,6 +1006,7 @@ static int adwdgrad_impl(const swd_radon_params* p, int ns, int is, int w, doubl
   SWD_TRY(radon_idft_scatter<double>(g, b_g.as<Gather>(), 2, b_Gx.as<double2>(), b_W.as<double2>(),
                                      b_out.as<double>(), 0, st, mode == 2 ? b_tab.as<double2>() : nullptr,
                                      mode == 2 ? b_tab.as<double2>() + g.ntd : nullptr));
+  if (maxnorm) SWD_TRY(divide_by_maxabs(b_out.as<double>(), nsz, b_max.as<unsigned long long>(), st));
   // [nt][ng] -> MATLAB nt x ng
   SWD_TRY(transpose<double, double>(b_out.as<double>(), 0, b_out_t.as<double>(), 0, 1, g.nt, g.ng, st));
   SWD_CUDA(cudaMemcpyAsync(a_data_res, b_out_t.p, nsz * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -829,6 +1022,15 @@ int swd_adwdgrad(const swd_radon_params* p, int ns, int is, int w, double soft_a
   clear_error();
   return adwdgrad_impl(p, ns, is, w, soft_arg_norm, grad_output_r, grad_output_l, space_m, mm_r, ml_raw_r, mm_l,
                        ml_raw_l, nullptr, nullptr, 0, a_data_res);
+}
+
+int swd_adwdgrad_maxnorm(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,
+                         const double* grad_output_r, const double* grad_output_l, const double* space_m,
+                         const double* mm_r, const double* ml_raw_r, const double* mm_l, const double* ml_raw_l,
+                         double* a_data_res) {
+  clear_error();
+  return adwdgrad_impl(p, ns, is, w, soft_arg_norm, grad_output_r, grad_output_l, space_m, mm_r, ml_raw_r, mm_l,
+                       ml_raw_l, nullptr, nullptr, 0, a_data_res, true);
 }
 
 int swd_adwdgrad_limband(const swd_radon_params* p, int ns, int is, int w, double soft_arg_norm,

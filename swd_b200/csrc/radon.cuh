@@ -39,15 +39,34 @@ template <typename S>
 int radon_dft(const RadonGeom& g, const Gather* d_gath, int G, const S* seis, size_t sstride, const double2* W,
               double2* D, cudaStream_t st);
 // MM[g][f][p] = sum_x K[f][x][p] D[g][f][x]; mlraw = |MM|; ml = mlraw / max_p mlraw
+// only (nullable, [G]): gathers with only[g] == 0 are left as they are
 int radon_contract(const RadonGeom& g, const Gather* d_gath, int G, const double2* K, const double2* D, double2* MM,
-                   double* mlraw, double* ml, cudaStream_t st);
+                   double* mlraw, double* ml, cudaStream_t st, const int* only = nullptr);
 // mlraw = |MM|, ml = mlraw / max_p mlraw for an MM computed elsewhere (valid gathers only)
 int radon_amplitudes(const RadonGeom& g, const Gather* d_gath, int G, const double2* MM, double* mlraw, double* ml,
                      cudaStream_t st);
 // pickFDC1 + LHDispPick per gather: cr_pre = picks + vmin, res = mean((cr_pre-cr0)^2), dc = cr_pre - cr0.
 // Gathers with valid <= 0 are skipped (res = NaN); d_gath may be null (all gathers picked).
+// Options of the guided picker.
+//  * Field-data variants: raw ([g][npair][np], the unnormalised spectrum) picks the seed column as
+//    the first one holding its global maximum, and the seed row from raw (value_from_raw,
+//    pickFDCValue) or from ml (pickFDC1); r0 > 0 restricts the misfit to rows r0..npair-r1_from_end.
+//  * Certification (split-BF16 spectra): with cert set, every hard decision records its margin
+//    (the gap between the compared spectrum values: top two of each argmax, adjacent samples of
+//    each local-minimum scan) and a gather with a margin below delta gets cert[g] = 1 (and
+//    cert_count is incremented); with only set, gathers whose only[g] is 0 are skipped.
+struct PickSeed {
+  const double* raw = nullptr;
+  int value_from_raw = 0;
+  int r0 = 0, r1_from_end = 0;
+  int* cert = nullptr;
+  double delta = 0.0;
+  unsigned long long* cert_count = nullptr;
+  const int* only = nullptr;
+};
 int pick_batch(int np, int npair, int G, int ini, int method, double vmin, const Gather* d_gath, const double* ml,
-               const double* cr0, double* cr_pre, double* dc, double* res, int* status, cudaStream_t st);
+               const double* cr0, double* cr_pre, double* dc, double* res, int* status, cudaStream_t st,
+               PickSeed seed = PickSeed{});
 // SoftMax gradient + adjoint Radon: Gx[g][f][x] = sum_p conj(K[f][x][p]) * gm[g][f][p];
 // with `pick` ([g][f]) the weights are ADWDgrad_norm's Gaussian around pick - pick_off (= cr_pre - vmin);
 // with `limband` they are ADWDgradlimband's power weights, mlr.^beta normalised per column

@@ -45,6 +45,8 @@ struct Request {
   int status = SWD_OK;
   std::string err;
   bool done = false, cancelled = false, reused = false;
+  bool cancel_running = false;  // cancelled after it started: its engine's time loops are told to stop
+  swd_engine* eng = nullptr;    // the engine running it (set by its worker, under the server lock)
   size_t bytes = 0;
   Clock::time_point t_submit, t_start, t_done;
 };
@@ -124,16 +126,33 @@ static void worker(swd_server* S, std::shared_ptr<Request> r, swd_engine* eng) {
     o.device = S->opt.device;
     rc = swd_engine_create(&r->sv, &o, &eng);
   }
+  if (rc == SWD_OK) {
+    std::lock_guard<std::mutex> lk(S->mu);
+    r->eng = eng;
+    if (r->cancel_running) rc = swd_engine_cancel(eng);  // cancelled while its engine was being built
+  }
   if (rc == SWD_OK) rc = run_request(S, *r, eng);
   std::string err = rc == SWD_OK ? "" : swd_last_error();
   std::lock_guard<std::mutex> lk(S->mu);
+  if (r->cancel_running && eng) {
+    // cancelled while running: a cancel that landed after the engine's call had finished is
+    // still pending on the engine; withdraw it so that it cannot cancel the next request, and
+    // report this one as cancelled either way
+    const int crc = swd_engine_cancel_clear(eng);
+    if (rc == SWD_OK || rc == SWD_ERR_CANCELLED) {
+      rc = crc == SWD_OK ? SWD_ERR_CANCELLED : crc;
+      err = crc == SWD_OK ? "request cancelled while running" : swd_last_error();
+    }
+  }
   r->status = rc;
   r->err = err;
   r->t_done = Clock::now();
   r->done = true;
+  r->eng = nullptr;
   S->inflight--;
   S->st.completed++;
-  if (eng && rc == SWD_OK && r->key != 0 && S->opt.keep_engines) {
+  // a cancelled call leaves its engine ready for the next one (the cancel word is cleared)
+  if (eng && (rc == SWD_OK || rc == SWD_ERR_CANCELLED) && r->key != 0 && S->opt.keep_engines) {
     Idle d{r->key, r->sv, eng, r->bytes};
     d.sv.sx = d.sv.sz = nullptr;
     d.sv.shot_no = nullptr;
@@ -322,12 +341,19 @@ int swd_server_cancel(swd_server* S, uint64_t id) {
   auto it = S->reqs.find(id);
   SWD_CHECK(it != S->reqs.end(), "unknown request id %llu", (unsigned long long)id);
   auto& r = it->second;
-  if (r->done || r->t_start != Clock::time_point{}) {
-    set_error("request %llu already started", (unsigned long long)id);
+  if (r->done) {
+    set_error("request %llu already finished", (unsigned long long)id);
     return SWD_ERR_INVALID;
   }
-  r->cancelled = true;
   S->st.cancelled++;
+  if (r->t_start != Clock::time_point{}) {
+    // running: its engine's FD launches return at once from here on, and the call reports
+    // SWD_ERR_CANCELLED to swd_server_wait; an engine still being built is told when it is ready
+    r->cancel_running = true;
+    if (r->eng) SWD_TRY(swd_engine_cancel(r->eng));
+    return SWD_OK;
+  }
+  r->cancelled = true;
   S->cv_done.notify_all();
   S->cv_sched.notify_all();
   return SWD_OK;

@@ -72,6 +72,9 @@ def _bind():
         "swd_engine_gradient": [vp, _dp, _dp, ctypes.POINTER(GradientOut)],
         "swd_engine_gradient_device": [vp, vp, vp, vp, _dp],
         "swd_engine_stream": [vp, ctypes.POINTER(vp)],
+        "swd_engine_cancel": [vp],
+        "swd_engine_cancel_clear": [vp],
+        "swd_engine_radon_stats": [vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)],
         "swd_engine_shot_sums_device": [vp, vp, vp, vp, _dp, _ip],
         "swd_engine_assemble_device": [vp, vp, vp],
         "swd_engine_set_timing": [vp, _i],
@@ -89,7 +92,8 @@ ENGINE_SYMBOLS = ["swd_engine_create", "swd_engine_destroy", "swd_engine_info", 
                   "swd_engine_set_observed", "swd_engine_observed_curves", "swd_engine_misfit",
                   "swd_engine_gradient", "swd_engine_gradient_device", "swd_engine_stream",
                   "swd_engine_shot_sums_device", "swd_engine_assemble_device", "swd_engine_set_timing",
-                  "swd_engine_phase_times"]
+                  "swd_engine_phase_times", "swd_engine_cancel", "swd_engine_cancel_clear",
+                  "swd_engine_radon_stats"]
 
 
 def survey_struct(s):
@@ -205,6 +209,19 @@ class GradientEngine:
              ctypes.c_void_p(d_vs.data_ptr()), ctypes.c_void_p(d_dk.data_ptr() if d_dk is not None else 0),
              ctypes.byref(r))
         return r.value
+
+    def radon_stats(self):
+        """Split-BF16 spectra: gathers picked so far and how many were recomputed in FP64 because a
+        pick decision fell inside the certification margin."""
+        g, r = ctypes.c_uint64(), ctypes.c_uint64()
+        call("swd_engine_radon_stats", self._h, ctypes.byref(g), ctypes.byref(r))
+        return {"gathers": g.value, "recomputed_fp64": r.value}
+
+    def cancel(self):
+        """Cancel the call in flight on this engine (from another thread; returns at once): that
+        call raises SwdError with status SWD_ERR_CANCELLED (5); a cancel raised while no call
+        runs cancels the next one."""
+        call("swd_engine_cancel", self._h)
 
     def stream(self):
         p = ctypes.c_void_p()

@@ -6,6 +6,10 @@
     ADWDgrad_norm               core/ADWDgrad_norm.m:1
     ADWDgradlimband             core/ADWDgradlimband.m:1
     weight_data_muti3           core/weight_data_muti3.m:1 (the WD adjoint source)
+    norm_trace                  core/norm_trace.m:1
+    LHDispPick_field            fieldexamples/outcrop/core/LHDispPick.m:2 (pickFDCValue.m:1),
+                                fieldexamples/QadimahFault/core/LHDispPick.m:2 (mode 1)
+    ADWDgrad_1_maxnorm          fieldexamples/outcrop/core/ADWDgrad_1.m:1
 
 Each call runs on the GPU through libswd.so (FP64, like the reference's MATLAB
 code).  Arrays use MATLAB's layout; saveForBackward is a dict with the
@@ -87,6 +91,42 @@ def LHDispPick(ml, vmin, cr_0, method=1, ini=10):
     return res.value, cr
 
 
+def LHDispPick_field(ml, vmin, cr_0, method, saveForBackward, variant=1):
+    """[res,cr_pre]=LHDispPick(ml,vmin,cr_0,method,saveForBackward) of the field-data drivers:
+    variant 1 fieldexamples/outcrop/core/LHDispPick.m:2 (pickFDCValue seeded at the global maximum
+    of saveForBackward.mlr / .mll, misfit over rows 15..end-15), variant 2
+    fieldexamples/QadimahFault/core/LHDispPick.m:2 (its mode 1: pickFDC1 from that column, misfit
+    over rows 50..end-30)."""
+    ml = np.asfortranarray(np.asarray(ml, np.float64))
+    nv, npair = ml.shape
+    sv = saveForBackward
+    raw = np.asfortranarray(np.asarray(sv["mlr"] if "uxtposr" in sv else sv["mll"], np.float64))
+    if raw.shape != ml.shape:
+        raise ValueError("saveForBackward's spectrum does not match ml")
+    cr0 = np.ascontiguousarray(np.broadcast_to(np.asarray(cr_0, np.float64).reshape(-1), (npair,)))
+    cr = np.zeros(npair)
+    res = ctypes.c_double()
+    call("swd_pick_field", ptr(ml), ptr(raw), nv, npair, float(vmin), ptr(cr0), int(method), int(variant),
+         ctypes.byref(res), ptr(cr))
+    return res.value, cr
+
+
+def norm_trace(data_in):
+    """data_out = norm_trace(data_in) (core/norm_trace.m:1): every trace over its largest magnitude."""
+    d = np.asfortranarray(np.asarray(data_in, np.float64))
+    out = np.zeros(d.shape, order="F")
+    call("swd_norm_trace", ptr(d), d.shape[0], d.shape[1], ptr(out))
+    return out
+
+
+def ADWDgrad_1_maxnorm(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
+                       saveForBackwardr, saveForBackwardl):
+    """[a_data_res]=ADWDgrad_1(...) of fieldexamples/outcrop/core/ADWDgrad_1.m:1: the adjoint source
+    divided by its largest magnitude (:79)."""
+    return _adwdgrad(3, nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
+                     saveForBackwardr, saveForBackwardl)
+
+
 def ADWDgrad_norm(nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr, grad_outputl, space_M,
                   saveForBackwardr, saveForBackwardl):
     """[a_data_res]=ADWDgrad_norm(...) (core/ADWDgrad_norm.m:1): ADWDgrad_1 with normpdf weights
@@ -132,7 +172,10 @@ def _adwdgrad(gauss, nt, ng, ns, npair, is_, w, m, M, SoftArgNorm, grad_outputr,
     mml, rawl, gl = side(sl, grad_outputl, "mll")
     spm = None if space_M is None else np.asfortranarray(np.asarray(space_M, np.float64))
     cp = lambda x: None if x is None else x.ctypes.data_as(dp)
-    if gauss == 2:
+    if gauss == 3:
+        call("swd_adwdgrad_maxnorm", ctypes.byref(p), int(ns), int(is_), int(w), float(SoftArgNorm), cp(gr), cp(gl),
+             cp(spm), cp(mmr), cp(rawr), cp(mml), cp(rawl), ptr(a))
+    elif gauss == 2:
         call("swd_adwdgrad_limband", ctypes.byref(p), int(ns), int(is_), int(w), float(SoftArgNorm), cp(gr), cp(gl),
              cp(spm), cp(mmr), cp(rawr), cp(mml), cp(rawl), ptr(a))
     elif gauss:

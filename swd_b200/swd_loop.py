@@ -8,6 +8,16 @@ SoftMax adjoint sources of the .m functions (RTrAD/RTlAD, LHDispPick, ADWDgrad_1
                   adjoint source cast to single (SWD_single.m:193)
     single=False  SWD.m: FP64 FD (the _double MEX pair), all in double
 
+    field=1       the field-data flow of fieldexamples/outcrop/outcrop.m:168-196: each predicted
+                  gather trace-normalised (norm_trace), picks seeded at the spectrum's global
+                  maximum with the misfit over rows 15..end-15 (that directory's LHDispPick /
+                  pickFDCValue), the adjoint source divided by its largest magnitude (its
+                  ADWDgrad_1.m:79); the observed curves are the caller's (manual picks,
+                  outcrop.m:137-160).  The outcrop driver runs it with single=False (its wrappers
+                  call the _double MEX, staggerfd_eigen.m:139-141 there).
+    field=2       the same with fieldexamples/QadimahFault's picker (pickFDC1 from the column
+                  of the global maximum, misfit over rows 50..end-30).
+
 The batched engine (swd_b200.engine) computes the same gradient in one pipeline; this loop
 is the per-shot path and the full-FP64 path the engine's precision is measured against.
 Images are accumulated in FP64 in both modes.
@@ -19,7 +29,7 @@ import math
 import numpy as np
 
 from .fd import e2drtm_eigen, e2drtm_eigend, staggerfd_eigen, staggerfd_eigend
-from .spectrum import ADWDgrad_1, LHDispPick, RTlAD, RTrAD
+from .spectrum import ADWDgrad_1, ADWDgrad_1_maxnorm, LHDispPick, LHDispPick_field, RTlAD, RTrAD, norm_trace
 
 
 def _mround(x):
@@ -77,25 +87,36 @@ def spectra(s, seismo, is_):
     return out
 
 
-def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True):
-    """SWD.m:172-193 for shot is_ (1-based in s): images cl, cm, illum plus picks and misfits."""
+def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True, field=0):
+    """SWD.m:172-193 for shot is_ (1-based in s): images cl, cm, illum plus picks and misfits
+    (field 1 / 2: the field-data flow, see the module docstring)."""
     sw, www = _seismogram(s, is_, vs, single)
+    if field:
+        # outcrop.m:174; on single data MATLAB divides in single (the FP64 quotient rounded to
+        # FP32 is that same single quotient)
+        sw = norm_trace(sw).astype(np.float32) if single else norm_trace(sw)
     sp = spectra(s, sw, is_)
     npair = s.npair
     shot_no = int(s.shot_no[is_ - 1]) if s.shot_no is not None else is_
     ns = s.ns_total or s.ns
     out = {"seismo_w": sw, "res_r": np.nan, "res_l": np.nan, "crp_r": np.ones(npair), "crp_l": np.ones(npair)}
+    def pick(sd, cr0):
+        if field:
+            return LHDispPick_field(sd[0], s.vmin, cr0, 1, sd[2], variant=field)
+        return LHDispPick(sd[0], s.vmin, cr0, 1, s.ini)
+
     if "r" in sp:
         out["ml_r"] = sp["r"][0]
-        out["res_r"], out["crp_r"] = LHDispPick(sp["r"][0], s.vmin, cr0_r[:, is_ - 1], 1, s.ini)
+        out["res_r"], out["crp_r"] = pick(sp["r"], cr0_r[:, is_ - 1])
     if "l" in sp:
         out["ml_l"] = sp["l"][0]
-        out["res_l"], out["crp_l"] = LHDispPick(sp["l"][0], s.vmin, cr0_l[:, is_ - 1], 1, s.ini)
+        out["res_l"], out["crp_l"] = pick(sp["l"], cr0_l[:, is_ - 1])
     gr = out["crp_r"] - cr0_r[:, is_ - 1]  # SWD.m:186-187
     gl = out["crp_l"] - cr0_l[:, is_ - 1]
     space = np.repeat(np.arange(1.0, s.np_vel + 1)[:, None], npair, 1)  # SWD.m:133-136
-    a = ADWDgrad_1(s.nt, s.ng, ns, npair, shot_no, s.w, s.m, s.M, s.soft_arg_norm, gr, gl, space,
-                   sp["r"][2] if "r" in sp else None, sp["l"][2] if "l" in sp else None)
+    adj = ADWDgrad_1_maxnorm if field else ADWDgrad_1
+    a = adj(s.nt, s.ng, ns, npair, shot_no, s.w, s.m, s.M, s.soft_arg_norm, gr, gl, space,
+            sp["r"][2] if "r" in sp else None, sp["l"][2] if "l" in sp else None)
     if single:
         a = a.astype(np.float32)  # SWD_single.m:193
         cl, cm, il = e2drtm_eigen(www, a, is_, s.nbc, s.nt, s.dtx, s.dx, s.dt, s.gx, np.ones(s.ng), s.source(),
@@ -107,12 +128,12 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True):
     return out
 
 
-def gradient(s, vs, cr0_r, cr0_l, single=True, keep_shots=False):
+def gradient(s, vs, cr0_r, cr0_l, single=True, keep_shots=False, field=0):
     """SWD.m:171-201: shot sums in shot order (FP64), Vs gradient, smoothing, misfit."""
     g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
     res_r, res_l, crp_r, crp_l, per = [], [], [], [], []
     for is_ in range(1, s.ns + 1):
-        p = shot_gradient(s, is_, vs, cr0_r, cr0_l, single)
+        p = shot_gradient(s, is_, vs, cr0_r, cr0_l, single, field)
         for k in g:
             g[k] = g[k] + p[k]
         res_r.append(p["res_r"])

@@ -19,7 +19,7 @@ class MexError(RuntimeError):
 class Shim:
     def __init__(self, name, outdir):
         src = os.path.join(ROOT, "mex", name + ".c")
-        so = os.path.join(outdir, name + ".so")
+        so = os.path.join(outdir, name.replace("/", "_") + ".so")
         cmd = ["gcc", "-O1", "-std=c11", "-D_GNU_SOURCE", "-shared", "-fPIC", "-I", HERE, "-I",
                os.path.join(ROOT, "mex"), "-I", os.path.join(ROOT, "include"), src, os.path.join(HERE, "mexsim.c"),
                "-L", LIBDIR, "-lswd", "-Wl,-rpath," + LIBDIR, "-lm", "-o", so]

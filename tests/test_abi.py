@@ -55,8 +55,8 @@ def test_engine_options_validate_before_touching_the_gpu():
     from swd_b200 import _lib, configs
     from swd_b200.engine import EngineOpts, GradientEngine, survey_struct
     s = configs.tiny(nt=400, ns=2)
-    for fs in (-1, 6):
-        with pytest.raises(_lib.SwdError, match="fd_schedule must lie in 0..5") as e:
+    for fs in (-1, 7):
+        with pytest.raises(_lib.SwdError, match="fd_schedule must lie in 0..6") as e:
             GradientEngine(s, fd_schedule=fs)
         assert e.value.status == 1
     sc = survey_struct(s)
@@ -76,3 +76,13 @@ def test_product_never_imports_the_oracle():
             if f.endswith((".py", ".cu", ".cuh", ".h", ".cpp")):
                 src = open(os.path.join(dp, f)).read()
                 assert "oracle" not in re.sub(r"(#|//).*", "", src).lower() or f == "build.py", f
+
+
+def test_engine_cancel_rejects_a_null_engine():
+    """swd_engine_cancel validates its argument on the host, before any CUDA call."""
+    from swd_b200 import _lib
+    from swd_b200.engine import _bind
+    _bind()
+    with pytest.raises(_lib.SwdError, match="null engine") as e:
+        _lib.call("swd_engine_cancel", None)
+    assert e.value.status == 1

@@ -86,7 +86,15 @@ def test_modes_are_bit_identical(tiny_case):
                {"snapshot_mode": 2, "ckpt_interval": 20, "fd_schedule": 5, "chunk_rows": 1},
                {"snapshot_mode": 1, "fd_schedule": 5, "warps": 2, "ring_fwd": 6, "chunk_rows": 3, "max_batch": 2},
                {"snapshot_mode": 1, "fd_schedule": 5, "ring_adj": 6, "chunk_rows": 2, "max_batch": 3,
-                "use_graphs": False}):
+                "use_graphs": False},
+               # two columns per lane in packed FP32 pairs, two steps per launch (one step for odd spans)
+               {"snapshot_mode": 1, "fd_schedule": 6}, {"snapshot_mode": 2, "ckpt_interval": 35, "fd_schedule": 6},
+               {"snapshot_mode": 2, "ckpt_interval": 20, "fd_schedule": 6, "chunk_rows": 1},
+               {"snapshot_mode": 1, "fd_schedule": 6, "warps": 2, "ring_fwd": 6, "chunk_rows": 3, "max_batch": 2},
+               {"snapshot_mode": 1, "fd_schedule": 6, "warps": 8, "ring_adj": 4, "chunk_rows": 2, "max_batch": 3,
+                "use_graphs": False},
+               {"snapshot_mode": 2, "ckpt_interval": 35, "fd_schedule": 6, "warps": 4, "ring_fwd": 6, "ring_adj": 6,
+                "chunk_rows": 5}):
         with GradientEngine(s, **kw) as e:
             e.set_observed(cr0_r, cr0_l)
             outs.append(e.gradient(s.vp, s.vs))
@@ -95,7 +103,7 @@ def test_modes_are_bit_identical(tiny_case):
             assert np.array_equal(o[k], outs[0][k]), k
 
 
-@pytest.mark.parametrize("sched", [0, 2, 5])
+@pytest.mark.parametrize("sched", [0, 2, 5, 6])
 def test_warp_chunks_are_capped_at_60_rows(sched):
     """The warp schedules mark a chunk's checked rows in a 64-bit mask, so their chunks are at
     most 60 rows: a 70-row grid asked for 500-row chunks runs 60 + 10 rows and gives the bits
@@ -113,7 +121,7 @@ def test_warp_chunks_are_capped_at_60_rows(sched):
         assert np.array_equal(outs[1][k], outs[0][k]), k
 
 
-@pytest.mark.parametrize("sched", [1, 2, 3, 4, 5])
+@pytest.mark.parametrize("sched", [1, 2, 3, 4, 5, 6])
 def test_other_schedules_on_the_plain_survey_match_the_oracle(O, sched):
     """The one-barrier (1), warp-streaming (2), two-steps-per-launch (3, the default),
     two-barrier (4) and two-shots-per-warp (5) schedules against the oracle on the 30 x 120
@@ -205,20 +213,30 @@ def test_autotuned_engine_is_bit_identical(tiny_case, mode):
         assert np.array_equal(outs[0][k], outs[1][k]), k
 
 
-def test_split_bf16_radon_in_the_engine(tiny_case):
-    """radon_precision='bf16x2': the forward contraction on the tensor cores.  Spectra move by
-    ~1e-5 relative, so picks may change only at near-ties; the gradient stays close."""
-    s, cr0_r, cr0_l, _ = tiny_case
-    outs = []
+@pytest.mark.parametrize("survey", ["tiny", "plain"])
+def test_split_bf16_radon_in_the_engine(tiny_case, survey, O):
+    """radon_precision='bf16x2': the forward contraction on the tensor cores, with the picker
+    certifying every gather (a decision within 1e-4 of the column maximum sends the gather to the
+    FP64 contraction and is picked again).  Picks are identical to the FP64 engine's -- also on
+    the 30 x 120 survey, where uncertified split-BF16 spectra moved one pick in 672 -- and the
+    gradient stays within the north-star bar (1e-4)."""
+    if survey == "tiny":
+        s, cr0_r, cr0_l, _ = tiny_case
+    else:
+        s = configs.plain_c1()
+        cr0_r, cr0_l = O.observed_curves(s, s.vs_true)
+    outs, stats = [], None
     for prec in ("fp64", "bf16x2"):
         with GradientEngine(s, radon_precision=prec) as e:
             e.set_observed(cr0_r, cr0_l)
             outs.append(e.gradient(s.vp, s.vs))
+            if prec == "bf16x2":
+                stats = e.radon_stats()
     a, b = outs
-    same = np.mean(np.concatenate([(a["cr_pre_r"] == b["cr_pre_r"]).ravel(), (a["cr_pre_l"] == b["cr_pre_l"]).ravel()]))
-    err = _rel(b["dk_vs"], a["dk_vs"])
-    print("identical picks", same, "dk rel L2", err)
-    assert same >= 0.95 and err < 1e-2
+    print(survey, "recomputed in FP64", stats, "dk rel L2", _rel(b["dk_vs"], a["dk_vs"]))
+    assert np.array_equal(a["cr_pre_r"], b["cr_pre_r"]) and np.array_equal(a["cr_pre_l"], b["cr_pre_l"])
+    assert stats["gathers"] > 0 and stats["recomputed_fp64"] <= stats["gathers"]
+    assert _rel(b["dk_vs"], a["dk_vs"]) < 1e-4
 
 
 def test_gaussian_adjoint_weight_matches_oracle(tiny_case):
@@ -252,7 +270,8 @@ def test_wd_adjoint_source_matches_oracle(tiny_case):
 
 
 @pytest.mark.parametrize("sched,mode,prec", [(0, 1, "fp32"), (0, 2, "fp32"), (4, 1, "fp32"), (5, 2, "fp32"),
-                                            (0, 2, "fp64"), (4, 1, "fp64"), (5, 1, "fp64")])
+                                            (6, 1, "fp32"), (6, 2, "fp32"), (0, 2, "fp64"), (4, 1, "fp64"),
+                                            (5, 1, "fp64"), (6, 1, "fp64"), (6, 2, "fp64")])
 def test_image_sums_match_the_oracle(O, tiny_case, sched, mode, prec):
     """image_precision='fp32' (the default) sums each shot's imaging terms in FP32, as the
     reference's single MEX does, and 'fp64' in FP64; against the oracle's shot loop with the same

@@ -18,7 +18,7 @@ from swd_b200 import configs  # noqa: E402
 
 SHIMS = ["eigen_staggerfd_single", "eigen_staggerfd_double", "eigen_e2drtm_single", "eigen_e2drtm_double",
          "RTrAD", "RTlAD", "RTr", "RTl", "LHDispPick", "ADWDgrad_1", "ADWDgrad_norm", "ADWDgradlimband",
-         "weight_data_muti3"]
+         "weight_data_muti3", "norm_trace", "field/LHDispPick", "field/ADWDgrad_1"]
 
 
 @pytest.fixture(scope="module")
@@ -36,7 +36,7 @@ def shim(tmp_path_factory):
 @pytest.mark.parametrize("name", SHIMS)
 def test_shim_builds_and_checks_argument_count(shim, name):
     with pytest.raises(mexsim.MexError, match="swd:nrhs"):
-        shim(name)(1, 1.0)
+        shim(name)(1, 1.0, 2.0)  # nlhs 1, two inputs: no shim takes two
 
 
 def _fd_args(O, single=True, adjoint=False):
