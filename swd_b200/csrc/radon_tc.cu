@@ -31,6 +31,9 @@ constexpr int BM = 128;  // velocities per tile = TMEM lanes
 constexpr int BN = 96;   // shots per tile (MMA N)
 constexpr int BK = 32;   // offsets per pipeline stage (two MMA K-steps of 16)
 constexpr int kThreads = 128;
+// pipeline slots: BF16X2 2 x 56 KB (two CTAs per SM), BF16X3 2 x 84 KB (one CTA per SM)
+constexpr int kStagesX2 = 2;
+constexpr int kStagesX3 = 2;
 
 // Operand tile of R rows x BK bf16 in the canonical K-major layout without swizzle:
 // 8-row x 16-byte core matrices, [R/8][BK/8][8 rows][8 elements].  Leading byte offset
@@ -74,31 +77,27 @@ __device__ inline void mma_commit(uint32_t mbar) {
 __device__ inline void mbar_init(uint32_t mbar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(mbar), "r"(count) : "memory");
 }
-// Bounded wait for phase `parity` of an mbarrier (non-blocking tests with a short sleep
-// between them, about half a second at most); false if it did not complete.
+// Bounded wait for phase `parity` of an mbarrier: try_wait suspends the warp in hardware until
+// the phase completes or a short time limit passes, so a waiting warp takes no issue slots from
+// the others; the loop gives up after about half a second of SM clock (or 2^26 tries),
+// returning false.
+constexpr long long kWaitCycles = 1LL << 30;
 __device__ inline bool mbar_wait(uint32_t mbar, uint32_t parity) {
-  for (uint32_t it = 0; it < (1u << 22); ++it) {
+  const long long t0 = clock64();
+  for (uint32_t it = 0; it < (1u << 26); ++it) {
     uint32_t ok;
     asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}\n"
         : "=r"(ok)
         : "r"(mbar), "r"(parity)
         : "memory");
     if (ok) return true;
-    if (it > 64) __nanosleep(100);
+    if (clock64() - t0 > kWaitCycles) break;
   }
   return false;
 }
 __device__ inline void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ inline void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ inline void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-
-__device__ inline void cp16(uint32_t dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
-}
-__device__ inline void cp_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ inline void cp_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
 
 // 32 lanes x 32 consecutive FP32 columns of TMEM into registers (this warp's lane quarter).
 __device__ inline void tmem_ld32(uint32_t taddr, float* v) {
@@ -135,29 +134,105 @@ struct TcArgs {
   int* status;                    // set to 1 when a wait timed out
 };
 
-// One CTA: frequency f, a BM-velocity tile and a BN-shot tile; all offsets through a
-// STAGES-deep cp.async pipeline.  Thread 0 issues the MMAs; TMEM holds the real part in
-// columns [0, BN) and the imaginary part in [BN, 2 BN).
+// 1-D bulk copy (the TMA engine, no tensor map, no multicast) of `bytes` from global memory into
+// this CTA's shared memory; completion is counted on `mbar` as transaction bytes.  Both
+// addresses 16-byte aligned, bytes a multiple of 16.
+__device__ inline void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t mbar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(mbar)
+               : "memory");
+}
+__device__ inline void mbar_expect_tx(uint32_t mbar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mbar), "r"(bytes) : "memory");
+}
+
+// The MMAs of one stage: two K-steps of 16 offsets, the split products of order < NS
+// (hi*hi, hi*lo, lo*hi, ...), real and imaginary accumulators.  Operand parts in the slot:
+// A re_0..re_{NS-1}, im_0..; then B likewise.  The descriptors of a slot differ only in their
+// start-address field (bits 0-13, 16-byte units; shared memory ends below 2^18 bytes, so no
+// carry leaves the field): one base per operand, compile-time offsets per MMA.  Only the first
+// MMA into each accumulator of the first stage overwrites it.
+template <int NS>
+__device__ inline void stage_mmas(uint32_t tmem, uint32_t sa, uint32_t sb, bool first) {
+  constexpr uint64_t a_part = (BM * BK * 2) >> 4, b_part = (BN * BK * 2) >> 4, k_step = (2 * kLBO) >> 4;
+  const uint64_t da = smem_desc(sa), db = smem_desc(sb);
+  const uint32_t id_pos = idesc_bf16(BM, BN, false), id_neg = idesc_bf16(BM, BN, true);
+  const uint32_t acc0 = first ? 0u : 1u;
+#pragma unroll
+  for (int kk = 0; kk < BK / 16; ++kk)
+#pragma unroll
+    for (int i = 0; i < NS; ++i)
+#pragma unroll
+      for (int j = 0; j < NS; ++j) {
+        if (i + j >= NS) continue;
+        const uint64_t ar = da + (i * a_part + kk * k_step), ai = da + ((NS + i) * a_part + kk * k_step);
+        const uint64_t br = db + (j * b_part + kk * k_step), bi = db + ((NS + j) * b_part + kk * k_step);
+        const uint32_t acc = (kk | i | j) ? 1u : acc0;
+        mma_bf16(tmem, ar, br, id_pos, acc);       // re += Kr Dr
+        mma_bf16(tmem, ai, bi, id_neg, 1u);        // re -= Ki Di
+        mma_bf16(tmem + BN, ar, bi, id_pos, acc);  // im += Kr Di
+        mma_bf16(tmem + BN, ai, br, id_pos, 1u);   // im += Ki Dr
+      }
+}
+
+// The tile's accumulators to mm in FP64: warp w (0..3) reads TMEM lanes 32w..32w+31, one
+// velocity per thread, the real part from columns [0, BN) and the imaginary from [BN, 2 BN).
+__device__ inline void store_tile(const TcArgs& a, uint32_t tmem, int mt, int nt, int f, int warp, int lane) {
+  const int p = mt * BM + warp * 32 + lane;
+  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+#pragma unroll 1
+  for (int c0 = 0; c0 < BN; c0 += 32) {
+    float re[32], im[32];
+    tmem_ld32(tmem + lane_base + c0, re);
+    tmem_ld32(tmem + lane_base + BN + c0, im);
+    if (p < a.np) {
+#pragma unroll
+      for (int c = 0; c < 32; ++c) {
+        const int s = nt * BN + c0 + c;
+        if (s < a.ns) a.mm[((size_t)s * a.nf + f) * a.np + p] = make_double2(re[c], im[c]);
+      }
+    }
+  }
+}
+
+// One CTA: frequency f, a BM-velocity tile and a BN-shot tile; all offsets through a STAGES-deep pipeline of shared-memory slots, warp-specialised:
+//   warp 0, lane 0   producer: one bulk copy of the stage's pre-tiled kernel block and one of
+//                    its spectra block into a free slot (slot `full` barrier: transaction bytes);
+//   warp 1, lane 0   MMA issuer: waits for a full slot, issues its tcgen05.mma and commits to the
+//                    slot's `empty` barrier, which frees the slot for the producer;
+//   all 4 warps      epilogue (store_tile).
+// With two stages a CTA takes 112 KB of shared memory and 256 TMEM columns, so two CTAs share
+// an SM and one's epilogue overlaps the other's main loop.
+//
+// Every wait is bounded (mbar_wait).  A producer or MMA wait that gives up sets `failed` and
+// stops that role issuing; the producer then waits for the copies it issued, the MMA issuer
+// commits once more so that `done` covers every MMA it issued, all threads wait for `done`, and
+// TMEM is released either way; the launch reports through `status`.
 template <int NS, int STAGES>
 __global__ void __launch_bounds__(kThreads) tc_contract_kernel(TcArgs a) {
   constexpr int P = 2 * NS;  // parts per operand tile set
-  constexpr size_t A_STAGE = (size_t)P * BM * BK * 2, B_STAGE = (size_t)P * BN * BK * 2;
-  constexpr size_t STAGE = A_STAGE + B_STAGE;
+  constexpr uint32_t A_STAGE = (uint32_t)P * BM * BK * 2, B_STAGE = (uint32_t)P * BN * BK * 2;
+  constexpr uint32_t STAGE = A_STAGE + B_STAGE;
   constexpr uint32_t kCols = 256;  // >= 2*BN, power of two
-  extern __shared__ __align__(1024) uint8_t smem[];
-  __shared__ __align__(8) uint64_t mbar[STAGES];
+  extern __shared__ __align__(128) uint8_t smem[];  // no-swizzle operand tiles need 16-byte alignment
+  __shared__ __align__(8) uint64_t full[STAGES];
+  __shared__ __align__(8) uint64_t empty[STAGES];
+  __shared__ __align__(8) uint64_t done;
   __shared__ uint32_t tmem_slot;
   __shared__ int failed;
 
   const int mt = blockIdx.x, nt = blockIdx.y, f = blockIdx.z;
-  const int tid = threadIdx.x, warp = tid >> 5;
-  const size_t a_blk = (size_t)P * BM * BK, b_blk = (size_t)P * BN * BK;
-  const __nv_bfloat16* Ag = a.A + (((size_t)f * a.mtiles + mt) * a.ktiles) * a_blk;
-  const __nv_bfloat16* Bg = a.B + (((size_t)f * a.ntiles + nt) * a.ktiles) * b_blk;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint8_t* Ag = reinterpret_cast<const uint8_t*>(a.A) + ((size_t)f * a.mtiles + mt) * a.ktiles * A_STAGE;
+  const uint8_t* Bg = reinterpret_cast<const uint8_t*>(a.B) + ((size_t)f * a.ntiles + nt) * a.ktiles * B_STAGE;
 
   if (tid == 0) {
     failed = 0;
-    for (int s = 0; s < STAGES; ++s) mbar_init(smem_u32(&mbar[s]), 1);
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(smem_u32(&full[s]), 1);   // the producer's arrive (with the expected bytes)
+      mbar_init(smem_u32(&empty[s]), 1);  // the MMA issuer's commit
+    }
+    mbar_init(smem_u32(&done), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 0) {
@@ -169,98 +244,52 @@ __global__ void __launch_bounds__(kThreads) tc_contract_kernel(TcArgs a) {
   __syncthreads();
   fence_after_sync();
   const uint32_t tmem = tmem_slot;
-
-  auto load_stage = [&](int kt) {
-    const int slot = kt % STAGES;
-    const uint32_t sa = smem_u32(smem + slot * STAGE);
-    const uint8_t* ga = (const uint8_t*)(Ag + (size_t)kt * a_blk);
-    const uint8_t* gb = (const uint8_t*)(Bg + (size_t)kt * b_blk);
-    for (int i = tid; i < (int)(A_STAGE / 16); i += kThreads) cp16(sa + i * 16, ga + (size_t)i * 16);
-    for (int i = tid; i < (int)(B_STAGE / 16); i += kThreads) cp16(sa + A_STAGE + i * 16, gb + (size_t)i * 16);
-  };
-
+  const uint32_t s0 = smem_u32(smem);
   const int nk = a.ktiles;
-  for (int s = 0; s < STAGES - 1; ++s) {
-    if (s < nk) load_stage(s);
-    cp_commit();
-  }
-  // A wait that times out sets `failed`.  Every write to it comes before the barrier at the top of
-  // the next stage, so all threads read the same value there and leave the loop together: no
-  // further copies into slots that MMAs may still read, and no further MMAs.
-  int kt = 0;
-  for (; kt < nk; ++kt) {
-    cp_wait<STAGES - 2>();  // this thread's copies of stage kt have landed
-    fence_proxy_async();
-    __syncthreads();
-    if (failed) break;
-    const int slot = kt % STAGES;
-    if (tid == 0) {
-      fence_after_sync();
-      const uint32_t sa = smem_u32(smem + slot * STAGE), sb = sa + (uint32_t)A_STAGE;
-      constexpr uint32_t a_part = BM * BK * 2, b_part = BN * BK * 2;
-      const uint32_t id_pos = idesc_bf16(BM, BN, false), id_neg = idesc_bf16(BM, BN, true);
-#pragma unroll
-      for (int kk = 0; kk < BK / 16; ++kk) {
-        const uint32_t ko = kk * 2 * kLBO;  // two core matrices of K per MMA
-#pragma unroll
-        for (int i = 0; i < NS; ++i)
-#pragma unroll
-          for (int j = 0; j < NS; ++j) {
-            if (i + j >= NS) continue;  // keep products of order < NS (hi*hi, hi*lo, lo*hi, ...)
-            const uint64_t ar = smem_desc(sa + i * a_part + ko), ai = smem_desc(sa + (NS + i) * a_part + ko);
-            const uint64_t br = smem_desc(sb + j * b_part + ko), bi = smem_desc(sb + (NS + j) * b_part + ko);
-            const uint32_t acc = (kt | kk | i | j) ? 1u : 0u;
-            mma_bf16(tmem, ar, br, id_pos, acc);            // re += Kr Dr
-            mma_bf16(tmem, ai, bi, id_neg, 1u);             // re -= Ki Di
-            mma_bf16(tmem + BN, ar, bi, id_pos, acc);       // im += Kr Di
-            mma_bf16(tmem + BN, ai, br, id_pos, 1u);        // im += Ki Dr
-          }
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int kt = 0;
+      for (; kt < nk; ++kt) {
+        const int slot = kt % STAGES;
+        if (kt >= STAGES && !mbar_wait(smem_u32(&empty[slot]), (uint32_t)((kt / STAGES - 1) & 1))) {
+          failed = 1;
+          break;
+        }
+        const uint32_t fb = smem_u32(&full[slot]), sa = s0 + slot * STAGE;
+        mbar_expect_tx(fb, STAGE);
+        bulk_g2s(sa, Ag + (size_t)kt * A_STAGE, A_STAGE, fb);
+        bulk_g2s(sa + A_STAGE, Bg + (size_t)kt * B_STAGE, B_STAGE, fb);
       }
-      mma_commit(smem_u32(&mbar[slot]));
+      // the copies issued last into each slot have landed before the CTA may leave (already so
+      // when the MMA issuer consumed them)
+      for (int j = kt > STAGES ? kt - STAGES : 0; j < kt; ++j)
+        if (!mbar_wait(smem_u32(&full[j % STAGES]), (uint32_t)((j / STAGES) & 1))) failed = 1;
     }
-    // refill the slot consumed by the previous stage once its MMAs are done; a thread whose
-    // wait gave up copies nothing into it
-    const int kn = kt + STAGES - 1;
-    if (kn < nk) {
-      bool free_slot = true;
-      if (kn >= STAGES) {
-        const int ps = kn % STAGES;  // == (kt - 1) % STAGES
-        free_slot = mbar_wait(smem_u32(&mbar[ps]), (uint32_t)((kn / STAGES - 1) & 1));
-        if (!free_slot) failed = 1;
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      for (int kt = 0; kt < nk; ++kt) {
+        const int slot = kt % STAGES;
+        if (!mbar_wait(smem_u32(&full[slot]), (uint32_t)((kt / STAGES) & 1))) {
+          failed = 1;
+          break;
+        }
+        fence_after_sync();
+        const uint32_t sa = s0 + slot * STAGE;
+        stage_mmas<NS>(tmem, sa, sa + A_STAGE, kt == 0);
+        mma_commit(smem_u32(&empty[slot]));
       }
-      if (free_slot) load_stage(kn);
+      mma_commit(smem_u32(&done));  // arrives once every MMA issued above has completed
     }
-    cp_commit();
+    __syncwarp();
   }
-  cp_wait<0>();  // this thread's copies in flight
-  // the MMAs: the last commit (stage kt-1) covers every earlier tcgen05 operation of thread 0;
-  // after a failure this one more wait is bounded too, and TMEM is released either way
-  if (kt > 0) {
-    const int last = kt - 1;
-    if (!mbar_wait(smem_u32(&mbar[last % STAGES]), (uint32_t)((last / STAGES) & 1))) failed = 1;
-  }
+  if (!mbar_wait(smem_u32(&done), 0u)) failed = 1;
   fence_after_sync();
   __syncthreads();
 
-  if (!failed) {
-    const int p = mt * BM + warp * 32 + (tid & 31);
-    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-#pragma unroll 1
-    for (int c0 = 0; c0 < BN; c0 += 32) {
-      float re[32], im[32];
-      tmem_ld32(tmem + lane_base + c0, re);
-      tmem_ld32(tmem + lane_base + BN + c0, im);
-      if (p < a.np) {
-#pragma unroll
-        for (int c = 0; c < 32; ++c) {
-          const int s = nt * BN + c0 + c;
-          if (s < a.ns) a.mm[((size_t)s * a.nf + f) * a.np + p] = make_double2(re[c], im[c]);
-        }
-      }
-    }
-  } else if (tid == 0) {
-    atomicExch(a.status, 1);
-  }
+  if (!failed) store_tile(a, tmem, mt, nt, f, warp, lane);
+  else if (tid == 0) atomicExch(a.status, 1);
   fence_before_sync();
   __syncthreads();
   if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols));
@@ -294,22 +323,46 @@ __global__ void tc_ktable_kernel(int nf, int np, int nx, int mtiles, int ktiles,
   for (int i = 0; i < ns_split; ++i) base[(size_t)(ns_split + i) * BM * BK + tile_offset(r, k)] = h[i];
 }
 
-// Spectra [s][f][x] (complex double) split and pre-tiled: B[f][nt][kt][part][tile].
-__global__ void tc_split_spec_kernel(int nf, int nx, int nsh, int ntiles, int ktiles, int ns_split,
-                                     const double2* spec, __nv_bfloat16* B) {
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
-  const int s = blockIdx.y, f = blockIdx.z;
-  if (x >= ktiles * BK) return;
-  double2 v = make_double2(0.0, 0.0);
-  if (s < nsh && x < nx) v = spec[((size_t)s * nf + f) * nx + x];
-  const int nt = s / BN, r = s % BN, kt = x / BK, k = x % BK;
+// Spectra [s][f][x] (complex double) split and pre-tiled: B[f][nt][kt][part][tile].  One warp
+// per (frequency, 8 shots, 32 offsets): lane = row (shot) r & 7 + 8 * (offset group of 8), so
+// each lane reads 8 consecutive offsets of one shot (128 contiguous bytes) and the warp writes
+// each part's 8 rows x 32 offsets as one contiguous 512-byte run of the tile layout.
+__global__ void __launch_bounds__(256) tc_split_spec_kernel(int nf, int nx, int nsh, int ntiles, int ktiles,
+                                                            int ns_split, const double2* __restrict__ spec,
+                                                            __nv_bfloat16* __restrict__ B) {
+  const int lane = threadIdx.x & 31;
+  const int rg = blockIdx.y * 8 + (threadIdx.x >> 5);  // group of 8 shot rows
+  const int kt = blockIdx.x, f = blockIdx.z;
+  if (rg * 8 >= ntiles * BN) return;
+  const int s = rg * 8 + (lane & 7), g = lane >> 3;  // shot, offset group within the tile
+  const int x0 = kt * BK + g * 8;
+  float re[8], im[8];
+#pragma unroll
+  for (int e = 0; e < 8; ++e) {
+    double2 v = make_double2(0.0, 0.0);
+    if (s < nsh && x0 + e < nx) v = spec[((size_t)s * nf + f) * nx + x0 + e];
+    re[e] = (float)v.x;
+    im[e] = (float)v.y;
+  }
+  const int nt = s / BN, r = s % BN;
   const size_t blk = (size_t)2 * ns_split * BN * BK;
-  __nv_bfloat16* base = B + (((size_t)f * ntiles + nt) * ktiles + kt) * blk;
-  __nv_bfloat16 h[3];
-  split_value(v.x, ns_split, h);
-  for (int i = 0; i < ns_split; ++i) base[(size_t)i * BN * BK + tile_offset(r, k)] = h[i];
-  split_value(v.y, ns_split, h);
-  for (int i = 0; i < ns_split; ++i) base[(size_t)(ns_split + i) * BN * BK + tile_offset(r, k)] = h[i];
+  __nv_bfloat16* base = B + (((size_t)f * ntiles + nt) * ktiles + kt) * blk + tile_offset(r, g * 8);
+  for (int part = 0; part < ns_split; ++part) {
+    uint32_t wr[4], wi[4];
+#pragma unroll
+    for (int e = 0; e < 8; e += 2) {
+      const __nv_bfloat16 r0 = __float2bfloat16_rn(re[e]), r1 = __float2bfloat16_rn(re[e + 1]);
+      const __nv_bfloat16 i0 = __float2bfloat16_rn(im[e]), i1 = __float2bfloat16_rn(im[e + 1]);
+      re[e] -= __bfloat162float(r0);
+      re[e + 1] -= __bfloat162float(r1);
+      im[e] -= __bfloat162float(i0);
+      im[e + 1] -= __bfloat162float(i1);
+      wr[e / 2] = (uint32_t)__bfloat16_as_ushort(r0) | ((uint32_t)__bfloat16_as_ushort(r1) << 16);
+      wi[e / 2] = (uint32_t)__bfloat16_as_ushort(i0) | ((uint32_t)__bfloat16_as_ushort(i1) << 16);
+    }
+    *reinterpret_cast<uint4*>(base + (size_t)part * BN * BK) = make_uint4(wr[0], wr[1], wr[2], wr[3]);
+    *reinterpret_cast<uint4*>(base + (size_t)(ns_split + part) * BN * BK) = make_uint4(wi[0], wi[1], wi[2], wi[3]);
+  }
 }
 
 }  // namespace tc
@@ -402,10 +455,21 @@ struct swd_contract {
   int nf = 0, np = 0, nx = 0, ns = 0, precision = 0, device = 0;
   int mtiles = 0, ntiles = 0, ktiles = 0, nsplit = 0;
   DevBuf axes;    // freq, vel, off
-  DevBuf table;   // K (CUDA cores) or split pre-tiled A (tensor cores)
+  DevBuf table;   // K (CUDA cores) or split pre-tiled A (tensor cores, offsets not uniform)
   DevBuf bsplit;  // split pre-tiled spectra
   DevBuf status;
 };
+
+namespace {
+template <typename K>
+int smem_attrs(K kernel, size_t bytes) {
+  SWD_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  // two CTAs per SM (BF16X2) need the largest shared-memory carveout
+  SWD_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared));
+  return SWD_OK;
+}
+}  // namespace
 
 extern "C" {
 
@@ -449,13 +513,10 @@ int swd_contract_create(int nf, const double* freq, int np, const double* vel, i
     tc::tc_ktable_kernel<<<grid, 128>>>(nf, np, nx, c->mtiles, c->ktiles, c->nsplit, d_ax, d_ax + nf,
                                         d_ax + nf + np, c->table.as<__nv_bfloat16>());
     count_launch(1);
-    const size_t smem = c->nsplit == 2 ? tc::tc_smem_bytes<2>(3) : tc::tc_smem_bytes<3>(2);
     if (c->nsplit == 2)
-      SWD_CUDA(cudaFuncSetAttribute(tc::tc_contract_kernel<2, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+      SWD_TRY(smem_attrs(tc::tc_contract_kernel<2, tc::kStagesX2>, tc::tc_smem_bytes<2>(tc::kStagesX2)));
     else
-      SWD_CUDA(cudaFuncSetAttribute(tc::tc_contract_kernel<3, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)smem));
+      SWD_TRY(smem_attrs(tc::tc_contract_kernel<3, tc::kStagesX3>, tc::tc_smem_bytes<3>(tc::kStagesX3)));
   }
   SWD_CUDA(cudaGetLastError());
   SWD_CUDA(cudaDeviceSynchronize());
@@ -480,17 +541,18 @@ int swd_contract_run(swd_contract* c, const double* d_spec, double* d_mm, void* 
     return SWD_OK;
   }
   {
-    dim3 grid((c->ktiles * tc::BK + 127) / 128, c->ntiles * tc::BN, c->nf);
-    tc::tc_split_spec_kernel<<<grid, 128, 0, st>>>(c->nf, c->nx, c->ns, c->ntiles, c->ktiles, c->nsplit, spec,
+    const int row_groups = c->ntiles * tc::BN / 8;  // 8 shot rows per warp, 8 warps per block
+    dim3 grid(c->ktiles, (row_groups + 7) / 8, c->nf);
+    tc::tc_split_spec_kernel<<<grid, 256, 0, st>>>(c->nf, c->nx, c->ns, c->ntiles, c->ktiles, c->nsplit, spec,
                                                    c->bsplit.as<__nv_bfloat16>());
   }
   tc::TcArgs a{c->nf, c->np, c->nx, c->ns, c->mtiles, c->ntiles, c->ktiles, c->table.as<__nv_bfloat16>(),
                c->bsplit.as<__nv_bfloat16>(), mm, c->status.as<int>()};
   dim3 grid(c->mtiles, c->ntiles, c->nf);
   if (c->nsplit == 2)
-    tc::tc_contract_kernel<2, 3><<<grid, tc::kThreads, tc::tc_smem_bytes<2>(3), st>>>(a);
+    tc::tc_contract_kernel<2, tc::kStagesX2><<<grid, tc::kThreads, tc::tc_smem_bytes<2>(tc::kStagesX2), st>>>(a);
   else
-    tc::tc_contract_kernel<3, 2><<<grid, tc::kThreads, tc::tc_smem_bytes<3>(2), st>>>(a);
+    tc::tc_contract_kernel<3, tc::kStagesX3><<<grid, tc::kThreads, tc::tc_smem_bytes<3>(tc::kStagesX3), st>>>(a);
   count_launch(2);
   SWD_CUDA(cudaGetLastError());
   return SWD_OK;

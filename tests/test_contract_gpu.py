@@ -14,11 +14,11 @@ from swd_b200.contract import Contraction
 TOL = {"fp64": 1e-12, "fp32": 1e-5, "bf16x2": 2e-4, "bf16x3": 1e-5}
 
 
-def _case(seed=3, nf=7, np_=200, nx=70, ns=100):
+def _case(seed=3, nf=7, np_=200, nx=70, ns=100, uniform=True):
     rng = np.random.default_rng(seed)
     freq = np.linspace(3.0, 80.0, nf)
     vel = np.linspace(80.0, 1200.0, np_)
-    off = np.arange(nx) * 0.5
+    off = np.arange(nx) * 0.5 if uniform else np.sort(rng.uniform(0.0, 35.0, nx))
     spec = (rng.standard_normal((ns, nf, nx)) + 1j * rng.standard_normal((ns, nf, nx))).astype(np.complex64)
     return freq, vel, off, spec.astype(np.complex128)
 
@@ -60,3 +60,21 @@ def test_contraction_matches_oracle(O, prec):
     print(prec, "rel L2", err)
     assert np.all(np.isfinite(got)) and err < TOL[prec]
     assert np.array_equal(got, got2)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("prec", ["bf16x2", "bf16x3"])
+def test_contraction_with_uneven_offsets_matches_oracle(O, prec):
+    """General axes: offsets that are not evenly spaced (the engine's are)."""
+    import torch
+    freq, vel, off, spec = _case(seed=4, uniform=False)
+    ref = O.contract(freq, vel, off, spec)
+    with Contraction(freq, vel, off, spec.shape[0], prec) as c:
+        d_mm = torch.full(c.shape_out, np.nan, dtype=torch.complex128, device="cuda")
+        c.run(torch.from_numpy(spec).cuda(), d_mm)
+        torch.cuda.synchronize()
+        assert not c.timed_out()
+        got = d_mm.cpu().numpy()
+    err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    print(prec, "uneven offsets rel L2", err)
+    assert np.all(np.isfinite(got)) and err < TOL[prec]
