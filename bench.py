@@ -31,13 +31,17 @@ import numpy as np  # noqa: E402
 
 METRIC = "shot-gradients/s (fwd+adj)"
 UNIT = "shot-gradients/s"
-# DRAM traffic per padded cell and launch of the FD step kernels (plain variants, without the
-# snapshot or imaging step) for each FD schedule, measured with ncu (dram__bytes_read.sum +
-# dram__bytes_write.sum) on one launch over 96 shots x 132 x 660 cells, divided by the cells.
-# A schedule without an entry has no capture yet and reports traffic null.
-NCU_BYTES_PER_CELL_LAUNCH = {4: {"fd_fwd_step": 36.1, "fd_adj_step": 36.1},
-                             2: {"fd_fwd_step": 35.05, "fd_adj_step": 34.99},
-                             3: {"fd_fwd_step": 35.22, "fd_adj_step": 35.35}}
+# DRAM bytes of the FD step kernels, measured with ncu (dram__bytes_read.sum +
+# dram__bytes_write.sum) on the 100x600 survey (132 x 660 padded cells), per FD schedule:
+# (B per padded shot-cell of a plain launch, B per interior shot-cell that a launch writing a
+# snapshot (forward) or applying the imaging condition (adjoint, by image-sum precision) adds).
+# A launch-averaged figure is plain * cells + (steps per launch / nt_wf) * extra * interior
+# cells.  None: that variant has no capture, and the line reports traffic null.
+NCU_TRAFFIC = {2: {"fd_fwd_step": (35.05, None), "fd_adj_step": (34.99, {})},
+               3: {"fd_fwd_step": (35.09, 10.89), "fd_adj_step": (35.14, {"fp32": 36.67})},
+               4: {"fd_fwd_step": (36.1, 13.2), "fd_adj_step": (36.1, {"fp64": 64.8})},
+               5: {"fd_fwd_step": (36.00, 11.11), "fd_adj_step": (35.99, {"fp32": 36.01})},
+               6: {"fd_fwd_step": (36.40, 11.07), "fd_adj_step": (36.42, {"fp32": 36.08})}}
 # Compulsory DRAM bytes of the fused one-sweep kernels: 5 state fields read + 5 written per
 # shot-cell and launch (a launch advances one step, or two under schedules 3 and 5; materials
 # are shared by the shots of a launch), plus per interior cell every nt_wf steps the 3-field
@@ -84,6 +88,8 @@ def parse():
                    help="FP32 engine vs the full-FP64 per-shot path: seismograms, spectra, picks, gradient, misfit")
     p.add_argument("--invert", type=int, default=0,
                    help="SWD inversion iterations (gradient + line search) on the batched 100x600 survey")
+    p.add_argument("--invert-plain", action="store_true",
+                   help="run the inversion on the plain one-shot-per-launch path (no CUDA graphs) instead")
     p.add_argument("--plain-sample", type=int, default=8,
                    help="served stream: requests re-run serially on the plain path for the comparison")
     return p.parse_args()
@@ -458,7 +464,8 @@ def run_invert(args):
         return 0
     s = survey(args)
     vs0 = np.repeat(np.linspace(np.min(s.vs_true), np.max(s.vs_true), s.nz)[:, None], s.nx, 1)
-    inv = Inversion(s, vs0, s.vs_true, autotune=True)
+    opts = {"max_batch": 1, "use_graphs": False} if args.invert_plain else {"autotune": True}
+    inv = Inversion(s, vs0, s.vs_true, **opts)
     inv.run(1)  # warm-up: engine, graphs, observed curves
     torch.cuda.synchronize()
     t0 = time.perf_counter()
@@ -470,7 +477,9 @@ def run_invert(args):
     line = {"metric": "SWD iterations/hour", "value": len(hist[1:]) / dt * 3600 if len(hist) > 1 else None,
             "unit": "iterations/hour", "n_gpus": 1, "higher_is_better": True, "dtype": "f32",
             "data": "synthetic (seeded layered model + Gaussian anomaly)",
-            "config": workload_config(s, {"iterations_timed": len(hist) - 1}),
+            "config": workload_config(s, {"iterations_timed": len(hist) - 1,
+                                          "path": "plain: one shot per launch, no CUDA graphs" if args.invert_plain
+                                          else "batched engine, CUDA graphs, autotuned"}),
             "seconds_per_iteration": dt / max(1, len(hist) - 1),
             "residual": [h.residual for h in hist], "accepted_misfit": [h.res0 for h in hist],
             "misfit_passes": [h.misfit_passes for h in hist], "offset": [h.offset for h in hist],
@@ -609,7 +618,8 @@ def main():
     # cell, shared by the shots), 3 snapshot fields written (forward) or read with the 3 image
     # sums read and written (adjoint) per interior cell every nt_wf steps
     mat = s.nzbc * s.nxbc * 16
-    fwd_comp = cells * COMPULSORY_STATE_B + mat + spl * inner * 12 / s.nt_wf
+    snaps = info["mode"] == 1  # checkpoint mode: the forward phase writes no snapshots
+    fwd_comp = cells * COMPULSORY_STATE_B + mat + (spl * inner * 12 / s.nt_wf if snaps else 0)
     adj_comp = cells * COMPULSORY_STATE_B + mat + spl * inner * (12 + img_rmw) / s.nt_wf
     fwd_launch_ms = fwd_ms / s.nt * spl
     # checkpoint mode: the adjoint phase also re-runs the forward steps segment by segment
@@ -620,14 +630,21 @@ def main():
         # achieved: the compulsory bytes of one launch (state once in and out, materials,
         # snapshot / image terms) over its average CUDA-event time
         ach = comp / (launch_ms / 1e3) / 1e9
-        tr = NCU_BYTES_PER_CELL_LAUNCH.get(info["fd_schedule"], {}).get(name)
+        plain, extra = NCU_TRAFFIC.get(info["fd_schedule"], {}).get(name, (None, None))
+        if name == "fd_adj_step":
+            extra = (extra or {}).get(args.image_precision)
+        elif not snaps:
+            extra = 0.0
+        tr = plain * cells + spl / s.nt_wf * extra * inner if plain is not None and extra is not None else None
         return {"kernel": name, "bound": "hbm", "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak,
                 "peak_source": "measured (MEASURED_PEAKS.json hbm_gbs, copy kernel)" if peak_kind == "measured"
                 else "fallback 6650 GB/s",
-                "traffic": (tr * cells) if tr else None,
-                "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum, plain variant of FD schedule "
-                                   f"{info['fd_schedule']}, per launch") if tr else
-                f"no ncu capture of FD schedule {info['fd_schedule']} yet",
+                "traffic": tr,
+                "traffic_source": (f"ncu dram__bytes_read.sum + dram__bytes_write.sum of FD schedule "
+                                   f"{info['fd_schedule']}: plain launches and the snapshot / imaging variants, "
+                                   "averaged over the launches of the phase") if tr else
+                f"no ncu capture of every variant of FD schedule {info['fd_schedule']} with "
+                f"{args.image_precision} image sums",
                 "steps_per_launch": spl, "algorithmic_bytes_per_launch": comp,
                 "algorithmic_bytes": "compulsory: 40 B per shot-cell per launch (5 state fields in and out) + "
                                      "snapshot write / snapshot read + image update per interior cell every "
