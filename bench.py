@@ -64,6 +64,8 @@ def parse():
     p.add_argument("--plain-shots", type=int, default=8, help="shots timed on the one-shot-per-launch path")
     p.add_argument("--cpu-shots", type=int, default=0, help="CPU baseline sample size (0: one per host thread)")
     p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    p.add_argument("--no-variants", action="store_true",
+                   help="skip the legs with checkpoints every 50 steps and with FP64 image sums")
     p.add_argument("--snapshot-mode", type=int, default=0, help="0 auto, 1 store snapshots, 2 checkpoint")
     p.add_argument("--ckpt", type=int, default=0,
                    help="steps between checkpoints (snapshot mode 2; 0: memory-optimal)")
@@ -165,6 +167,42 @@ def workload_config(s, extra=None):
     if extra:
         c.update(extra)
     return c
+
+
+def variant_legs(s, info, cr0_r, cr0_l, dev, steps):
+    """The survey's stated configuration variants, on the same kernels and shape as the main line,
+    timed like `value` (inputs resident on the device, CUDA events on the engine's stream, one
+    warm-up step that captures the graphs): checkpoints every 50 steps with the adjoint
+    recomputing each segment, and FP64 per-shot image sums (the FP64 accumulation over time
+    steps) in the main line's adjoint mode."""
+    import torch
+
+    from swd_b200.engine import GradientEngine
+    shape = {k: info[k] for k in ("fd_schedule", "warps", "cells", "ring_fwd", "ring_adj")}
+    shape["chunk_rows"] = info["chunk_rows"]
+    legs = {"checkpoint_every_50_steps": {"snapshot_mode": 2, "ckpt_interval": 50},
+            "fp64_image_sums": {"snapshot_mode": info["mode"], "image_precision": "fp64"}}
+    d_vp = torch.from_numpy(np.ascontiguousarray(s.vp.T)).to(dev)
+    d_vs = torch.from_numpy(np.ascontiguousarray(s.vs.T)).to(dev)
+    d_dk = torch.zeros((s.nx, s.nz), dtype=torch.float64, device=dev)
+    out = {}
+    for name, kw in legs.items():
+        with GradientEngine(s, device=dev.index, **shape, **kw) as e:
+            e.set_observed(cr0_r, cr0_l)
+            e.gradient_device(d_vp, d_vs, d_dk)
+            st = torch.cuda.ExternalStream(e.stream(), device=dev)
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+            for _ in range(steps):
+                e.gradient_device(d_vp, d_vs, d_dk)
+            e1.record(st)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            out[name] = {"value": s.ns / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps,
+                         "adjoint": {1: "stored strain snapshots", 2: "checkpoint+recompute"}[e.info["mode"]],
+                         "ckpt_interval": e.info["ckpt_interval"], "image_sums": kw.get("image_precision", "fp32")}
+    return out
 
 
 # ------------------------------------------------------------------ CPU baseline (the reference's CPU path)
@@ -690,6 +728,8 @@ def main():
                              "how": "same kernels, one shot per launch, no CUDA graphs, host in/out per call"}
         line["batched_over_plain"] = line["e2e"]["value"] / line["plain_gpu"]["value"]
     sg.close()
+    if world == 1 and not args.no_variants and args.workload == "batched-100x600":
+        line["variants"] = variant_legs(s, info, cr0_r, cr0_l, dev, max(1, min(args.steps, 2)))
     if world == 1 and rank == 0 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(s, args.cpu_shots)
     if rank == 0:

@@ -219,7 +219,7 @@ def test_split_bf16_radon_in_the_engine(tiny_case, survey, O):
     certifying every gather (a decision within 1e-4 of the column maximum sends the gather to the
     FP64 contraction and is picked again).  Picks are identical to the FP64 engine's -- also on
     the 30 x 120 survey, where uncertified split-BF16 spectra moved one pick in 672 -- and the
-    gradient stays within the north-star bar (1e-4)."""
+    gradient stays within the 1e-4 gradient tolerance."""
     if survey == "tiny":
         s, cr0_r, cr0_l, _ = tiny_case
     else:
