@@ -197,6 +197,15 @@ int swd_adwdgrad_maxnorm(const swd_radon_params* p, int ns, int is, int w, doubl
  * magnitude (an all-zero trace becomes NaN, 0/0, as in the reference). */
 int swd_norm_trace(const double* data_in, int nt, int ng, double* data_out);
 
+/* Replaces [dfk]=fk_filter(d,dt,dx) (core/fk_filter.m:1-302; the same file in the
+ * fieldexamples drivers' core folders): the dip filter that the field drivers apply to a gather before the
+ * Radon transform when FK == 1 (fieldexamples/QadimahFault/core/RTrAD.m:14-16, RTlAD.m:15-17).
+ * d, dfk: ns x ntr (column-major, host).  The gather is zero-padded to 2ns x 2ntr; of its f-k
+ * spectrum the quadrants with frequency and wavenumber of the same sign (in fftshift order) are
+ * removed; the result is the leading ns x ntr block of the real part.  dt and dx only set axes
+ * that fk_filter.m computes and never uses; they are accepted for the same call. */
+int swd_fk_filter(const double* d, int ns, int ntr, double dt, double dx, double* dfk);
+
 /* Replaces ADWDgrad_norm(...) (core/ADWDgrad_norm.m:1-102, same arguments as ADWDgrad_1):
  * the SoftMax weights are replaced by normpdf(1:np, cr, 16) around the picks
  * (core/paddingMl_norm.m:1-9).  cr_r / cr_l: npair, saveForBackward.cr_r / cr_l = cr_pre - vmin

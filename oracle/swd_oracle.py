@@ -390,14 +390,18 @@ def velocities(vmin, vmax, dv=1.0):
     return vmin + dv * np.arange(n, dtype=np.float64)
 
 
-def radon(seismo, is_, df, dt, vmin, vmax, fmin, fmax, b, ds, offset, m, M, side, dv=1.0):
-    """RTrAD.m:2-35 / RTlAD.m:2-36 (ml is also RTr/RTl's output).
+def radon(seismo, is_, df, dt, vmin, vmax, fmin, fmax, b, ds, offset, m, M, side, dv=1.0, FK=0):
+    """RTrAD.m:2-35 / RTlAD.m:2-36 (ml is also RTr/RTl's output).  FK=1: the field drivers'
+    variant that f-k filters the gather before the transform
+    (fieldexamples/QadimahFault/core/RTrAD.m:14-16, RTlAD.m:15-17).
 
     Returns ml (np x npair, column-max normalised), dataLen and saveForBackward
     {mm (np x nf complex), ll0, lf, nf, ccn, ml_raw (np x npair), uxtpos (1-based cols, ascending)}.
     """
     cols = radon_window(is_, b, offset, m, M, side)
     uxt = np.asarray(seismo, np.float64)[:, [c - 1 for c in cols]]
+    if FK == 1:
+        uxt = fk_filter(uxt, dt, ds)
     noff = uxt.shape[1]
     x = (m + np.arange(noff, dtype=np.float64)) * ds
     ccn = int(math.trunc(1.0 / df / dt))
@@ -594,6 +598,24 @@ def norm_trace(data_in):
     d = np.asarray(data_in, np.float64)
     with np.errstate(invalid="ignore", divide="ignore"):
         return d / np.nanmax(np.abs(d), axis=0, keepdims=True)  # MATLAB's max skips NaN
+
+
+def fk_filter(d, dt, dx):
+    """core/fk_filter.m:1-302 (the same file in fieldexamples/*/core): the live code is the
+    fixed dip filter of its "case 6".  The ns x ntr data are zero-padded to 2ns x 2ntr (:49-51),
+    transformed by fft2 and fftshift (:52-53); in the shifted spectrum the quadrants
+    (i <= nf/2, j <= nk/2) and (i > nf/2, j > nk/2) are zeroed (:283-289); fftshift again (an
+    inverse shift for even sizes), real(ifft2) and the leading ns x ntr block (:293-296).
+    dt and dx only set axes that the live code never uses (:56-67, :237)."""
+    d = np.asarray(d, np.float64)
+    ns, ntr = d.shape
+    D = np.zeros((2 * ns, 2 * ntr))
+    D[:ns, :ntr] = d
+    D = np.fft.fftshift(np.fft.fft2(D))
+    nf, nk = D.shape
+    D[: nf // 2, : nk // 2] = 0.0
+    D[nf // 2:, nk // 2:] = 0.0
+    return np.real(np.fft.ifft2(np.fft.fftshift(D)))[:ns, :ntr]
 
 
 # --------------------------------------------------------------------------------------

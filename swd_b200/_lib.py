@@ -54,6 +54,7 @@ _SIGS = {
     "swd_adwdgrad_maxnorm": [_rpp, _c_int, _c_int, _c_int, _c_dbl] + [_f64p] * 8,
     "swd_pick_field": [_f64p, _f64p, _c_int, _c_int, _c_dbl, _f64p, _c_int, _c_int, _f64p, _f64p],
     "swd_norm_trace": [_f64p, _c_int, _c_int, _f64p],
+    "swd_fk_filter": [_f64p, _c_int, _c_int, ctypes.c_double, ctypes.c_double, _f64p],
     "swd_wd_residual": [_c_int, _c_int, _f64p, _f64p, _c_int, _c_dbl, _c_dbl, _c_int, _c_dbl, _c_int, _c_int,
                         _c_dbl, _c_int, _c_int, _f64p, _c_int, _c_dbl, _c_dbl] + [_f64p] * 4 + [_c_int, _f64p],
 }

@@ -35,6 +35,7 @@ SOURCES = {
     "server.cu": [],
     "radon_tc.cu": [],
     "wd.cu": [],
+    "fk.cu": [],
 }
 
 

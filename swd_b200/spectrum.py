@@ -35,11 +35,25 @@ def sizes(p: RadonParams):
     return tuple(o.value for o in out)  # np, npair, lf, nf, ccn
 
 
-def _radon(side, seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv):
+def _radon(side, seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv, FK=0):
     seis = np.asfortranarray(np.asarray(seismo_v1, np.float64))
     if seis.shape != (int(a), int(b)):
         raise ValueError(f"seismogram is {seis.shape}, expected a x b = {(a, b)}")
     p = radon_params(df, dt, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv)
+    if FK == 1:
+        # the field drivers' RTrAD/RTlAD filter the gather (as the transform orders it: the left
+        # side reversed) before transforming it; the filtered gather goes back into the same
+        # columns of a copy, in the same order, so that swd_radon reads exactly it
+        n = ctypes.c_int()
+        pos = np.zeros(int(offset) + 1, np.int32)
+        nv0 = sizes(p)[0]
+        call("swd_radon", ctypes.byref(p), side, int(is_), ptr(seis), ptr(np.zeros((nv0, sizes(p)[1]), order="F")),
+             None, None, ctypes.byref(n), ptr(pos))
+        cols = np.sort(pos[: n.value]) - 1
+        if side == 1:
+            cols = cols[::-1]
+        seis = seis.copy(order="F")
+        seis[:, cols] = fk_filter(seis[:, cols], dt, ds)
     nv, npair, lf, nf, ccn = sizes(p)
     if np_ is not None and int(np_) != nv:
         raise ValueError(f"np={np_} but the velocity axis has {nv} entries")
@@ -58,25 +72,27 @@ def _radon(side, seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, 
     return ml, n.value, save
 
 
-def RTrAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0):
-    """[ml,dataLen,saveForBackward]=RTrAD(...) (core/RTrAD.m:2)."""
-    return _radon(0, seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv)
+def RTrAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0, FK=0):
+    """[ml,dataLen,saveForBackward]=RTrAD(...) (core/RTrAD.m:2); FK=1 f-k filters the gather first, as
+    fieldexamples/QadimahFault/core/RTrAD.m:14-16 does."""
+    return _radon(0, seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv, FK)
 
 
-def RTlAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0):
-    """[ml,dataLen,saveForBackward]=RTlAD(...) (core/RTlAD.m:2)."""
-    return _radon(1, seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv)
+def RTlAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0, FK=0):
+    """[ml,dataLen,saveForBackward]=RTlAD(...) (core/RTlAD.m:2); FK=1 f-k filters the gather first, as
+    fieldexamples/QadimahFault/core/RTlAD.m:15-17 does."""
+    return _radon(1, seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv, FK)
 
 
-def RTr(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0):
-    """[ml,dataLen]=RTr(...) (core/RTr.m:2)."""
-    ml, n, _ = RTrAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv)
+def RTr(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0, FK=0):
+    """[ml,dataLen]=RTr(...) (core/RTr.m:2); FK as in RTrAD."""
+    ml, n, _ = RTrAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv, FK)
     return ml, n
 
 
-def RTl(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0):
-    """[ml,dataLen]=RTl(...) (core/RTl.m:2)."""
-    ml, n, _ = RTlAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv)
+def RTl(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv=1.0, FK=0):
+    """[ml,dataLen]=RTl(...) (core/RTl.m:2); FK as in RTlAD."""
+    ml, n, _ = RTlAD(seismo_v1, is_, df, dt, np_, vmin, vmax, fmin, fmax, a, b, ds, offset, m, M, dv, FK)
     return ml, n
 
 
@@ -109,6 +125,16 @@ def LHDispPick_field(ml, vmin, cr_0, method, saveForBackward, variant=1):
     call("swd_pick_field", ptr(ml), ptr(raw), nv, npair, float(vmin), ptr(cr0), int(method), int(variant),
          ctypes.byref(res), ptr(cr))
     return res.value, cr
+
+
+def fk_filter(d, dt, dx):
+    """[dfk]=fk_filter(d,dt,dx) (core/fk_filter.m:1): the f-k dip filter of the field drivers."""
+    d = np.asfortranarray(np.asarray(d, np.float64))
+    if d.ndim != 2:
+        raise ValueError("fk_filter takes a 2-D gather (time x traces)")
+    out = np.zeros(d.shape, order="F")
+    call("swd_fk_filter", ptr(d), d.shape[0], d.shape[1], float(dt), float(dx), ptr(out))
+    return out
 
 
 def norm_trace(data_in):

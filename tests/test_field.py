@@ -63,6 +63,35 @@ def test_norm_trace_oracle(O):
     assert np.allclose(np.abs(out[:, ok]).max(0), 1.0)
 
 
+def _fk_by_offset_operator(d):
+    """The f-k filter as the GPU computes it: time DFT of the padded traces, one wavenumber
+    operator per frequency half (h_plus for u_f < nf/2, h_minus otherwise), inverse time DFT."""
+    ns, ntr = d.shape
+    nf, nk = 2 * ns, 2 * ntr
+    T = np.fft.fft(np.vstack([d, np.zeros_like(d)]), axis=0)  # nf x ntr
+    u = np.arange(nk)
+    m = (np.arange(ntr)[None, :] - np.arange(ntr)[:, None]) % nk  # [x, x'] -> x' - x mod nk
+    e = np.exp(2j * np.pi * np.outer(np.arange(nk), u) / nk) / nk  # [m, u_k]
+    hp, hm = e[:, u >= nk // 2].sum(1), e[:, u < nk // 2].sum(1)
+    R = np.where((np.arange(nf) < nf // 2)[:, None], T @ hp[m], T @ hm[m])
+    return np.real(np.fft.ifft(R, axis=0))[:ns]
+
+
+def test_fk_filter_oracle_and_the_gpu_algebra(O):
+    rng = np.random.default_rng(6)
+    for ns, ntr in ((40, 7), (33, 1), (64, 12)):
+        d = rng.standard_normal((ns, ntr))
+        ref = O.fk_filter(d, 1e-3, 0.5)
+        assert np.allclose(_fk_by_offset_operator(d), ref, rtol=0, atol=1e-12 * np.abs(ref).max())
+    # a dip filter: an event whose arrival time grows with the trace index passes, the opposite
+    # dip is mostly removed
+    t, x = np.arange(128)[:, None], np.arange(16)[None, :]
+    fwd = np.exp(-0.5 * ((t - 20 - 3.0 * x) / 2.0) ** 2)
+    bwd = np.exp(-0.5 * ((t - 70 + 3.0 * x) / 2.0) ** 2)
+    assert np.linalg.norm(O.fk_filter(fwd, 1e-3, 0.5)) > 0.8 * np.linalg.norm(fwd)
+    assert np.linalg.norm(O.fk_filter(bwd, 1e-3, 0.5)) < 0.3 * np.linalg.norm(bwd)
+
+
 # ------------------------------------------------------------------ GPU
 
 @pytest.mark.gpu
@@ -133,3 +162,39 @@ def test_field_shot_loop_with_manual_picks_matches_oracle(O, field):
     for k in ("g_cl", "g_cm", "g_illum", "dk_vs"):
         assert np.linalg.norm(got[k] - ref[k]) / np.linalg.norm(ref[k]) < 1e-9, k
     np.testing.assert_allclose(got["res_r"], ref["res_r"], rtol=1e-12, equal_nan=True)
+
+
+@pytest.mark.gpu
+def test_fk_filter_matches_oracle(O):
+    from swd_b200 import spectrum as SP
+    rng = np.random.default_rng(7)
+    for ns, ntr in ((400, 17), (37, 5), (1000, 1), (8000, 45)):  # 2*37: a 2 x 37 four-step split
+        d = rng.standard_normal((ns, ntr))
+        ref = O.fk_filter(d, 5e-5, 0.5)
+        got = SP.fk_filter(d, 5e-5, 0.5)
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-12, (ns, ntr)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("side", ["r", "l"])
+def test_radon_with_fk_filter_matches_oracle(O, side):
+    """RTrAD/RTlAD with FK=1 (the field drivers' option): the gather, in the transform's trace
+    order, is f-k filtered before the transform."""
+    from swd_b200 import spectrum as SP
+    s = configs.plain_c1()
+    inp = O.fd_inputs(s.nbc, s.nt, s.dtx, s.dx, s.dt, int(s.sx[5]), 1, s.gx, np.ones(s.ng), s.vp, s.vs,
+                      in_wf=s.nt_wf)
+    seis = O.mex_staggerfd(inp, s.source())[1].astype(np.float64)
+    for is_ in (1, 6, 12):
+        ml_ref, n_ref, save_ref = O.radon(seis, is_, s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.ng, s.ds,
+                                          s.offset, s.m, s.M, side, s.dv, FK=1)
+        f = SP.RTrAD if side == "r" else SP.RTlAD
+        ml, n, save = f(seis, is_, s.df, s.dt, None, s.vmin, s.vmax, s.fmin, s.fmax, s.nt, s.ng, s.ds, s.offset,
+                        s.m, s.M, s.dv, FK=1)
+        assert n == n_ref
+        assert np.linalg.norm(ml - ml_ref) / np.linalg.norm(ml_ref) < 1e-9, is_
+        assert np.linalg.norm(save["mm"] - save_ref["mm"]) / np.linalg.norm(save_ref["mm"]) < 1e-9, is_
+        plain = f(seis, is_, s.df, s.dt, None, s.vmin, s.vmax, s.fmin, s.fmax, s.nt, s.ng, s.ds, s.offset, s.m,
+                  s.M, s.dv)[0]
+        if n > 2:  # a one-trace gather's normalised spectrum is all ones, filtered or not
+            assert not np.allclose(plain, ml)  # the filter changed the spectrum

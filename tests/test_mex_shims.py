@@ -18,7 +18,7 @@ from swd_b200 import configs  # noqa: E402
 
 SHIMS = ["eigen_staggerfd_single", "eigen_staggerfd_double", "eigen_e2drtm_single", "eigen_e2drtm_double",
          "RTrAD", "RTlAD", "RTr", "RTl", "LHDispPick", "ADWDgrad_1", "ADWDgrad_norm", "ADWDgradlimband",
-         "weight_data_muti3", "norm_trace", "field/LHDispPick", "field/ADWDgrad_1"]
+         "weight_data_muti3", "norm_trace", "fk_filter", "field/LHDispPick", "field/ADWDgrad_1"]
 
 
 @pytest.fixture(scope="module")
