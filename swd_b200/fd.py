@@ -134,6 +134,17 @@ def staggerfd_eigend(is_, nbc, nt, dtx, dx, dt, sx, sz, gx, gz, s, vp, vs, isfs=
                       parameter_type, in_wf)
 
 
+def staggerfd_eigen_field(is_, nbc, nt, dtx, dx, dt, sx, sz, gx, gz, s, vp, vs, isfs, fsz, fd_order, source_type,
+                          parameter_type, dt_wf=None, nt_wf=None):
+    """[seismo_u,seismo_w,www]=staggerfd_eigen(...) of the QadimahFault driver
+    (fieldexamples/QadimahFault/core/staggerfd_eigen.m:2, function staggerfd8): core's wrapper with
+    the snapshot interval given as a time, in_wf = dt_wf/dt (:157; dt_wf = dt when omitted,
+    :37-40).  fsz and nt_wf are accepted and unused, as there."""
+    in_wf = (dt if dt_wf is None else dt_wf) / dt  # goes to the single input vector, as there
+    return _staggerfd(True, is_, nbc, nt, dtx, dx, dt, sx, sz, gx, gz, s, vp, vs, isfs, fd_order, source_type,
+                      parameter_type, in_wf)
+
+
 def _e2drtm(single, wavefield_gradient, seismo_w, is_, nbc, nt, dtx, dx, dt, gx, gz, s, vp, vs, isfs, fd_order,
             parameter_type, in_wf, fp64_out=False):
     if parameter_type != 0:
@@ -154,6 +165,16 @@ def _e2drtm(single, wavefield_gradient, seismo_w, is_, nbc, nt, dtx, dx, dt, gx,
 def e2drtm_eigen(wavefield_gradient, seismo_w, is_, nbc, nt, dtx, dx, dt, gx, gz, s, vp, vs, isfs=1, fd_order=22,
                  parameter_type=0, in_wf=5, fp64_out=False):
     """[cl_img,cm_img,illum_div]=e2drtm_eigen(...) (core/e2drtm_eigen.m:8)."""
+    return _e2drtm(True, wavefield_gradient, seismo_w, is_, nbc, nt, dtx, dx, dt, gx, gz, s, vp, vs, isfs, fd_order,
+                   parameter_type, in_wf, fp64_out)
+
+
+def e2drtm_eigen_field(wavefield_gradient, seismo_w, is_, nbc, nt, dtx, dx, dt, gx, gz, s, vp, vs, isfs, fsz, fd_order,
+                       parameter_type, dt_wf=None, fp64_out=False):
+    """[cl_img,cm_img,illum_div]=e2drtm_eigen(...) of the QadimahFault driver
+    (fieldexamples/QadimahFault/core/e2drtm_eigen.m:8): core's wrapper with in_wf = dt_wf/dt (:147;
+    dt_wf = dt when omitted, :43-45).  fsz only enters statements without effect there (:85-87, :94)."""
+    in_wf = (dt if dt_wf is None else dt_wf) / dt
     return _e2drtm(True, wavefield_gradient, seismo_w, is_, nbc, nt, dtx, dx, dt, gx, gz, s, vp, vs, isfs, fd_order,
                    parameter_type, in_wf, fp64_out)
 

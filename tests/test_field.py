@@ -198,3 +198,24 @@ def test_radon_with_fk_filter_matches_oracle(O, side):
                   s.M, s.dv)[0]
         if n > 2:  # a one-trace gather's normalised spectrum is all ones, filtered or not
             assert not np.allclose(plain, ml)  # the filter changed the spectrum
+
+
+@pytest.mark.gpu
+def test_qadimahfault_fd_wrappers_are_core_with_a_time_interval():
+    """QademahSWD3.m's staggerfd_eigen / e2drtm_eigen take an unused fsz and the snapshot interval
+    as a time (dt_wf = 10 dt there, :96): the same bits as core's wrappers with in_wf = 10."""
+    from swd_b200 import fd as F
+    s = configs.tiny(nt=400)
+    w = s.source().astype(np.float32)
+    geo = (1, s.nbc, s.nt, s.dtx, s.dx, s.dt, 5, 1, s.gx, np.ones(s.ng), w, s.vp, s.vs)
+    su, sw, www = F.staggerfd_eigen(*geo, 1, 22, "w", 0, 10)
+    fu, fw, fww = F.staggerfd_eigen_field(*geo, 1, 0, 22, "w", 0, 10 * s.dt, (s.nt - 1) // 10 + 1)
+    assert np.array_equal(su, fu) and np.array_equal(sw, fw)
+    for k in ("fux", "fuz", "bwx", "bwz"):
+        assert np.array_equal(www[k], fww[k]), k
+    res = np.asfortranarray(sw * 0.5)
+    adj = (1, s.nbc, s.nt, s.dtx, s.dx, s.dt, s.gx, np.ones(s.ng), w, s.vp, s.vs)
+    core = F.e2drtm_eigen(www, res, *adj, 1, 22, 0, 10)
+    field = F.e2drtm_eigen_field(fww, res, *adj, 1, 0, 22, 0, 10 * s.dt)
+    for a, b in zip(core, field):
+        assert np.array_equal(a, b)
