@@ -110,6 +110,8 @@ extern "C" int swd_fk_filter(const double* d, int ns, int ntr, double dt, double
   (void)dx;
   clear_error();
   SWD_CHECK(d && dfk && ns >= 1 && ntr >= 1, "bad fk_filter arguments (ns %d, ntr %d)", ns, ntr);
+  SWD_CHECK(ntr <= 65535 && ns <= (1 << 29), "fk_filter gather too large (ns %d, ntr %d; traces index the grid's "
+            "y dimension, at most 65535)", ns, ntr);
   const int nf = 2 * ns, nk = 2 * ntr;
   int L1 = 1;
   for (int q = 1; (long long)q * q <= nf; ++q)

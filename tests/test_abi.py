@@ -49,6 +49,16 @@ def test_calls_validate_before_touching_the_gpu():
     assert e.value.status == 1
 
 
+def test_fk_filter_validates_before_touching_the_gpu():
+    import numpy as np
+    from swd_b200 import _lib
+    d = np.zeros((4, 3))
+    for ns, ntr in ((0, 3), (4, 0), (4, 70000)):
+        with pytest.raises(_lib.SwdError) as e:
+            _lib.call("swd_fk_filter", _lib.ptr(d), ns, ntr, 1e-3, 0.5, _lib.ptr(d))
+        assert e.value.status == 1
+
+
 def test_engine_options_validate_before_touching_the_gpu():
     """Out-of-range engine options are reported as such, before any CUDA call."""
     import ctypes
