@@ -873,13 +873,13 @@ def _sides(s, is_):
     return has_right(g, _ns(s), s.m, s.M, s.w), has_left(g, s.m, s.M, s.w)
 
 
-def _spectra(s, seis, is_):
+def _spectra(s, seis, is_, FK=0):
     out = {}
     r_on, l_on = _sides(s, is_)
     for side, on in (("r", r_on), ("l", l_on)):
         if on:
             out[side] = radon(seis, _gno(s, is_), s.df, s.dt, s.vmin, s.vmax, s.fmin, s.fmax, s.ng, s.ds, s.offset,
-                              s.m, s.M, side, s.dv)
+                              s.m, s.M, side, s.dv, FK)
     return out
 
 
@@ -911,21 +911,24 @@ def _fd_pair(fd, single, accum_fp64):
 
 
 def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=False, single=True, vp=None, weight="softmax",
-                  fd="oracle", field=0):
+                  fd="oracle", field=0, FK=0):
     """SWD_single.m:172-193 for one shot: forward (FP32), spectra, picks, ADWDgrad_1, adjoint.
     single=False: SWD.m's double path (FP64 FD, adjoint source kept in double).  accum_fp64=False
     (default) sums the single path's images in FP32, as the reference's single MEX does.
     fd="reference" runs the FD steps on the reference's own MEX sources (oracle/_ref).
     field=1 / 2: the field-data flow (fieldexamples/outcrop/outcrop.m:168-196): norm_trace of the
     predicted gather (in the data's precision), the field picker variant, the max-normalised
-    ADWDgrad_1 (fieldexamples/outcrop/core/ADWDgrad_1.m:79)."""
+    ADWDgrad_1 (fieldexamples/outcrop/core/ADWDgrad_1.m:79).  FK=1: the gathers are f-k filtered
+    before the Radon transform (fieldexamples/QadimahFault/QademahSWD3.m:119, core/RTrAD.m:14-16);
+    the adjoint source is built from the filtered spectra, with no filter in the backward pass, as
+    there."""
     fwd, adj = _fd_pair(fd, single, accum_fp64)
     inp = _survey_fd(s, is_, vs, single, vp=vp)
     _, sw, wf = fwd(inp, s.source())
     if field:
         sw_n = norm_trace(sw.astype(np.float64))
         sw = sw_n.astype(np.float32) if single else sw_n
-    sp = _spectra(s, sw.astype(np.float64), is_)
+    sp = _spectra(s, sw.astype(np.float64), is_, FK)
     npair = s.npair
     out = {"res_r": np.nan, "res_l": np.nan, "crp_r": np.ones(npair), "crp_l": np.ones(npair)}
     def pick(sd, cr0):
@@ -961,7 +964,7 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, accum_fp64=False, single=True, vp=No
 
 
 def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=False, single=True, vp=None, weight="softmax",
-             fd="oracle", field=0):
+             fd="oracle", field=0, FK=0):
     """SWD_single.m:171-201 (SWD.m with single=False) with the shot sum in FP64 in shot order
     (per-shot images as shot_gradient)."""
     from concurrent.futures import ThreadPoolExecutor
@@ -969,9 +972,9 @@ def gradient(s, vs, cr0_r, cr0_l, threads=1, accum_fp64=False, single=True, vp=N
     if threads > 1:
         with ThreadPoolExecutor(threads) as ex:
             per = list(ex.map(lambda i: shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight, fd,
-                                                      field), shots))
+                                                      field, FK), shots))
     else:
-        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight, fd, field) for i in shots]
+        per = [shot_gradient(s, i, vs, cr0_r, cr0_l, accum_fp64, single, vp, weight, fd, field, FK) for i in shots]
     g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
     for p in per:
         for k in g:

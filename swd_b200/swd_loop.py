@@ -73,29 +73,31 @@ def _seismogram(s, is_, vs, single, want_wf=True):
     return sw, www
 
 
-def spectra(s, seismo, is_):
-    """RTrAD / RTlAD of one shot's vertical-component record for the sides it has (SWD.m:174-185)."""
+def spectra(s, seismo, is_, FK=0):
+    """RTrAD / RTlAD of one shot's vertical-component record for the sides it has (SWD.m:174-185);
+    FK=1 f-k filters the gathers first (the field drivers' option)."""
     shot_no = int(s.shot_no[is_ - 1]) if s.shot_no is not None else is_
     ns = s.ns_total or s.ns
     args = (shot_no, s.df, s.dt, s.np_vel, s.vmin, s.vmax, s.fmin, s.fmax, s.nt, s.ng, s.ds, s.offset, s.m, s.M,
             s.dv)
     out = {}
     if has_right(shot_no, ns, s.m, s.M, s.w):
-        out["r"] = RTrAD(np.asarray(seismo, np.float64), *args)
+        out["r"] = RTrAD(np.asarray(seismo, np.float64), *args, FK=FK)
     if has_left(shot_no, s.m, s.M, s.w):
-        out["l"] = RTlAD(np.asarray(seismo, np.float64), *args)
+        out["l"] = RTlAD(np.asarray(seismo, np.float64), *args, FK=FK)
     return out
 
 
-def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True, field=0):
+def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True, field=0, FK=0):
     """SWD.m:172-193 for shot is_ (1-based in s): images cl, cm, illum plus picks and misfits
-    (field 1 / 2: the field-data flow, see the module docstring)."""
+    (field 1 / 2: the field-data flow, see the module docstring; FK=1: the gathers f-k filtered
+    before the transform, QademahSWD3.m:119)."""
     sw, www = _seismogram(s, is_, vs, single)
     if field:
         # outcrop.m:174; on single data MATLAB divides in single (the FP64 quotient rounded to
         # FP32 is that same single quotient)
         sw = norm_trace(sw).astype(np.float32) if single else norm_trace(sw)
-    sp = spectra(s, sw, is_)
+    sp = spectra(s, sw, is_, FK)
     npair = s.npair
     shot_no = int(s.shot_no[is_ - 1]) if s.shot_no is not None else is_
     ns = s.ns_total or s.ns
@@ -128,12 +130,12 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True, field=0):
     return out
 
 
-def gradient(s, vs, cr0_r, cr0_l, single=True, keep_shots=False, field=0):
+def gradient(s, vs, cr0_r, cr0_l, single=True, keep_shots=False, field=0, FK=0):
     """SWD.m:171-201: shot sums in shot order (FP64), Vs gradient, smoothing, misfit."""
     g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
     res_r, res_l, crp_r, crp_l, per = [], [], [], [], []
     for is_ in range(1, s.ns + 1):
-        p = shot_gradient(s, is_, vs, cr0_r, cr0_l, single, field)
+        p = shot_gradient(s, is_, vs, cr0_r, cr0_l, single, field, FK)
         for k in g:
             g[k] = g[k] + p[k]
         res_r.append(p["res_r"])

@@ -146,18 +146,19 @@ def test_maxnorm_adjoint_source_matches_oracle(O):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("field", [1, 2])
-def test_field_shot_loop_with_manual_picks_matches_oracle(O, field):
+@pytest.mark.parametrize("field,FK", [(1, 0), (2, 0), (2, 1)])
+def test_field_shot_loop_with_manual_picks_matches_oracle(O, field, FK):
     """outcrop.m's shot loop in double (its wrappers call the _double MEX) with manual-pick
-    observed curves: picks identical, gradient and misfit to 1e-9."""
+    observed curves: picks identical, gradient and misfit to 1e-9; FK=1 is QademahSWD3.m's
+    f-k filter option (:119)."""
     from swd_b200 import swd_loop
     s = dataclasses.replace(configs.tiny(nt=400, ns=5), df=1.0)  # 161 frequencies: room for the edge rows
     cr0_r, cr0_l = O.observed_curves(s, s.vs_true, single=False)
     rng = np.random.default_rng(5)
     man_r = cr0_r + rng.integers(-4, 5, cr0_r.shape)  # "manual" picks: the true curves, hand-nudged
     man_l = cr0_l + rng.integers(-4, 5, cr0_l.shape)
-    ref = O.gradient(s, s.vs, man_r, man_l, single=False, field=field)
-    got = swd_loop.gradient(s, s.vs, man_r, man_l, single=False, field=field)
+    ref = O.gradient(s, s.vs, man_r, man_l, single=False, field=field, FK=FK)
+    got = swd_loop.gradient(s, s.vs, man_r, man_l, single=False, field=field, FK=FK)
     assert np.array_equal(got["cr_pre_r"], ref["cr_pre_r"]) and np.array_equal(got["cr_pre_l"], ref["cr_pre_l"])
     for k in ("g_cl", "g_cm", "g_illum", "dk_vs"):
         assert np.linalg.norm(got[k] - ref[k]) / np.linalg.norm(ref[k]) < 1e-9, k
