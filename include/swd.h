@@ -59,6 +59,23 @@ int swd_staggerfd_single(const float* iv, int n_iv, const float* temp, const flo
                          const float* b1, const float* s, float* seismo_u, float* seismo_w,
                          float* fux, float* fuz, float* bwx, float* bwz);
 
+/* Several eigen_staggerfd_single calls, on grids of any sizes, advanced together: one launch per
+ * time step covers the tiles of every job (each CTA finds its job from the jobs' running tile
+ * counts and reads that job's geometry, materials, state, source and receivers).  It has no
+ * counterpart in the reference, where each shot and model is a separate MEX call
+ * (core/staggerfd_eigen.m:138-140).  A job is one call's arguments as for
+ * swd_staggerfd_single, without the wavefield outputs; its seismograms are the same, bit for bit.
+ * Jobs may differ in grid, nt, source and receivers; a job with fewer steps idles after them. */
+typedef struct {
+  const float* iv;      /* input_vector (16 entries) */
+  int n_iv;
+  const float *temp, *ca, *cl, *cm, *cm1, *b, *b1; /* nzbc x nxbc */
+  const float* s;       /* wavelet, nt */
+  float* seismo_u;      /* nt x ng, may be NULL */
+  float* seismo_w;      /* nt x ng */
+} swd_staggerfd_job;
+int swd_staggerfd_single_batch(int n_jobs, const swd_staggerfd_job* jobs);
+
 /* Replaces eigen_staggerfd_double (binary-only in the reference; interface at
  * core/staggerfd_eigend.m:139).  Same arguments in double precision. */
 int swd_staggerfd_double(const double* iv, int n_iv, const double* temp, const double* ca,

@@ -4,6 +4,8 @@
 #include <cstdarg>
 #include <cstring>
 #include <atomic>
+#include <memory>
+#include <string>
 #include <type_traits>
 #include <vector>
 
@@ -503,12 +505,24 @@ int fill_geom(FdGeom& g, int NZ, int NX, int nz, int nx, int nbc, int nt, int nt
   return SWD_OK;
 }
 
+// The device side of one MEX-convention forward call: its buffers, arguments and host outputs.
 template <typename T>
-int staggerfd_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, const T* cm, const T* cm1,
-                  const T* b, const T* b1, const T* s, T* seis_u, T* seis_w, T* fux, T* fuz, T* bwx, T* bwz) {
-  clear_error();
-  (void)cm;  // passed by the reference, unused by its kernel (cm1 carries mu)
-  FwdIv p;
+struct FwdJob {
+  FwdIv p{};
+  FdGeom g{};
+  DevBuf d_in, d_m1, d_m2, d_state, d_seis, d_seis_t, d_snap, d_snap_t, d_src;
+  FwdArgs<T> a{};
+  T* bufs[2] = {nullptr, nullptr};
+  T* out[6] = {};  // host: seis_u, seis_w, fux, fuz, bwx, bwz
+};
+
+// Validates the call, allocates and fills the job's device buffers on st (materials packed,
+// state and seismograms cleared); the time loop then sets a.in / a.out from bufs.
+template <typename T>
+int fwd_job_setup(FwdJob<T>& J, const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, const T* cm1,
+                  const T* b, const T* b1, const T* s, T* seis_u, T* seis_w, T* fux, T* fuz, T* bwx, T* bwz,
+                  cudaStream_t st) {
+  FwdIv& p = J.p;
   SWD_TRY(parse_fwd_iv(iv, n_iv, p));
   const int nbc = (p.nxbc - p.nx) / 2;  // core/eigen_staggerfd_single.cpp:116
   SWD_TRY(validate_geom(p.nt, p.nzbc, p.nxbc, p.nz, p.nx, nbc, p.nt_wf, p.fd_order, p.ng, p.gz, p.gx, p.dg));
@@ -516,63 +530,82 @@ int staggerfd_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl
   SWD_CHECK(temp && ca && cl && cm1 && b && b1 && s && seis_w, "null input/output pointer");
   const bool want_wf = fux || fuz || bwx || bwz;
   SWD_CHECK(!want_wf || (fux && fuz && bwx && bwz), "fux/fuz/bwx/bwz must all be given or all be NULL");
-  FdGeom g{};
+  FdGeom& g = J.g;
   fill_geom<T>(g, p.nzbc, p.nxbc, p.nz, p.nx, nbc, p.nt, p.nt_wf, p.ng, p.gz, p.gx, p.dg);
   plan_decomposition(g, 1, 0);
   using V = typename Vec4<T>::type;
   using V2 = typename Vec2<T>::type;
   const size_t NN = (size_t)p.nzbc * p.nxbc, plane = (size_t)p.nz * p.nx;
-  DevBuf d_in, d_m1, d_m2, d_state, d_seis, d_seis_t, d_snap, d_snap_t, d_src;
-  SWD_TRY(d_in.alloc(6 * NN * sizeof(T) + p.nt * sizeof(T)));
-  SWD_TRY(d_m1.alloc(g.field * sizeof(V)));
-  SWD_TRY(d_m2.alloc(g.field * sizeof(V2)));
-  SWD_TRY(d_state.alloc(2 * 5 * g.field * sizeof(T)));
-  SWD_TRY(d_seis.alloc(2 * (size_t)p.nt * p.ng * sizeof(T)));
-  SWD_TRY(d_seis_t.alloc(2 * (size_t)p.nt * p.ng * sizeof(T)));
-  SWD_TRY(d_src.alloc(sizeof(int2)));
+  SWD_TRY(J.d_in.alloc(6 * NN * sizeof(T) + p.nt * sizeof(T)));
+  SWD_TRY(J.d_m1.alloc(g.field * sizeof(V)));
+  SWD_TRY(J.d_m2.alloc(g.field * sizeof(V2)));
+  SWD_TRY(J.d_state.alloc(2 * 5 * g.field * sizeof(T)));
+  SWD_TRY(J.d_seis.alloc(2 * (size_t)p.nt * p.ng * sizeof(T)));
+  SWD_TRY(J.d_seis_t.alloc(2 * (size_t)p.nt * p.ng * sizeof(T)));
+  SWD_TRY(J.d_src.alloc(sizeof(int2)));
   if (want_wf) {
-    SWD_TRY(d_snap.alloc((size_t)g.nrec * 4 * plane * sizeof(T)));
-    SWD_TRY(d_snap_t.alloc((size_t)g.nrec * plane * sizeof(T)));
+    SWD_TRY(J.d_snap.alloc((size_t)g.nrec * 4 * plane * sizeof(T)));
+    SWD_TRY(J.d_snap_t.alloc((size_t)g.nrec * plane * sizeof(T)));
   }
-  cudaStream_t st = 0;
-  T* din = d_in.as<T>();
+  T* din = J.d_in.template as<T>();
   const T* hsrc[6] = {temp, b, b1, ca, cl, cm1};
   for (int i = 0; i < 6; ++i) SWD_CUDA(cudaMemcpyAsync(din + i * NN, hsrc[i], NN * sizeof(T), cudaMemcpyHostToDevice, st));
   T* d_s = din + 6 * NN;
   SWD_CUDA(cudaMemcpyAsync(d_s, s, p.nt * sizeof(T), cudaMemcpyHostToDevice, st));
-  int2 sp = make_int2(p.sz, p.sx);
-  SWD_CUDA(cudaMemcpyAsync(d_src.p, &sp, sizeof(int2), cudaMemcpyHostToDevice, st));
-  SWD_TRY(pack_materials<T>(din, din + NN, din + 2 * NN, din + 3 * NN, din + 4 * NN, din + 5 * NN, d_m1.as<V>(),
-                            d_m2.as<V2>(), p.nzbc, p.nxbc, g.pitch, st));
-  SWD_CUDA(cudaMemsetAsync(d_state.p, 0, d_state.bytes, st));
-  SWD_CUDA(cudaMemsetAsync(d_seis.p, 0, d_seis.bytes, st));
-  FwdArgs<T> a{};
-  a.g = g; a.mat = d_m1.as<V>(); a.mb = d_m2.as<V2>();
-  a.src = d_src.as<int2>(); a.src_type = p.src_type; a.s = d_s; a.dtx = (T)p.dtx;
-  a.seis_w = d_seis.as<T>(); a.seis_u = a.seis_w + (size_t)p.nt * p.ng;
-  a.snap = want_wf ? d_snap.as<T>() : nullptr;
+  const int2 sp = make_int2(p.sz, p.sx);
+  SWD_CUDA(cudaMemcpyAsync(J.d_src.p, &sp, sizeof(int2), cudaMemcpyHostToDevice, st));
+  SWD_TRY(pack_materials<T>(din, din + NN, din + 2 * NN, din + 3 * NN, din + 4 * NN, din + 5 * NN, J.d_m1.template as<V>(),
+                            J.d_m2.template as<V2>(), p.nzbc, p.nxbc, g.pitch, st));
+  SWD_CUDA(cudaMemsetAsync(J.d_state.p, 0, J.d_state.bytes, st));
+  SWD_CUDA(cudaMemsetAsync(J.d_seis.p, 0, J.d_seis.bytes, st));
+  FwdArgs<T>& a = J.a;
+  a.g = g; a.mat = J.d_m1.template as<V>(); a.mb = J.d_m2.template as<V2>();
+  a.src = J.d_src.template as<int2>(); a.src_type = p.src_type; a.s = d_s; a.dtx = (T)p.dtx;
+  a.seis_w = J.d_seis.template as<T>(); a.seis_u = a.seis_w + (size_t)p.nt * p.ng;
+  a.snap = want_wf ? J.d_snap.template as<T>() : nullptr;
   a.n_shots = 1;
-  T* bufs[2] = {d_state.as<T>(), d_state.as<T>() + 5 * g.field};
-  for (int it = 0; it < p.nt; ++it) {
-    a.in = bufs[it & 1];
-    a.out = bufs[(it + 1) & 1];
-    SWD_TRY(launch_fwd_step<T, 4>(a, it, st));  // a dispatch or geometry error ends the call
-  }
-  SWD_CUDA(cudaGetLastError());
-  // seismograms: [2][nt][ng] -> MATLAB nt x ng (column-major) each
-  SWD_TRY(transpose<T, T>(d_seis.as<T>(), (size_t)p.nt * p.ng, d_seis_t.as<T>(), (size_t)p.nt * p.ng, 2, p.nt, p.ng, st));
-  SWD_CUDA(cudaMemcpyAsync(seis_w, d_seis_t.as<T>(), (size_t)p.nt * p.ng * sizeof(T), cudaMemcpyDeviceToHost, st));
-  if (seis_u)
-    SWD_CUDA(cudaMemcpyAsync(seis_u, d_seis_t.as<T>() + (size_t)p.nt * p.ng, (size_t)p.nt * p.ng * sizeof(T),
-                             cudaMemcpyDeviceToHost, st));
-  if (want_wf) {
-    // snapshots [nrec][f][nz][nx] -> MATLAB nz x nx x nrec per field
-    T* outs[4] = {fux, fuz, bwx, bwz};
+  J.bufs[0] = J.d_state.template as<T>();
+  J.bufs[1] = J.d_state.template as<T>() + 5 * g.field;
+  T* const outs[6] = {seis_u, seis_w, fux, fuz, bwx, bwz};
+  for (int i = 0; i < 6; ++i) J.out[i] = outs[i];
+  return SWD_OK;
+}
+
+// Enqueues the job's outputs on st: seismograms [2][nt][ng] -> MATLAB nt x ng (column-major)
+// each; snapshots [nrec][f][nz][nx] -> nz x nx x nrec per field.
+template <typename T>
+int fwd_job_finish(FwdJob<T>& J, cudaStream_t st) {
+  const FwdIv& p = J.p;
+  const size_t plane = (size_t)p.nz * p.nx, nn = (size_t)p.nt * p.ng;
+  SWD_TRY(transpose<T, T>(J.d_seis.template as<T>(), nn, J.d_seis_t.template as<T>(), nn, 2, p.nt, p.ng, st));
+  SWD_CUDA(cudaMemcpyAsync(J.out[1], J.d_seis_t.template as<T>(), nn * sizeof(T), cudaMemcpyDeviceToHost, st));
+  if (J.out[0]) SWD_CUDA(cudaMemcpyAsync(J.out[0], J.d_seis_t.template as<T>() + nn, nn * sizeof(T), cudaMemcpyDeviceToHost, st));
+  if (J.a.snap) {
     for (int f = 0; f < 4; ++f) {
-      SWD_TRY(transpose<T, T>(d_snap.as<T>() + f * plane, 4 * plane, d_snap_t.as<T>(), plane, g.nrec, p.nz, p.nx, st));
-      SWD_CUDA(cudaMemcpyAsync(outs[f], d_snap_t.p, (size_t)g.nrec * plane * sizeof(T), cudaMemcpyDeviceToHost, st));
+      SWD_TRY(transpose<T, T>(J.d_snap.template as<T>() + f * plane, 4 * plane, J.d_snap_t.template as<T>(), plane, J.g.nrec, p.nz,
+                              p.nx, st));
+      SWD_CUDA(cudaMemcpyAsync(J.out[2 + f], J.d_snap_t.p, (size_t)J.g.nrec * plane * sizeof(T),
+                               cudaMemcpyDeviceToHost, st));
     }
   }
+  return SWD_OK;
+}
+
+template <typename T>
+int staggerfd_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, const T* cm, const T* cm1,
+                  const T* b, const T* b1, const T* s, T* seis_u, T* seis_w, T* fux, T* fuz, T* bwx, T* bwz) {
+  clear_error();
+  (void)cm;  // passed by the reference, unused by its kernel (cm1 carries mu)
+  cudaStream_t st = 0;
+  FwdJob<T> J;
+  SWD_TRY(fwd_job_setup(J, iv, n_iv, temp, ca, cl, cm1, b, b1, s, seis_u, seis_w, fux, fuz, bwx, bwz, st));
+  for (int it = 0; it < J.p.nt; ++it) {
+    J.a.in = J.bufs[it & 1];
+    J.a.out = J.bufs[(it + 1) & 1];
+    SWD_TRY(launch_fwd_step<T, 4>(J.a, it, st));  // a dispatch or geometry error ends the call
+  }
+  SWD_CUDA(cudaGetLastError());
+  SWD_TRY(fwd_job_finish(J, st));
   SWD_CUDA(cudaStreamSynchronize(st));
   return SWD_OK;
 }
@@ -669,6 +702,60 @@ int swd_staggerfd_single(const float* iv, int n_iv, const float* temp, const flo
                          const float* cm, const float* cm1, const float* b, const float* b1, const float* s,
                          float* seismo_u, float* seismo_w, float* fux, float* fuz, float* bwx, float* bwz) {
   return staggerfd_mex<float>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, s, seismo_u, seismo_w, fux, fuz, bwx, bwz);
+}
+int swd_staggerfd_single_batch(int n_jobs, const swd_staggerfd_job* jobs) {
+  clear_error();
+  SWD_CHECK(jobs && n_jobs >= 1, "a batch needs at least one job (got %d)", n_jobs);
+  cudaStream_t st = 0;
+  std::vector<std::unique_ptr<FwdJob<float>>> J;
+  std::vector<int> cta0(n_jobs + 1, 0);
+  int nt_max = 0;
+  for (int j = 0; j < n_jobs; ++j) {
+    const swd_staggerfd_job& q = jobs[j];
+    J.push_back(std::make_unique<FwdJob<float>>());
+    FwdJob<float>& w = *J.back();
+    const int rc = fwd_job_setup(w, q.iv, q.n_iv, q.temp, q.ca, q.cl, q.cm1, q.b, q.b1, q.s, q.seismo_u, q.seismo_w,
+                                 (float*)nullptr, (float*)nullptr, (float*)nullptr, (float*)nullptr, st);
+    if (rc != SWD_OK) {
+      set_error("job %d: %s", j, std::string(swd_last_error()).c_str());
+      return rc;
+    }
+    // the one kernel shape of the MEX-convention forward (launch_fwd_step with b, b1 arrays)
+    SWD_CHECK(w.g.sched == 0 && w.g.warps == 4 && w.g.cells == 1 && w.g.ring_fwd == 4,
+              "internal: batch job %d planned for another FD kernel", j);
+    const long blocks = (long)w.g.n_strips * w.g.n_chunks;
+    SWD_CHECK(cta0[j] + blocks < (1L << 31), "batch too large for one launch");
+    cta0[j + 1] = cta0[j] + (int)blocks;
+    nt_max = std::max(nt_max, w.p.nt);
+  }
+  // the jobs' arguments for even and odd steps (state buffers swapped) and their first tiles
+  std::vector<FwdArgs<float>> args(2 * (size_t)n_jobs);
+  for (int j = 0; j < n_jobs; ++j) {
+    args[j] = J[j]->a;
+    args[j].in = J[j]->bufs[0];
+    args[j].out = J[j]->bufs[1];
+    args[n_jobs + j] = J[j]->a;
+    args[n_jobs + j].in = J[j]->bufs[1];
+    args[n_jobs + j].out = J[j]->bufs[0];
+  }
+  DevBuf d_args, d_cta;
+  SWD_TRY(d_args.alloc(args.size() * sizeof(FwdArgs<float>)));
+  SWD_TRY(d_cta.alloc(cta0.size() * sizeof(int)));
+  SWD_CUDA(cudaMemcpyAsync(d_args.p, args.data(), args.size() * sizeof(FwdArgs<float>), cudaMemcpyHostToDevice, st));
+  SWD_CUDA(cudaMemcpyAsync(d_cta.p, cta0.data(), cta0.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  auto kernel = fd_fwd_smem_multi<float, 4, 4, 1, 4, true>;
+  constexpr size_t smem = smem_bytes<float, 4, 1, 4, true>();
+  static int ready = set_smem(kernel, smem);
+  SWD_TRY(ready);
+  const FwdArgs<float>* da = d_args.as<FwdArgs<float>>();
+  for (int it = 0; it < nt_max; ++it) {  // one launch per step for every job's tiles
+    kernel<<<(unsigned)cta0[n_jobs], 32 * 4, smem, st>>>(it & 1 ? da + n_jobs : da, d_cta.as<int>(), n_jobs, it);
+    count_launch(1);
+  }
+  SWD_CUDA(cudaGetLastError());
+  for (int j = 0; j < n_jobs; ++j) SWD_TRY(fwd_job_finish(*J[j], st));
+  SWD_CUDA(cudaStreamSynchronize(st));
+  return SWD_OK;
 }
 int swd_staggerfd_double(const double* iv, int n_iv, const double* temp, const double* ca, const double* cl,
                          const double* cm, const double* cm1, const double* b, const double* b1, const double* s,

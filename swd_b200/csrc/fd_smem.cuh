@@ -135,11 +135,11 @@ constexpr size_t smem_bytes() {
 
 // ---------------------------------------------------------------- forward
 
-// SNAP: this launch writes strain snapshots (it % nt_wf == 0); the other steps use
-// the variant without the snapshot code.
+// One tile (strip, row chunk, shot = `block` in that order) of a forward step.  SNAP: the step
+// writes strain snapshots (it % nt_wf == 0); the other steps use the variant without the
+// snapshot code.
 template <typename T, int NF, int W, int C, int D, bool GB, bool SNAP>
-__global__ void __launch_bounds__(32 * W)
-fd_fwd_smem(FwdArgs<T> a, int it) {
+__device__ __forceinline__ void fwd_smem_tile(const FwdArgs<T>& a, int it, int block) {
   if (cta_cancelled(a.cancel)) return;  // every thread of the CTA reaches this first
   static_assert(D >= 4 && D % 2 == 0, "rows k, k+1 in use, rows in flight, even depth for static slots");
   constexpr int NT = 32 * W;
@@ -152,8 +152,8 @@ fd_fwd_smem(FwdArgs<T> a, int it) {
   T* sw = su + 2 * kWin;                     // new ww of row k [kWin]
   const unsigned ring_addr = (unsigned)__cvta_generic_to_shared(ring);
   const FdGeom& g = a.g;
-  const int strip = blockIdx.x % g.n_strips;
-  const int rest = blockIdx.x / g.n_strips;
+  const int strip = block % g.n_strips;
+  const int rest = block / g.n_strips;
   const int chunk = rest % g.n_chunks;
   const int shot = rest / g.n_chunks;
   const int tid = threadIdx.x;
@@ -345,6 +345,27 @@ fd_fwd_smem(FwdArgs<T> a, int it) {
     }
   }
   cp_async_wait<0>();  // no copy may still target this CTA's shared memory at exit
+}
+
+template <typename T, int NF, int W, int C, int D, bool GB, bool SNAP>
+__global__ void __launch_bounds__(32 * W)
+fd_fwd_smem(FwdArgs<T> a, int it) {
+  fwd_smem_tile<T, NF, W, C, D, GB, SNAP>(a, it, blockIdx.x);
+}
+
+// Several forward calls advanced by one launch per step, on grids of any sizes: CTA b runs tile
+// b - cta0[j] of job j, where cta0 holds the running sums of the jobs' tile counts (cta0[0] = 0,
+// cta0[n_jobs] = the grid); a job whose time steps are done leaves at once.  The jobs share the
+// CTA shape, so one shared-memory size serves all of them; each reads its own geometry,
+// materials, state, source and receivers from its FwdArgs.  No snapshots.
+template <typename T, int NF, int W, int C, int D, bool GB>
+__global__ void __launch_bounds__(32 * W)
+fd_fwd_smem_multi(const FwdArgs<T>* __restrict__ jobs, const int* __restrict__ cta0, int n_jobs, int it) {
+  int j = 0;
+  while (j + 1 < n_jobs && (int)blockIdx.x >= cta0[j + 1]) ++j;
+  const FwdArgs<T>& a = jobs[j];
+  if (it >= a.g.nt) return;  // uniform over the CTA
+  fwd_smem_tile<T, NF, W, C, D, GB, false>(a, it, (int)blockIdx.x - cta0[j]);
 }
 
 // ---------------------------------------------------------------- adjoint

@@ -15,6 +15,8 @@ computation runs in libswd.so on the GPU.
 """
 from __future__ import annotations
 
+import ctypes
+
 import numpy as np
 
 from ._lib import call, ptr
@@ -24,6 +26,37 @@ _SRC = {"p": 1, "s": 2, "s1": 3, "z": 4, "w": 5}  # core/staggerfd_eigen.m:126-1
 
 def _f(a, dt):
     return np.asfortranarray(np.asarray(a, dt))
+
+
+class _FdJob(ctypes.Structure):
+    """swd_staggerfd_job of include/swd.h."""
+    _fields_ = [("iv", ctypes.c_void_p), ("n_iv", ctypes.c_int)] + \
+               [(k, ctypes.c_void_p) for k in ("temp", "ca", "cl", "cm", "cm1", "b", "b1", "s", "seismo_u",
+                                                "seismo_w")]
+
+
+def eigen_staggerfd_single_batch(jobs):
+    """Several eigen_staggerfd_single calls, on grids of any sizes, advanced together by one launch per
+    time step; it has no counterpart in the reference (one MEX call per shot and model).  jobs: a
+    list of (iv, temp, ca, cl, cm, cm1, b, b1, s) as for eigen_staggerfd_single.  Returns
+    [(seismo_u, seismo_w)], bit for bit those of the separate calls."""
+    keep, outs = [], []
+    arr = (_FdJob * len(jobs))()
+    for k, (iv, temp, ca, cl, cm, cm1, b, b1, s) in enumerate(jobs):
+        iv = np.ascontiguousarray(np.asarray(iv, np.float32).reshape(-1))
+        nt, ng = int(iv[0]), int(iv[4])
+        mats = [_f(a, np.float32) for a in (temp, ca, cl, cm, cm1, b, b1)]
+        s = np.ascontiguousarray(np.asarray(s, np.float32).reshape(-1))
+        if s.size < nt:
+            raise ValueError(f"job {k}: source wavelet has {s.size} samples, nt={nt}")
+        su = np.zeros((nt, ng), np.float32, order="F")
+        sw = np.zeros((nt, ng), np.float32, order="F")
+        keep += [iv, s, *mats]
+        outs.append((su, sw))
+        arr[k] = _FdJob(iv.ctypes.data, iv.size, *[m.ctypes.data for m in mats], s.ctypes.data, su.ctypes.data,
+                        sw.ctypes.data)
+    call("swd_staggerfd_single_batch", len(jobs), ctypes.cast(arr, ctypes.c_void_p))
+    return outs
 
 
 def _mex_fwd(fn, dt, iv, temp, ca, cl, cm, cm1, b, b1, s, want_wf=True):

@@ -1,0 +1,49 @@
+"""Several MEX-convention forward calls on grids of different sizes, advanced together by one
+launch per time step (swd_staggerfd_single_batch): every job's seismograms equal those of its own
+swd_staggerfd_single call bit for bit, and those equal the oracle's."""
+import dataclasses
+
+import numpy as np
+import pytest
+
+import swd_b200 as S
+from swd_b200 import configs
+from swd_b200.fd import eigen_staggerfd_single_batch
+
+pytestmark = pytest.mark.gpu
+
+
+def _job(O, s, is_, src="w"):
+    inp = O.fd_inputs(s.nbc, s.nt, s.dtx, s.dx, s.dt, int(s.sx[is_ - 1]), 1, s.gx, np.ones(s.ng), s.vp, s.vs,
+                      source_type=src, in_wf=s.nt_wf)
+    return inp, s.source()
+
+
+def test_batch_of_grids_matches_separate_calls_and_oracle(O):
+    tiny = configs.tiny(nt=400)
+    c1 = dataclasses.replace(configs.plain_c1(), nt=800)
+    cases = [(tiny, 2, "w"), (c1, 5, "w"), (tiny, 3, "p"), (c1, 11, "z")]  # different grids, nt, sources
+    jobs, refs = [], []
+    for s, is_, src in cases:
+        inp, w = _job(O, s, is_, src)
+        jobs.append((inp.iv, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w))
+        refs.append((inp, w))
+    got = eigen_staggerfd_single_batch(jobs)
+    for (inp, w), (su, sw), (s, is_, src) in zip(refs, got, cases):
+        one = S.eigen_staggerfd_single(inp.iv, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w,
+                                       want_wf=False)
+        assert np.abs(sw).max() > 0
+        assert np.array_equal(sw, one[1]) and np.array_equal(su, one[0]), (s.name, is_, src)
+        ref = O.mex_staggerfd(inp, w, want_wf=False)
+        assert np.array_equal(sw, ref[1]) and np.array_equal(su, ref[0]), (s.name, is_, src)
+
+
+def test_batch_rejects_a_bad_job_by_index(O):
+    from swd_b200._lib import SwdError
+    s = configs.tiny(nt=400)
+    inp, w = _job(O, s, 1)
+    bad = inp.iv.copy()
+    bad[11] = 24  # fd_order 24 is not supported
+    with pytest.raises(SwdError, match="job 1"):
+        eigen_staggerfd_single_batch([(inp.iv, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w),
+                                      (bad, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w)])
