@@ -59,6 +59,24 @@ def test_fk_filter_validates_before_touching_the_gpu():
         assert e.value.status == 1
 
 
+def test_staggerfd_batch_validates_before_touching_the_gpu():
+    import ctypes
+
+    import numpy as np
+    from swd_b200 import _lib
+    from swd_b200.fd import _FdJob
+    with pytest.raises(_lib.SwdError) as e:
+        _lib.call("swd_staggerfd_single_batch", 0, None)
+    assert e.value.status == 1
+    iv = np.zeros(16, np.float32)
+    iv[:] = [100, 10, 20, 1e-4, 5, 3, 5, 3, 3, 1, 5, 24, 5, 4, 10, 3]  # fd_order 24: unsupported
+    z = np.zeros(200, np.float32)
+    jobs = (_FdJob * 1)(_FdJob(iv.ctypes.data, 16, *[z.ctypes.data] * 10))
+    with pytest.raises(_lib.SwdError, match="job 0") as e:
+        _lib.call("swd_staggerfd_single_batch", 1, ctypes.cast(jobs, ctypes.c_void_p))
+    assert e.value.status == 2
+
+
 def test_engine_options_validate_before_touching_the_gpu():
     """Out-of-range engine options are reported as such, before any CUDA call."""
     import ctypes
