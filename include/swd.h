@@ -61,11 +61,11 @@ int swd_staggerfd_single(const float* iv, int n_iv, const float* temp, const flo
 
 /* Several eigen_staggerfd_single calls, on grids of any sizes, advanced together: one launch per
  * time step covers the tiles of every job (each CTA finds its job from the jobs' running tile
- * counts and reads that job's geometry, materials, state, source and receivers).  It has no
- * counterpart in the reference, where each shot and model is a separate MEX call
- * (core/staggerfd_eigen.m:138-140).  A job is one call's arguments as for
- * swd_staggerfd_single, without the wavefield outputs; its seismograms are the same, bit for bit.
- * Jobs may differ in grid, nt, source and receivers; a job with fewer steps idles after them. */
+ * counts and reads that job's geometry, materials, state, source, receivers and snapshot
+ * buffer).  It has no counterpart in the reference, where each shot and model is a separate MEX
+ * call (core/staggerfd_eigen.m:138-140).  A job is one call's arguments and outputs as for
+ * swd_staggerfd_single; its outputs are the same, bit for bit.  Jobs may differ in grid, nt,
+ * nt_wf, source and receivers; a job with fewer steps idles after them. */
 typedef struct {
   const float* iv;      /* input_vector (16 entries) */
   int n_iv;
@@ -73,6 +73,7 @@ typedef struct {
   const float* s;       /* wavelet, nt */
   float* seismo_u;      /* nt x ng, may be NULL */
   float* seismo_w;      /* nt x ng */
+  float *fux, *fuz, *bwx, *bwz; /* nz x nx x nt/nt_wf each, or all NULL */
 } swd_staggerfd_job;
 int swd_staggerfd_single_batch(int n_jobs, const swd_staggerfd_job* jobs);
 

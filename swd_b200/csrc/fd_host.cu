@@ -715,7 +715,7 @@ int swd_staggerfd_single_batch(int n_jobs, const swd_staggerfd_job* jobs) {
     J.push_back(std::make_unique<FwdJob<float>>());
     FwdJob<float>& w = *J.back();
     const int rc = fwd_job_setup(w, q.iv, q.n_iv, q.temp, q.ca, q.cl, q.cm1, q.b, q.b1, q.s, q.seismo_u, q.seismo_w,
-                                 (float*)nullptr, (float*)nullptr, (float*)nullptr, (float*)nullptr, st);
+                                 q.fux, q.fuz, q.bwx, q.bwz, st);
     if (rc != SWD_OK) {
       set_error("job %d: %s", j, std::string(swd_last_error()).c_str());
       return rc;

@@ -357,7 +357,8 @@ fd_fwd_smem(FwdArgs<T> a, int it) {
 // b - cta0[j] of job j, where cta0 holds the running sums of the jobs' tile counts (cta0[0] = 0,
 // cta0[n_jobs] = the grid); a job whose time steps are done leaves at once.  The jobs share the
 // CTA shape, so one shared-memory size serves all of them; each reads its own geometry,
-// materials, state, source and receivers from its FwdArgs.  No snapshots.
+// materials, state, source, receivers and snapshot buffer from its FwdArgs, and takes the
+// snapshot variant on its own snapshot steps (it % nt_wf == 0).
 template <typename T, int NF, int W, int C, int D, bool GB>
 __global__ void __launch_bounds__(32 * W)
 fd_fwd_smem_multi(const FwdArgs<T>* __restrict__ jobs, const int* __restrict__ cta0, int n_jobs, int it) {
@@ -365,7 +366,9 @@ fd_fwd_smem_multi(const FwdArgs<T>* __restrict__ jobs, const int* __restrict__ c
   while (j + 1 < n_jobs && (int)blockIdx.x >= cta0[j + 1]) ++j;
   const FwdArgs<T>& a = jobs[j];
   if (it >= a.g.nt) return;  // uniform over the CTA
-  fwd_smem_tile<T, NF, W, C, D, GB, false>(a, it, (int)blockIdx.x - cta0[j]);
+  const int tile = (int)blockIdx.x - cta0[j];
+  if (a.snap && it % a.g.nt_wf == 0) fwd_smem_tile<T, NF, W, C, D, GB, true>(a, it, tile);
+  else fwd_smem_tile<T, NF, W, C, D, GB, false>(a, it, tile);
 }
 
 // ---------------------------------------------------------------- adjoint

@@ -32,29 +32,32 @@ class _FdJob(ctypes.Structure):
     """swd_staggerfd_job of include/swd.h."""
     _fields_ = [("iv", ctypes.c_void_p), ("n_iv", ctypes.c_int)] + \
                [(k, ctypes.c_void_p) for k in ("temp", "ca", "cl", "cm", "cm1", "b", "b1", "s", "seismo_u",
-                                                "seismo_w")]
+                                                "seismo_w", "fux", "fuz", "bwx", "bwz")]
 
 
-def eigen_staggerfd_single_batch(jobs):
+def eigen_staggerfd_single_batch(jobs, want_wf=False):
     """Several eigen_staggerfd_single calls, on grids of any sizes, advanced together by one launch per
     time step; it has no counterpart in the reference (one MEX call per shot and model).  jobs: a
     list of (iv, temp, ca, cl, cm, cm1, b, b1, s) as for eigen_staggerfd_single.  Returns
-    [(seismo_u, seismo_w)], bit for bit those of the separate calls."""
+    [(seismo_u, seismo_w, www or None)], bit for bit those of the separate calls."""
     keep, outs = [], []
     arr = (_FdJob * len(jobs))()
     for k, (iv, temp, ca, cl, cm, cm1, b, b1, s) in enumerate(jobs):
         iv = np.ascontiguousarray(np.asarray(iv, np.float32).reshape(-1))
-        nt, ng = int(iv[0]), int(iv[4])
+        nt, ng, nz, nx, ntwf = int(iv[0]), int(iv[4]), int(iv[13]), int(iv[14]), int(iv[12])
         mats = [_f(a, np.float32) for a in (temp, ca, cl, cm, cm1, b, b1)]
         s = np.ascontiguousarray(np.asarray(s, np.float32).reshape(-1))
         if s.size < nt:
             raise ValueError(f"job {k}: source wavelet has {s.size} samples, nt={nt}")
         su = np.zeros((nt, ng), np.float32, order="F")
         sw = np.zeros((nt, ng), np.float32, order="F")
+        wf = ({f: np.zeros((nz, nx, nt // max(ntwf, 1)), np.float32, order="F") for f in ("fux", "fuz", "bwx", "bwz")}
+              if want_wf else None)
         keep += [iv, s, *mats]
-        outs.append((su, sw))
+        outs.append((su, sw, wf))
+        w = [wf[f].ctypes.data if wf else None for f in ("fux", "fuz", "bwx", "bwz")]
         arr[k] = _FdJob(iv.ctypes.data, iv.size, *[m.ctypes.data for m in mats], s.ctypes.data, su.ctypes.data,
-                        sw.ctypes.data)
+                        sw.ctypes.data, *w)
     call("swd_staggerfd_single_batch", len(jobs), ctypes.cast(arr, ctypes.c_void_p))
     return outs
 

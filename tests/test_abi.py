@@ -71,7 +71,7 @@ def test_staggerfd_batch_validates_before_touching_the_gpu():
     iv = np.zeros(16, np.float32)
     iv[:] = [100, 10, 20, 1e-4, 5, 3, 5, 3, 3, 1, 5, 24, 5, 4, 10, 3]  # fd_order 24: unsupported
     z = np.zeros(200, np.float32)
-    jobs = (_FdJob * 1)(_FdJob(iv.ctypes.data, 16, *[z.ctypes.data] * 10))
+    jobs = (_FdJob * 1)(_FdJob(iv.ctypes.data, 16, *[z.ctypes.data] * 10, None, None, None, None))
     with pytest.raises(_lib.SwdError, match="job 0") as e:
         _lib.call("swd_staggerfd_single_batch", 1, ctypes.cast(jobs, ctypes.c_void_p))
     assert e.value.status == 2

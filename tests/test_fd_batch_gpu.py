@@ -29,13 +29,30 @@ def test_batch_of_grids_matches_separate_calls_and_oracle(O):
         jobs.append((inp.iv, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w))
         refs.append((inp, w))
     got = eigen_staggerfd_single_batch(jobs)
-    for (inp, w), (su, sw), (s, is_, src) in zip(refs, got, cases):
+    for (inp, w), (su, sw, _), (s, is_, src) in zip(refs, got, cases):
         one = S.eigen_staggerfd_single(inp.iv, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w,
                                        want_wf=False)
         assert np.abs(sw).max() > 0
         assert np.array_equal(sw, one[1]) and np.array_equal(su, one[0]), (s.name, is_, src)
         ref = O.mex_staggerfd(inp, w, want_wf=False)
         assert np.array_equal(sw, ref[1]) and np.array_equal(su, ref[0]), (s.name, is_, src)
+
+
+def test_batch_wavefields_match_the_oracle(O):
+    """With the strain wavefields: each job takes the snapshot variant on its own nt_wf steps
+    (jobs with nt_wf 5 and 10 in one batch)."""
+    tiny = configs.tiny(nt=400)
+    c1 = dataclasses.replace(configs.plain_c1(), nt=800, nt_wf=10)
+    jobs, refs = [], []
+    for s, is_ in ((tiny, 1), (c1, 7)):
+        inp, w = _job(O, s, is_)
+        jobs.append((inp.iv, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w))
+        refs.append(O.mex_staggerfd(inp, w))
+    for (su, sw, wf), ref in zip(eigen_staggerfd_single_batch(jobs, want_wf=True), refs):
+        assert np.array_equal(sw, ref[1]) and np.array_equal(su, ref[0])
+        for k in ("fux", "fuz", "bwx", "bwz"):
+            assert np.abs(ref[2][k]).max() > 0
+            assert np.array_equal(wf[k], ref[2][k]), k
 
 
 def test_batch_rejects_a_bad_job_by_index(O):
