@@ -77,6 +77,21 @@ typedef struct {
 } swd_staggerfd_job;
 int swd_staggerfd_single_batch(int n_jobs, const swd_staggerfd_job* jobs);
 
+/* The adjoint counterpart: several eigen_e2drtm_single calls, on grids of any sizes, advanced
+ * together by one launch per time step; each job counts its steps back from its own nt
+ * (core/eigen_e2drtm_single.cpp:181) and images on its own nt_wf steps.  No counterpart in the
+ * reference.  A job is one call's arguments and outputs as for swd_e2drtm_single; its images
+ * are the same, bit for bit. */
+typedef struct {
+  const float* iv;      /* input_vector (14 entries) */
+  int n_iv;
+  const float *temp, *ca, *cl, *cm, *cm1, *b, *b1; /* nzbc x nxbc */
+  const float* seismo_w;                            /* adjoint source, nt x ng */
+  const float *fux, *fuz, *bwx, *bwz;               /* nz x nx x nt/nt_wf each */
+  float *cl_img, *cm_img, *illum_div;               /* nz x nx each */
+} swd_e2drtm_job;
+int swd_e2drtm_single_batch(int n_jobs, const swd_e2drtm_job* jobs);
+
 /* Replaces eigen_staggerfd_double (binary-only in the reference; interface at
  * core/staggerfd_eigend.m:139).  Same arguments in double precision. */
 int swd_staggerfd_double(const double* iv, int n_iv, const double* temp, const double* ca,

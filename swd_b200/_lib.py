@@ -38,6 +38,7 @@ _SIGS = {
     "swd_kernel_launches": [],
     "swd_staggerfd_single": [_f32p, _c_int] + [_f32p] * 14,
     "swd_staggerfd_single_batch": [_c_int, ctypes.c_void_p],
+    "swd_e2drtm_single_batch": [_c_int, ctypes.c_void_p],
     "swd_staggerfd_double": [_f64p, _c_int] + [_f64p] * 14,
     "swd_e2drtm_single": [_f32p, _c_int] + [_f32p] * 15,
     "swd_e2drtm_single_f64out": [_f32p, _c_int] + [_f32p] * 12 + [_f64p] * 3,

@@ -610,12 +610,28 @@ int staggerfd_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl
   return SWD_OK;
 }
 
+// The device side of one MEX-convention adjoint call: its buffers, arguments and host outputs.
 template <typename T, typename TO>
-int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, const T* cm, const T* cm1,
-               const T* b, const T* b1, const T* res, const T* fux, const T* fuz, const T* bwx, const T* bwz,
-               TO* cl_img, TO* cm_img, TO* illum) {
-  clear_error();
-  (void)cm;
+struct AdjJob {
+  int nt = 0;
+  size_t plane = 0;
+  FdGeom g{};
+  DevBuf d_in, d_m1, d_m2, d_state, d_res, d_snap, d_img, d_out;
+  AdjArgs<T> a{};
+  T* bufs[2] = {nullptr, nullptr};
+  TO* out[3] = {};  // host: cl_img, cm_img, illum
+  // single in, single out: the images accumulate in FP32, as the reference's single MEX
+  // accumulates them (core/eigen_e2drtm_single.cpp:274-279); otherwise in FP64
+  static constexpr bool f32img = std::is_same<T, float>::value && std::is_same<TO, float>::value;
+};
+
+// Validates the call, allocates and fills the job's device buffers on st: materials packed, the
+// residual [nt][ng] and the snapshots [nrec][f][nz][nx] transposed from MATLAB's layout, state
+// and images cleared; the time loop then sets a.in / a.out from bufs.
+template <typename T, typename TO>
+int adj_job_setup(AdjJob<T, TO>& J, const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, const T* cm1,
+                  const T* b, const T* b1, const T* res, const T* fux, const T* fuz, const T* bwx, const T* bwz,
+                  TO* cl_img, TO* cm_img, TO* illum, cudaStream_t st) {
   SWD_CHECK(iv != nullptr && n_iv >= 14, "input_vector needs 14 entries (got %d)", n_iv);
   // core/eigen_e2drtm_single.cpp:69-84
   const int nt = (int)iv[0], NZ = (int)iv[1], NX = (int)iv[2], ng = (int)iv[4], nbc = (int)iv[5];
@@ -625,64 +641,84 @@ int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, c
   SWD_TRY(validate_geom(nt, NZ, NX, nz, nx, nbc, nt_wf, fd_order, ng, gz, gx, dg));
   SWD_CHECK(temp && ca && cl && cm1 && b && b1 && res && fux && fuz && bwx && bwz && cl_img && cm_img && illum,
             "null input/output pointer");
-  FdGeom g{};
+  FdGeom& g = J.g;
   fill_geom<T>(g, NZ, NX, nz, nx, nbc, nt, nt_wf, ng, gz, gx, dg);
   plan_decomposition(g, 1, 0);
   using V = typename Vec4<T>::type;
   using V2 = typename Vec2<T>::type;
   const size_t NN = (size_t)NZ * NX, plane = (size_t)nz * nx, nsnap = (size_t)g.nrec * plane;
-  DevBuf d_in, d_m1, d_m2, d_state, d_res, d_snap, d_img, d_out;
-  SWD_TRY(d_in.alloc(std::max(6 * NN, nsnap) * sizeof(T) + (size_t)nt * ng * sizeof(T)));
-  SWD_TRY(d_m1.alloc(g.field * sizeof(V)));
-  SWD_TRY(d_m2.alloc(g.field * sizeof(V2)));
-  SWD_TRY(d_state.alloc(2 * 5 * g.field * sizeof(T)));
-  SWD_TRY(d_res.alloc((size_t)nt * ng * sizeof(T)));
-  SWD_TRY(d_snap.alloc(4 * nsnap * sizeof(T)));
-  SWD_TRY(d_img.alloc(3 * plane * sizeof(double)));
-  SWD_TRY(d_out.alloc(3 * plane * sizeof(TO)));
-  cudaStream_t st = 0;
-  T* din = d_in.as<T>();
+  J.nt = nt;
+  J.plane = plane;
+  SWD_TRY(J.d_in.alloc(std::max(6 * NN, nsnap) * sizeof(T) + (size_t)nt * ng * sizeof(T)));
+  SWD_TRY(J.d_m1.alloc(g.field * sizeof(V)));
+  SWD_TRY(J.d_m2.alloc(g.field * sizeof(V2)));
+  SWD_TRY(J.d_state.alloc(2 * 5 * g.field * sizeof(T)));
+  SWD_TRY(J.d_res.alloc((size_t)nt * ng * sizeof(T)));
+  SWD_TRY(J.d_snap.alloc(4 * nsnap * sizeof(T)));
+  SWD_TRY(J.d_img.alloc(3 * plane * sizeof(double)));
+  SWD_TRY(J.d_out.alloc(3 * plane * sizeof(TO)));
+  T* din = J.d_in.template as<T>();
   T* dstage = din + std::max(6 * NN, nsnap);
   const T* hsrc[6] = {temp, b, b1, ca, cl, cm1};
   for (int i = 0; i < 6; ++i) SWD_CUDA(cudaMemcpyAsync(din + i * NN, hsrc[i], NN * sizeof(T), cudaMemcpyHostToDevice, st));
-  SWD_TRY(pack_materials<T>(din, din + NN, din + 2 * NN, din + 3 * NN, din + 4 * NN, din + 5 * NN, d_m1.as<V>(),
-                            d_m2.as<V2>(), NZ, NX, g.pitch, st));
+  SWD_TRY(pack_materials<T>(din, din + NN, din + 2 * NN, din + 3 * NN, din + 4 * NN, din + 5 * NN,
+                            J.d_m1.template as<V>(), J.d_m2.template as<V2>(), NZ, NX, g.pitch, st));
   // residual: MATLAB nt x ng -> [nt][ng]
   SWD_CUDA(cudaMemcpyAsync(dstage, res, (size_t)nt * ng * sizeof(T), cudaMemcpyHostToDevice, st));
-  SWD_TRY(transpose<T, T>(dstage, 0, d_res.as<T>(), 0, 1, ng, nt, st));
+  SWD_TRY(transpose<T, T>(dstage, 0, J.d_res.template as<T>(), 0, 1, ng, nt, st));
   // snapshots: MATLAB nz x nx x nrec per field -> [nrec][f][nz][nx]
   const T* wf[4] = {fux, fuz, bwx, bwz};
   for (int f = 0; f < 4; ++f) {
     SWD_CUDA(cudaMemcpyAsync(din, wf[f], nsnap * sizeof(T), cudaMemcpyHostToDevice, st));
-    SWD_TRY(transpose<T, T>(din, plane, d_snap.as<T>() + f * plane, 4 * plane, g.nrec, nx, nz, st));
+    SWD_TRY(transpose<T, T>(din, plane, J.d_snap.template as<T>() + f * plane, 4 * plane, g.nrec, nx, nz, st));
   }
-  SWD_CUDA(cudaMemsetAsync(d_state.p, 0, d_state.bytes, st));
-  SWD_CUDA(cudaMemsetAsync(d_img.p, 0, d_img.bytes, st));
-  AdjArgs<T> a{};
-  a.g = g; a.mat = d_m1.as<V>(); a.mb = d_m2.as<V2>();
-  a.res = d_res.as<T>(); a.snap = d_snap.as<T>(); a.img = d_img.as<double>();
-  // single in, single out: the images accumulate in FP32, as the reference's single MEX
-  // accumulates them (core/eigen_e2drtm_single.cpp:274-279); otherwise in FP64
-  constexpr bool f32img = std::is_same<T, float>::value && std::is_same<TO, float>::value;
-  if (f32img) a.img32 = d_img.as<float>();
+  SWD_CUDA(cudaMemsetAsync(J.d_state.p, 0, J.d_state.bytes, st));
+  SWD_CUDA(cudaMemsetAsync(J.d_img.p, 0, J.d_img.bytes, st));
+  AdjArgs<T>& a = J.a;
+  a.g = g; a.mat = J.d_m1.template as<V>(); a.mb = J.d_m2.template as<V2>();
+  a.res = J.d_res.template as<T>(); a.snap = J.d_snap.template as<T>(); a.img = J.d_img.template as<double>();
+  if (AdjJob<T, TO>::f32img) a.img32 = J.d_img.template as<float>();
   a.dtx = dtx; a.dt = dt; a.n_shots = 1;
-  T* bufs[2] = {d_state.as<T>(), d_state.as<T>() + 5 * g.field};
+  J.bufs[0] = J.d_state.template as<T>();
+  J.bufs[1] = J.d_state.template as<T>() + 5 * g.field;
+  J.out[0] = cl_img; J.out[1] = cm_img; J.out[2] = illum;
+  return SWD_OK;
+}
+
+// Enqueues the job's images on st: [3][nz][nx] -> MATLAB nz x nx each, in the output type.
+template <typename T, typename TO>
+int adj_job_finish(AdjJob<T, TO>& J, cudaStream_t st) {
+  const size_t plane = J.plane;
+  if constexpr (AdjJob<T, TO>::f32img)
+    SWD_TRY(transpose<float, float>(J.d_img.template as<float>(), plane, J.d_out.template as<float>(), plane, 3,
+                                    J.g.nz, J.g.nx, st));
+  else
+    SWD_TRY(transpose<double, TO>(J.d_img.template as<double>(), plane, J.d_out.template as<TO>(), plane, 3, J.g.nz,
+                                  J.g.nx, st));
+  for (int i = 0; i < 3; ++i)
+    SWD_CUDA(cudaMemcpyAsync(J.out[i], J.d_out.template as<TO>() + i * plane, plane * sizeof(TO),
+                             cudaMemcpyDeviceToHost, st));
+  return SWD_OK;
+}
+
+template <typename T, typename TO>
+int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, const T* cm, const T* cm1,
+               const T* b, const T* b1, const T* res, const T* fux, const T* fuz, const T* bwx, const T* bwz,
+               TO* cl_img, TO* cm_img, TO* illum) {
+  clear_error();
+  (void)cm;
+  cudaStream_t st = 0;
+  AdjJob<T, TO> J;
+  SWD_TRY(adj_job_setup(J, iv, n_iv, temp, ca, cl, cm1, b, b1, res, fux, fuz, bwx, bwz, cl_img, cm_img, illum, st));
   int cur = 0;
-  for (int it = nt - 2; it >= 0; --it) {  // core/eigen_e2drtm_single.cpp:181
-    a.in = bufs[cur];
-    a.out = bufs[cur ^ 1];
-    SWD_TRY(launch_adj_step<T, 4>(a, it, st));
+  for (int it = J.nt - 2; it >= 0; --it) {  // core/eigen_e2drtm_single.cpp:181
+    J.a.in = J.bufs[cur];
+    J.a.out = J.bufs[cur ^ 1];
+    SWD_TRY(launch_adj_step<T, 4>(J.a, it, st));
     cur ^= 1;
   }
   SWD_CUDA(cudaGetLastError());
-  // images [3][nz][nx] -> MATLAB nz x nx each, in the output type
-  if constexpr (f32img)
-    SWD_TRY(transpose<float, float>(d_img.as<float>(), plane, d_out.as<float>(), plane, 3, nz, nx, st));
-  else
-    SWD_TRY(transpose<double, TO>(d_img.as<double>(), plane, d_out.as<TO>(), plane, 3, nz, nx, st));
-  TO* outs[3] = {cl_img, cm_img, illum};
-  for (int i = 0; i < 3; ++i)
-    SWD_CUDA(cudaMemcpyAsync(outs[i], d_out.as<TO>() + i * plane, plane * sizeof(TO), cudaMemcpyDeviceToHost, st));
+  SWD_TRY(adj_job_finish(J, st));
   SWD_CUDA(cudaStreamSynchronize(st));
   return SWD_OK;
 }
@@ -762,6 +798,60 @@ int swd_staggerfd_double(const double* iv, int n_iv, const double* temp, const d
                          double* seismo_u, double* seismo_w, double* fux, double* fuz, double* bwx,
                          double* bwz) {
   return staggerfd_mex<double>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, s, seismo_u, seismo_w, fux, fuz, bwx, bwz);
+}
+int swd_e2drtm_single_batch(int n_jobs, const swd_e2drtm_job* jobs) {
+  clear_error();
+  SWD_CHECK(jobs && n_jobs >= 1, "a batch needs at least one job (got %d)", n_jobs);
+  cudaStream_t st = 0;
+  std::vector<std::unique_ptr<AdjJob<float, float>>> J;
+  std::vector<int> cta0(n_jobs + 1, 0);
+  int steps = 0;
+  for (int j = 0; j < n_jobs; ++j) {
+    const swd_e2drtm_job& q = jobs[j];
+    J.push_back(std::make_unique<AdjJob<float, float>>());
+    AdjJob<float, float>& w = *J.back();
+    const int rc = adj_job_setup(w, q.iv, q.n_iv, q.temp, q.ca, q.cl, q.cm1, q.b, q.b1, q.seismo_w, q.fux, q.fuz, q.bwx,
+                                 q.bwz, q.cl_img, q.cm_img, q.illum_div, st);
+    if (rc != SWD_OK) {
+      set_error("job %d: %s", j, std::string(swd_last_error()).c_str());
+      return rc;
+    }
+    // the one kernel shape of the MEX-convention adjoint (launch_adj_step with b, b1 arrays)
+    SWD_CHECK(w.g.sched == 0 && w.g.warps == 4 && w.g.cells == 1 && w.g.ring_adj == 4,
+              "internal: batch job %d planned for another FD kernel", j);
+    const long blocks = (long)w.g.n_strips * w.g.n_chunks;
+    SWD_CHECK(cta0[j] + blocks < (1L << 31), "batch too large for one launch");
+    cta0[j + 1] = cta0[j] + (int)blocks;
+    steps = std::max(steps, w.nt - 1);  // it = nt-2 .. 0
+  }
+  // the jobs' arguments for even and odd steps (state buffers swapped) and their first tiles
+  std::vector<AdjArgs<float>> args(2 * (size_t)n_jobs);
+  for (int j = 0; j < n_jobs; ++j) {
+    args[j] = J[j]->a;
+    args[j].in = J[j]->bufs[0];
+    args[j].out = J[j]->bufs[1];
+    args[n_jobs + j] = J[j]->a;
+    args[n_jobs + j].in = J[j]->bufs[1];
+    args[n_jobs + j].out = J[j]->bufs[0];
+  }
+  DevBuf d_args, d_cta;
+  SWD_TRY(d_args.alloc(args.size() * sizeof(AdjArgs<float>)));
+  SWD_TRY(d_cta.alloc(cta0.size() * sizeof(int)));
+  SWD_CUDA(cudaMemcpyAsync(d_args.p, args.data(), args.size() * sizeof(AdjArgs<float>), cudaMemcpyHostToDevice, st));
+  SWD_CUDA(cudaMemcpyAsync(d_cta.p, cta0.data(), cta0.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+  auto kernel = fd_adj_smem_multi<float, 4, 4, 1, 4, true>;
+  constexpr size_t smem = smem_bytes<float, 4, 1, 4, true>();
+  static int ready = set_smem(kernel, smem);
+  SWD_TRY(ready);
+  const AdjArgs<float>* da = d_args.as<AdjArgs<float>>();
+  for (int step = 0; step < steps; ++step) {  // one launch per step for every job's tiles
+    kernel<<<(unsigned)cta0[n_jobs], 32 * 4, smem, st>>>(step & 1 ? da + n_jobs : da, d_cta.as<int>(), n_jobs, step);
+    count_launch(1);
+  }
+  SWD_CUDA(cudaGetLastError());
+  for (int j = 0; j < n_jobs; ++j) SWD_TRY(adj_job_finish(*J[j], st));
+  SWD_CUDA(cudaStreamSynchronize(st));
+  return SWD_OK;
 }
 int swd_e2drtm_single(const float* iv, int n_iv, const float* temp, const float* ca, const float* cl,
                       const float* cm, const float* cm1, const float* b, const float* b1, const float* seismo_w,

@@ -391,9 +391,10 @@ __device__ __forceinline__ T adj_vel_w(bool inner, T ww, T Q1d, T Q1, T Q2d, T Q
   return ww;
 }
 
+// One tile (strip, row chunk, shot = `block` in that order) of an adjoint step.  IMG: the step
+// applies the imaging condition (it % nt_wf == 0).
 template <typename T, int NF, int W, int C, int D, bool GB, bool IMG>
-__global__ void __launch_bounds__(32 * W)
-fd_adj_smem(AdjArgs<T> a, int it) {
+__device__ __forceinline__ void adj_smem_tile(const AdjArgs<T>& a, int it, int block) {
   if (cta_cancelled(a.cancel)) return;  // every thread of the CTA reaches this first
   static_assert(D >= 4 && D % 2 == 0, "rows k, k+1 in use, rows in flight, even depth for static slots");
   constexpr int NT = 32 * W;
@@ -405,8 +406,8 @@ fd_adj_smem(AdjArgs<T> a, int it) {
   T* sw = su + 2 * kWin;                     // new ww of row k [kWin]
   const unsigned ring_addr = (unsigned)__cvta_generic_to_shared(ring);
   const FdGeom& g = a.g;
-  const int strip = blockIdx.x % g.n_strips;
-  const int rest = blockIdx.x / g.n_strips;
+  const int strip = block % g.n_strips;
+  const int rest = block / g.n_strips;
   const int chunk = rest % g.n_chunks;
   const int shot = rest / g.n_chunks;
   const int tid = threadIdx.x;
@@ -576,6 +577,29 @@ fd_adj_smem(AdjArgs<T> a, int it) {
     }
   }
   cp_async_wait<0>();
+}
+
+template <typename T, int NF, int W, int C, int D, bool GB, bool IMG>
+__global__ void __launch_bounds__(32 * W)
+fd_adj_smem(AdjArgs<T> a, int it) {
+  adj_smem_tile<T, NF, W, C, D, GB, IMG>(a, it, blockIdx.x);
+}
+
+// Several adjoint calls advanced by one launch per step, as fd_fwd_smem_multi: the jobs count
+// their steps backwards from their own nt (step s of job j is it = nt_j - 2 - s, as
+// core/eigen_e2drtm_single.cpp:181 counts), a job whose steps are done leaves at once, and each
+// takes the imaging variant on its own it % nt_wf == 0 steps.
+template <typename T, int NF, int W, int C, int D, bool GB>
+__global__ void __launch_bounds__(32 * W)
+fd_adj_smem_multi(const AdjArgs<T>* __restrict__ jobs, const int* __restrict__ cta0, int n_jobs, int step) {
+  int j = 0;
+  while (j + 1 < n_jobs && (int)blockIdx.x >= cta0[j + 1]) ++j;
+  const AdjArgs<T>& a = jobs[j];
+  const int it = a.g.nt - 2 - step;
+  if (it < 0) return;  // uniform over the CTA
+  const int tile = (int)blockIdx.x - cta0[j];
+  if (it % a.g.nt_wf == 0) adj_smem_tile<T, NF, W, C, D, GB, true>(a, it, tile);
+  else adj_smem_tile<T, NF, W, C, D, GB, false>(a, it, tile);
 }
 
 }  // namespace swd

@@ -62,6 +62,32 @@ def eigen_staggerfd_single_batch(jobs, want_wf=False):
     return outs
 
 
+class _AdjJob(ctypes.Structure):
+    """swd_e2drtm_job of include/swd.h."""
+    _fields_ = [("iv", ctypes.c_void_p), ("n_iv", ctypes.c_int)] + \
+               [(k, ctypes.c_void_p) for k in ("temp", "ca", "cl", "cm", "cm1", "b", "b1", "seismo_w", "fux", "fuz",
+                                                "bwx", "bwz", "cl_img", "cm_img", "illum_div")]
+
+
+def eigen_e2drtm_single_batch(jobs):
+    """Several eigen_e2drtm_single calls, on grids of any sizes, advanced together by one launch per
+    time step (no counterpart in the reference).  jobs: a list of (iv, temp, ca, cl, cm, cm1, b, b1,
+    seismo_w, fux, fuz, bwx, bwz) as for eigen_e2drtm_single.  Returns [(cl_img, cm_img, illum_div)],
+    FP32 as the single MEX, bit for bit those of the separate calls."""
+    keep, outs = [], []
+    arr = (_AdjJob * len(jobs))()
+    for k, job in enumerate(jobs):
+        iv = np.ascontiguousarray(np.asarray(job[0], np.float32).reshape(-1))
+        nz, nx = int(iv[11]), int(iv[12])
+        ins = [_f(a, np.float32) for a in job[1:]]
+        img = [np.zeros((nz, nx), np.float32, order="F") for _ in range(3)]
+        keep += [iv, *ins]
+        outs.append(tuple(img))
+        arr[k] = _AdjJob(iv.ctypes.data, iv.size, *[a.ctypes.data for a in ins], *[o.ctypes.data for o in img])
+    call("swd_e2drtm_single_batch", len(jobs), ctypes.cast(arr, ctypes.c_void_p))
+    return outs
+
+
 def _mex_fwd(fn, dt, iv, temp, ca, cl, cm, cm1, b, b1, s, want_wf=True):
     iv = np.ascontiguousarray(np.asarray(iv, dt).reshape(-1))
     nt, ng, nz, nx, ntwf = int(iv[0]), int(iv[4]), int(iv[13]), int(iv[14]), int(iv[12])

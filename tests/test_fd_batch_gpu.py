@@ -1,6 +1,6 @@
-"""Several MEX-convention forward calls on grids of different sizes, advanced together by one
-launch per time step (swd_staggerfd_single_batch): every job's seismograms equal those of its own
-swd_staggerfd_single call bit for bit, and those equal the oracle's."""
+"""Several MEX-convention forward (swd_staggerfd_single_batch) or adjoint (swd_e2drtm_single_batch)
+calls on grids of different sizes, advanced together by one launch per time step: every job's
+outputs equal those of its own single call bit for bit, and those equal the oracle's."""
 import dataclasses
 
 import numpy as np
@@ -8,7 +8,7 @@ import pytest
 
 import swd_b200 as S
 from swd_b200 import configs
-from swd_b200.fd import eigen_staggerfd_single_batch
+from swd_b200.fd import eigen_e2drtm_single_batch, eigen_staggerfd_single_batch
 
 pytestmark = pytest.mark.gpu
 
@@ -64,3 +64,25 @@ def test_batch_rejects_a_bad_job_by_index(O):
     with pytest.raises(SwdError, match="job 1"):
         eigen_staggerfd_single_batch([(inp.iv, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w),
                                       (bad, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w)])
+
+
+def test_adjoint_batch_matches_separate_calls_and_oracle(O):
+    """Jobs with different grids, nt and nt_wf: each counts its steps back from its own nt and
+    images on its own nt_wf steps; FP32 images as the single MEX accumulates them."""
+    tiny = configs.tiny(nt=400)
+    c1 = dataclasses.replace(configs.plain_c1(), nt=800, nt_wf=10)
+    jobs, refs = [], []
+    for s, is_ in ((tiny, 2), (c1, 4), (tiny, 3)):
+        inp, w = _job(O, s, is_)
+        _, sw, wf = O.mex_staggerfd(inp, w)
+        res = np.asfortranarray(sw * 0.5)
+        ai = O.fd_inputs(s.nbc, s.nt, s.dtx, s.dx, s.dt, int(s.sx[is_ - 1]), 1, s.gx, np.ones(s.ng), s.vp, s.vs,
+                         in_wf=s.nt_wf, adjoint=True)
+        args = (ai.iv, ai.temp, ai.ca, ai.cl, ai.cm, ai.cm1, ai.b, ai.b1, res, wf["fux"], wf["fuz"], wf["bwx"],
+                wf["bwz"])
+        jobs.append(args)
+        refs.append((S.eigen_e2drtm_single(*args), O.mex_e2drtm(ai, res, wf, accum_fp64=False)))
+    for got, (one, ref) in zip(eigen_e2drtm_single_batch(jobs), refs):
+        for g, a, r in zip(got, one, ref):
+            assert np.abs(r).max() > 0
+            assert np.array_equal(g, a) and np.array_equal(g, r)
