@@ -168,18 +168,28 @@ def _geometry(nbc, pad_top, gx, gz):
     return gx.size, gz[0] + pad_top, gx[0] + nbc, gx[1] - gx[0]
 
 
-def _staggerfd(single, is_, nbc, nt, dtx, dx, dt, sx, sz, gx, gz, s, vp, vs, isfs, fd_order, source_type,
-               parameter_type, in_wf):
+def staggerfd_mex_args(nbc, nt, dtx, dx, dt, sx, sz, gx, gz, vp, vs, isfs, fd_order, source_type, parameter_type,
+                       in_wf, single=True, m=None):
+    """The MEX arguments (iv, temp, ca, cl, cm, cm1, b, b1) that core/staggerfd_eigen.m:37-138
+    builds; m: prep_model's output when the caller already has it (the same for every shot)."""
     if parameter_type != 0:
         raise ValueError("parameter_type=1 reads undefined cl/cm in core/staggerfd_eigen.m:43-45")
-    m = prep_model(nbc, dtx, dx, dt, vp, vs, isfs, fd_order, single)
+    if m is None:
+        m = prep_model(nbc, dtx, dx, dt, vp, vs, isfs, fd_order, single)
     nz, nx = np.asarray(vs).shape
     NZ, NX = m["temp"].shape
     ng, gz0, gx0, dg = _geometry(nbc, m["pad_top"], gx, gz)
     iv = [nt, NZ, NX, dtx, ng, float(sz) + m["pad_top"], float(sx) + nbc, gz0, gx0, dg, _SRC[source_type], fd_order,
           in_wf, nz, nx, 3]  # core/staggerfd_eigen.m:138
+    return (iv, m["temp"], m["ca"], m["cl"], m["cm"], m["cm1"], m["b"], m["b1"])
+
+
+def _staggerfd(single, is_, nbc, nt, dtx, dx, dt, sx, sz, gx, gz, s, vp, vs, isfs, fd_order, source_type,
+               parameter_type, in_wf):
+    args = staggerfd_mex_args(nbc, nt, dtx, dx, dt, sx, sz, gx, gz, vp, vs, isfs, fd_order, source_type,
+                              parameter_type, in_wf, single)
     fn = eigen_staggerfd_single if single else eigen_staggerfd_double
-    return fn(iv, m["temp"], m["ca"], m["cl"], m["cm"], m["cm1"], m["b"], m["b1"], s)
+    return fn(*args, s)
 
 
 def staggerfd_eigen(is_, nbc, nt, dtx, dx, dt, sx, sz, gx, gz, s, vp, vs, isfs=1, fd_order=22, source_type="w",
@@ -207,18 +217,27 @@ def staggerfd_eigen_field(is_, nbc, nt, dtx, dx, dt, sx, sz, gx, gz, s, vp, vs, 
                       parameter_type, in_wf)
 
 
-def _e2drtm(single, wavefield_gradient, seismo_w, is_, nbc, nt, dtx, dx, dt, gx, gz, s, vp, vs, isfs, fd_order,
-            parameter_type, in_wf, fp64_out=False):
+def e2drtm_mex_args(wavefield_gradient, seismo_w, nbc, nt, dtx, dx, dt, gx, gz, vp, vs, isfs, fd_order,
+                    parameter_type, in_wf, single=True, m=None):
+    """The MEX arguments (iv, temp, ca, cl, cm, cm1, b, b1, seismo_w, fux, fuz, bwx, bwz) that
+    core/e2drtm_eigen.m:44-122 builds; m as in staggerfd_mex_args."""
     if parameter_type != 0:
         raise ValueError("parameter_type=1 reads undefined cl/cm in core/e2drtm_eigen.m:49-51")
-    m = prep_model(nbc, dtx, dx, dt, vp, vs, isfs, fd_order, single)
+    if m is None:
+        m = prep_model(nbc, dtx, dx, dt, vp, vs, isfs, fd_order, single)
     nz, nx = np.asarray(vs).shape
     NZ, NX = m["temp"].shape
     ng, gz0, gx0, dg = _geometry(nbc, m["pad_top"], gx, gz)
     iv = [nt, NZ, NX, dtx, ng, nbc, gz0, gx0, dg, fd_order, in_wf, nz, nx, dt]  # core/e2drtm_eigen.m:121
     wg = wavefield_gradient
-    args = (iv, m["temp"], m["ca"], m["cl"], m["cm"], m["cm1"], m["b"], m["b1"], seismo_w, wg["fux"], wg["fuz"],
+    return (iv, m["temp"], m["ca"], m["cl"], m["cm"], m["cm1"], m["b"], m["b1"], seismo_w, wg["fux"], wg["fuz"],
             wg["bwx"], wg["bwz"])
+
+
+def _e2drtm(single, wavefield_gradient, seismo_w, is_, nbc, nt, dtx, dx, dt, gx, gz, s, vp, vs, isfs, fd_order,
+            parameter_type, in_wf, fp64_out=False):
+    args = e2drtm_mex_args(wavefield_gradient, seismo_w, nbc, nt, dtx, dx, dt, gx, gz, vp, vs, isfs, fd_order,
+                           parameter_type, in_wf, single)
     if single:
         return eigen_e2drtm_single(*args, fp64_out=fp64_out)
     return eigen_e2drtm_double(*args)

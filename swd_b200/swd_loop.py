@@ -88,11 +88,9 @@ def spectra(s, seismo, is_, FK=0):
     return out
 
 
-def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True, field=0, FK=0):
-    """SWD.m:172-193 for shot is_ (1-based in s): images cl, cm, illum plus picks and misfits
-    (field 1 / 2: the field-data flow, see the module docstring; FK=1: the gathers f-k filtered
-    before the transform, QademahSWD3.m:119)."""
-    sw, www = _seismogram(s, is_, vs, single)
+def _shot_adjoint_source(s, is_, sw, cr0_r, cr0_l, single, field, FK):
+    """SWD.m:174-193 for shot is_ from its predicted gather sw: spectra, picks, misfits and the
+    adjoint source (FP32 on the single path, SWD_single.m:193)."""
     if field:
         # outcrop.m:174; on single data MATLAB divides in single (the FP64 quotient rounded to
         # FP32 is that same single quotient)
@@ -119,8 +117,16 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True, field=0, FK=0):
     adj = ADWDgrad_1_maxnorm if field else ADWDgrad_1
     a = adj(s.nt, s.ng, ns, npair, shot_no, s.w, s.m, s.M, s.soft_arg_norm, gr, gl, space,
             sp["r"][2] if "r" in sp else None, sp["l"][2] if "l" in sp else None)
+    return out, (a.astype(np.float32) if single else a)
+
+
+def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True, field=0, FK=0):
+    """SWD.m:172-193 for shot is_ (1-based in s): images cl, cm, illum plus picks and misfits
+    (field 1 / 2: the field-data flow, see the module docstring; FK=1: the gathers f-k filtered
+    before the transform, QademahSWD3.m:119)."""
+    sw, www = _seismogram(s, is_, vs, single)
+    out, a = _shot_adjoint_source(s, is_, sw, cr0_r, cr0_l, single, field, FK)
     if single:
-        a = a.astype(np.float32)  # SWD_single.m:193
         cl, cm, il = e2drtm_eigen(www, a, is_, s.nbc, s.nt, s.dtx, s.dx, s.dt, s.gx, np.ones(s.ng), s.source(),
                                   s.vp_ratio * vs, vs, s.isfs, s.fd_order, 0, s.nt_wf)
     else:
@@ -130,25 +136,56 @@ def shot_gradient(s, is_, vs, cr0_r, cr0_l, single=True, field=0, FK=0):
     return out
 
 
-def gradient(s, vs, cr0_r, cr0_l, single=True, keep_shots=False, field=0, FK=0):
-    """SWD.m:171-201: shot sums in shot order (FP64), Vs gradient, smoothing, misfit."""
+def _assemble(s, vs, per, keep_shots):
+    """SWD.m:188-201 from the per-shot results in shot order: FP64 shot sums, the Vs gradient,
+    smoothing and the misfit."""
     g = {k: np.zeros((s.nz, s.nx)) for k in ("cl", "cm", "il")}
-    res_r, res_l, crp_r, crp_l, per = [], [], [], [], []
-    for is_ in range(1, s.ns + 1):
-        p = shot_gradient(s, is_, vs, cr0_r, cr0_l, single, field, FK)
+    for p in per:
         for k in g:
             g[k] = g[k] + p[k]
-        res_r.append(p["res_r"])
-        res_l.append(p["res_l"])
-        crp_r.append(p["crp_r"])
-        crp_l.append(p["crp_l"])
-        if keep_shots:
-            per.append(p)
     dk = -4 * vs * (g["cl"] / g["il"]) + 2 * vs * (g["cm"] / g["il"])  # SWD.m:199-200
-    res_r = np.array(res_r)
+    res_r = np.array([p["res_r"] for p in per])
     out = {"g_cl": g["cl"], "g_cm": g["cm"], "g_illum": g["il"], "dk_vs": smooth2a(dk, s.smooth_z, s.smooth_x),
-           "res_r": res_r, "res_l": np.array(res_l), "cr_pre_r": np.stack(crp_r, 1), "cr_pre_l": np.stack(crp_l, 1),
+           "res_r": res_r, "res_l": np.array([p["res_l"] for p in per]),
+           "cr_pre_r": np.stack([p["crp_r"] for p in per], 1), "cr_pre_l": np.stack([p["crp_l"] for p in per], 1),
            "residual": float(np.nanmean(res_r)) if np.any(~np.isnan(res_r)) else float("nan")}
     if keep_shots:
         out["per_shot"] = per
     return out
+
+
+def gradient_many(cases, field=0, FK=0):
+    """SWD_single.m:171-201 for several surveys at once, on grids of any sizes: the forward of every
+    shot of every survey runs as one batch (swd_staggerfd_single_batch: one launch per time step
+    for all of them), the spectra, picks and adjoint sources per shot, then the adjoint of every
+    shot as one batch (swd_e2drtm_single_batch).  cases: [(s, vs, cr0_r, cr0_l)].  Returns one
+    dict per survey, equal to gradient(s, vs, cr0_r, cr0_l) of each (single path)."""
+    from .fd import (e2drtm_mex_args, eigen_e2drtm_single_batch, eigen_staggerfd_single_batch, prep_model,
+                     staggerfd_mex_args)
+    fwd, keys, mats = [], [], []
+    for c, (s, vs, _, _) in enumerate(cases):
+        m = prep_model(s.nbc, s.dtx, s.dx, s.dt, s.vp_ratio * vs, vs, s.isfs, s.fd_order, True)
+        mats.append(m)
+        for is_ in range(1, s.ns + 1):
+            args = staggerfd_mex_args(s.nbc, s.nt, s.dtx, s.dx, s.dt, int(s.sx[is_ - 1]), 1, s.gx, np.ones(s.ng),
+                                      s.vp_ratio * vs, vs, s.isfs, s.fd_order, s.source_type, 0, s.nt_wf, True, m)
+            fwd.append((*args, s.source()))
+            keys.append((c, is_))
+    seis = eigen_staggerfd_single_batch(fwd, want_wf=True)
+    per = [[] for _ in cases]
+    adj = []
+    for (c, is_), (_, sw, www) in zip(keys, seis):
+        s, vs, cr0_r, cr0_l = cases[c]
+        out, a = _shot_adjoint_source(s, is_, sw, cr0_r, cr0_l, True, field, FK)
+        per[c].append(out)
+        adj.append(e2drtm_mex_args(www, a, s.nbc, s.nt, s.dtx, s.dx, s.dt, s.gx, np.ones(s.ng), s.vp_ratio * vs, vs,
+                                   s.isfs, s.fd_order, 0, s.nt_wf, True, mats[c]))
+    for (c, _), (cl, cm, il), out in zip(keys, eigen_e2drtm_single_batch(adj), [o for p in per for o in p]):
+        out.update(cl=np.asarray(cl, np.float64), cm=np.asarray(cm, np.float64), il=np.asarray(il, np.float64))
+    return [_assemble(cases[c][0], cases[c][1], per[c], False) for c in range(len(cases))]
+
+
+def gradient(s, vs, cr0_r, cr0_l, single=True, keep_shots=False, field=0, FK=0):
+    """SWD.m:171-201: shot sums in shot order (FP64), Vs gradient, smoothing, misfit."""
+    per = [shot_gradient(s, is_, vs, cr0_r, cr0_l, single, field, FK) for is_ in range(1, s.ns + 1)]
+    return _assemble(s, vs, per, keep_shots)

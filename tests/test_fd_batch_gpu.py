@@ -86,3 +86,21 @@ def test_adjoint_batch_matches_separate_calls_and_oracle(O):
         for g, a, r in zip(got, one, ref):
             assert np.abs(r).max() > 0
             assert np.array_equal(g, a) and np.array_equal(g, r)
+
+
+def test_gradient_of_several_surveys_in_one_batch(O):
+    """swd_loop.gradient_many: the shots of two surveys on different grids go through one forward
+    batch and one adjoint batch; each survey's gradient, picks and misfits equal its own
+    swd_loop.gradient, bit for bit."""
+    from swd_b200 import swd_loop
+    cases = []
+    for s in (configs.tiny(nt=400), dataclasses.replace(configs.plain_c1(), nt=1000)):
+        cr0_r, cr0_l = O.observed_curves(s, s.vs_true)
+        cases.append((s, s.vs, cr0_r, cr0_l))
+    many = swd_loop.gradient_many(cases)
+    for (s, vs, cr0_r, cr0_l), got in zip(cases, many):
+        ref = swd_loop.gradient(s, vs, cr0_r, cr0_l)
+        for k in ("g_cl", "g_cm", "g_illum", "cr_pre_r", "cr_pre_l"):
+            assert np.array_equal(got[k], ref[k]), (s.name, k)
+        for k in ("dk_vs", "res_r", "res_l"):
+            assert np.array_equal(got[k], ref[k], equal_nan=True), (s.name, k)
