@@ -353,6 +353,18 @@ fd_fwd_smem(FwdArgs<T> a, int it) {
   fwd_smem_tile<T, NF, W, C, D, GB, SNAP>(a, it, blockIdx.x);
 }
 
+// The job that owns CTA b: the last j with cta0[j] <= b (binary search over the running tile counts,
+// cta0[0] = 0 <= b < cta0[n_jobs]).
+__device__ __forceinline__ int owning_job(const int* __restrict__ cta0, int n_jobs, int b) {
+  int lo = 0, hi = n_jobs - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cta0[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
 // Several forward calls advanced by one launch per step, on grids of any sizes: CTA b runs tile
 // b - cta0[j] of job j, where cta0 holds the running sums of the jobs' tile counts (cta0[0] = 0,
 // cta0[n_jobs] = the grid); a job whose time steps are done leaves at once.  The jobs share the
@@ -362,8 +374,7 @@ fd_fwd_smem(FwdArgs<T> a, int it) {
 template <typename T, int NF, int W, int C, int D, bool GB>
 __global__ void __launch_bounds__(32 * W)
 fd_fwd_smem_multi(const FwdArgs<T>* __restrict__ jobs, const int* __restrict__ cta0, int n_jobs, int it) {
-  int j = 0;
-  while (j + 1 < n_jobs && (int)blockIdx.x >= cta0[j + 1]) ++j;
+  const int j = owning_job(cta0, n_jobs, (int)blockIdx.x);
   const FwdArgs<T>& a = jobs[j];
   if (it >= a.g.nt) return;  // uniform over the CTA
   const int tile = (int)blockIdx.x - cta0[j];
@@ -592,8 +603,7 @@ fd_adj_smem(AdjArgs<T> a, int it) {
 template <typename T, int NF, int W, int C, int D, bool GB>
 __global__ void __launch_bounds__(32 * W)
 fd_adj_smem_multi(const AdjArgs<T>* __restrict__ jobs, const int* __restrict__ cta0, int n_jobs, int step) {
-  int j = 0;
-  while (j + 1 < n_jobs && (int)blockIdx.x >= cta0[j + 1]) ++j;
+  const int j = owning_job(cta0, n_jobs, (int)blockIdx.x);
   const AdjArgs<T>& a = jobs[j];
   const int it = a.g.nt - 2 - step;
   if (it < 0) return;  // uniform over the CTA
