@@ -9,8 +9,8 @@
 
 typedef size_t mwSize;
 typedef struct mxArray_tag mxArray;
-typedef enum { mxUNKNOWN_CLASS = 0, mxSTRUCT_CLASS = 2, mxDOUBLE_CLASS = 6, mxSINGLE_CLASS = 7,
-               mxINT32_CLASS = 12 } mxClassID;
+typedef enum { mxUNKNOWN_CLASS = 0, mxCELL_CLASS = 1, mxSTRUCT_CLASS = 2, mxDOUBLE_CLASS = 6,
+               mxSINGLE_CLASS = 7, mxINT32_CLASS = 12 } mxClassID;
 typedef enum { mxREAL = 0, mxCOMPLEX = 1 } mxComplexity;
 
 void mexErrMsgIdAndTxt(const char* id, const char* fmt, ...);
@@ -21,6 +21,10 @@ int mxIsSingle(const mxArray* a);
 int mxIsDouble(const mxArray* a);
 int mxIsComplex(const mxArray* a);
 int mxIsStruct(const mxArray* a);
+int mxIsCell(const mxArray* a);
+mxArray* mxGetCell(const mxArray* a, mwSize i);
+void mxSetCell(mxArray* a, mwSize i, mxArray* v);
+mxArray* mxCreateCellMatrix(mwSize m, mwSize n);
 void* mxGetData(const mxArray* a);
 double* mxGetPr(const mxArray* a);
 double* mxGetPi(const mxArray* a);

@@ -16,6 +16,7 @@ struct mxArray_tag {
   int nf;
   char* fname[MAXF];
   mxArray* fval[MAXF];
+  mxArray** cells; /* cell arrays: n elements (NULL = empty) */
 };
 
 static jmp_buf g_jmp;
@@ -44,6 +45,7 @@ static mxArray* make(mxClassID c, mwSize nd, const mwSize* dims, int cplx) {
   a->n = 1;
   for (size_t i = 0; i < nd; ++i) { a->dims[i] = dims[i]; a->n *= dims[i]; }
   a->esz = esz_of(c);
+  if (c == mxCELL_CLASS) a->cells = (mxArray**)calloc(a->n ? a->n : 1, sizeof(mxArray*));
   if (a->esz) {
     a->re = calloc(a->n ? a->n : 1, a->esz);
     if (cplx) a->im = calloc(a->n ? a->n : 1, a->esz);
@@ -58,6 +60,15 @@ int mxIsSingle(const mxArray* a) { return a->cls == mxSINGLE_CLASS; }
 int mxIsDouble(const mxArray* a) { return a->cls == mxDOUBLE_CLASS; }
 int mxIsComplex(const mxArray* a) { return a->cplx; }
 int mxIsStruct(const mxArray* a) { return a->cls == mxSTRUCT_CLASS; }
+int mxIsCell(const mxArray* a) { return a->cls == mxCELL_CLASS; }
+mxArray* mxGetCell(const mxArray* a, mwSize i) { return a->cls == mxCELL_CLASS && i < a->n ? a->cells[i] : NULL; }
+void mxSetCell(mxArray* a, mwSize i, mxArray* v) {
+  if (a->cls == mxCELL_CLASS && i < a->n) { mxDestroyArray(a->cells[i]); a->cells[i] = v; }
+}
+mxArray* mxCreateCellMatrix(mwSize m, mwSize n) {
+  mwSize d[2] = {m, n};
+  return make(mxCELL_CLASS, 2, d, 0);
+}
 void* mxGetData(const mxArray* a) { return a->re; }
 double* mxGetPr(const mxArray* a) { return a->cls == mxDOUBLE_CLASS ? (double*)a->re : NULL; }
 double* mxGetPi(const mxArray* a) { return a->cls == mxDOUBLE_CLASS ? (double*)a->im : NULL; }
@@ -95,6 +106,10 @@ mxArray* mxGetField(const mxArray* s, mwSize i, const char* name) {
 void mxDestroyArray(mxArray* a) {
   if (!a) return;
   for (int k = 0; k < a->nf; ++k) { free(a->fname[k]); mxDestroyArray(a->fval[k]); }
+  if (a->cells) {
+    for (size_t i = 0; i < a->n; ++i) mxDestroyArray(a->cells[i]);
+    free(a->cells);
+  }
   free(a->re);
   free(a->im);
   free(a);
@@ -121,6 +136,10 @@ int sim_nfields(const mxArray* a) { return a->nf; }
 const char* sim_field_name(const mxArray* a, int k) { return a->fname[k]; }
 mxArray* sim_field_value(const mxArray* a, int k) { return a->fval[k]; }
 void sim_destroy(mxArray* a) { mxDestroyArray(a); }
+mxArray* sim_cell(size_t n) { return mxCreateCellMatrix(1, n); }
+void sim_set_cell(mxArray* a, size_t i, mxArray* v) { mxSetCell(a, i, v); }
+mxArray* sim_get_cell(const mxArray* a, size_t i) { return mxGetCell(a, i); }
+size_t sim_numel(const mxArray* a) { return a->n; }
 const char* sim_error(void) { return g_err; }
 
 /* Run mexFunction; 0 on success, 1 if it raised an error (message in sim_error()). */

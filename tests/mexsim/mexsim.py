@@ -43,11 +43,23 @@ class Shim:
         L.sim_field_value.restype = vp
         L.sim_field_value.argtypes = [vp, ctypes.c_int]
         L.sim_destroy.argtypes = [vp]
+        L.sim_cell.restype = vp
+        L.sim_cell.argtypes = [ctypes.c_size_t]
+        L.sim_set_cell.argtypes = [vp, ctypes.c_size_t, vp]
+        L.sim_get_cell.restype = vp
+        L.sim_get_cell.argtypes = [vp, ctypes.c_size_t]
+        L.sim_numel.restype = ctypes.c_size_t
+        L.sim_numel.argtypes = [vp]
         L.sim_error.restype = ctypes.c_char_p
         L.sim_call.argtypes = [ctypes.c_int, ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
         self.L = L
 
     def _to_mx(self, x):
+        if isinstance(x, list):  # a 1 x n cell array
+            c = self.L.sim_cell(len(x))
+            for i, v in enumerate(x):
+                self.L.sim_set_cell(c, i, self._to_mx(v))
+            return c
         if isinstance(x, dict):
             s = self.L.sim_struct()
             for k, v in x.items():
@@ -68,6 +80,8 @@ class Shim:
 
     def _from_mx(self, p):
         L = self.L
+        if L.sim_class(p) == 1:
+            return [self._from_mx(L.sim_get_cell(p, i)) for i in range(L.sim_numel(p))]
         if L.sim_class(p) == 2:
             return {L.sim_field_name(p, k).decode(): self._from_mx(L.sim_field_value(p, k))
                     for k in range(L.sim_nfields(p))}

@@ -18,7 +18,8 @@ from swd_b200 import configs  # noqa: E402
 
 SHIMS = ["eigen_staggerfd_single", "eigen_staggerfd_double", "eigen_e2drtm_single", "eigen_e2drtm_double",
          "RTrAD", "RTlAD", "RTr", "RTl", "LHDispPick", "ADWDgrad_1", "ADWDgrad_norm", "ADWDgradlimband",
-         "weight_data_muti3", "norm_trace", "fk_filter", "field/LHDispPick", "field/ADWDgrad_1"]
+         "weight_data_muti3", "norm_trace", "fk_filter", "eigen_staggerfd_single_batch", "field/LHDispPick",
+         "field/ADWDgrad_1"]
 
 
 @pytest.fixture(scope="module")
@@ -79,6 +80,38 @@ def test_radon_shims_check_np_and_adwdgrad_needs_shim_structs(shim):
     with pytest.raises(mexsim.MexError, match="swd_params"):
         shim("ADWDgrad_1")(1, s.nt, s.ng, s.ns, npair, 2, s.w, s.m, s.M, 1e4, np.ones(npair), np.ones(npair),
                            np.ones((701, npair)), {"mm": np.zeros((3, 3))}, {"mm": np.zeros((3, 3))})
+
+
+def test_batch_shim_checks_its_cell_arrays(shim):
+    f = shim("eigen_staggerfd_single_batch")
+    with pytest.raises(mexsim.MexError, match="cell array"):
+        f(1, *([np.zeros(3, np.float32)] * 9))
+    with pytest.raises(mexsim.MexError, match="entries"):
+        f(1, *([[np.zeros(3, np.float32)]] * 8), [])
+
+
+@pytest.mark.gpu
+def test_batch_shim_matches_the_single_shim(O, shim):
+    """Two jobs on different grids in one eigen_staggerfd_single_batch call (cell arrays in and
+    out) give what two eigen_staggerfd_single calls give."""
+    import dataclasses
+
+    from swd_b200 import configs
+    cases = [configs.tiny(nt=400), dataclasses.replace(configs.plain_c1(), nt=800, nt_wf=10)]
+    args, refs = [[] for _ in range(9)], []
+    for s in cases:
+        inp = O.fd_inputs(s.nbc, s.nt, s.dtx, s.dx, s.dt, int(s.sx[1]), 1, s.gx, np.ones(s.ng), s.vp, s.vs,
+                          in_wf=s.nt_wf)
+        w = s.source().astype(np.float32)
+        one = (inp.iv, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w)
+        for k in range(9):
+            args[k].append(one[k])
+        refs.append(shim("eigen_staggerfd_single")(3, *one))
+    su, sw, www = shim("eigen_staggerfd_single_batch")(3, *args)
+    for j, (ru, rw, rwww) in enumerate(refs):
+        assert np.array_equal(su[j], ru) and np.array_equal(sw[j], rw), j
+        for k in ("fux", "fuz", "bwx", "bwz"):
+            assert np.array_equal(www[j][k], rwww[k]), (j, k)
 
 
 @pytest.mark.gpu
