@@ -102,15 +102,16 @@ int swd_staggerfd_double(const double* iv, int n_iv, const double* temp, const d
 /* Replaces eigen_e2drtm_single(iv,temp,ca,cl,cm,cm1,b,b1,seismo_w,fux,fuz,bwx,bwz)
  * (core/eigen_e2drtm_single.cpp:67-296, called at core/e2drtm_eigen.m:122).
  * iv: the 14-entry input_vector of core/e2drtm_eigen.m:121.  seismo_w: nt x ng
- * adjoint source.  Outputs nz x nx.  The images accumulate in FP64 on the GPU and
- * are rounded to float on return (the reference accumulates in float). */
+ * adjoint source.  Outputs nz x nx.  The images are summed over time steps in FP32, as the
+ * reference's single MEX sums them (core/eigen_e2drtm_single.cpp:274-279), and equal its
+ * images bit for bit. */
 int swd_e2drtm_single(const float* iv, int n_iv, const float* temp, const float* ca,
                       const float* cl, const float* cm, const float* cm1, const float* b,
                       const float* b1, const float* seismo_w, const float* fux, const float* fuz,
                       const float* bwx, const float* bwz, float* cl_img, float* cm_img,
                       float* illum_div);
 
-/* As swd_e2drtm_single, returning the FP64 accumulators unrounded. */
+/* As swd_e2drtm_single, with the images summed over time steps in FP64 and returned unrounded. */
 int swd_e2drtm_single_f64out(const float* iv, int n_iv, const float* temp, const float* ca,
                              const float* cl, const float* cm, const float* cm1, const float* b,
                              const float* b1, const float* seismo_w, const float* fux,

@@ -18,8 +18,8 @@ from swd_b200 import configs  # noqa: E402
 
 SHIMS = ["eigen_staggerfd_single", "eigen_staggerfd_double", "eigen_e2drtm_single", "eigen_e2drtm_double",
          "RTrAD", "RTlAD", "RTr", "RTl", "LHDispPick", "ADWDgrad_1", "ADWDgrad_norm", "ADWDgradlimband",
-         "weight_data_muti3", "norm_trace", "fk_filter", "eigen_staggerfd_single_batch", "field/LHDispPick",
-         "field/ADWDgrad_1"]
+         "weight_data_muti3", "norm_trace", "fk_filter", "eigen_staggerfd_single_batch", "eigen_e2drtm_single_batch",
+         "field/LHDispPick", "field/ADWDgrad_1"]
 
 
 @pytest.fixture(scope="module")
@@ -82,18 +82,20 @@ def test_radon_shims_check_np_and_adwdgrad_needs_shim_structs(shim):
                            np.ones((701, npair)), {"mm": np.zeros((3, 3))}, {"mm": np.zeros((3, 3))})
 
 
-def test_batch_shim_checks_its_cell_arrays(shim):
-    f = shim("eigen_staggerfd_single_batch")
+@pytest.mark.parametrize("name,nrhs", [("eigen_staggerfd_single_batch", 9), ("eigen_e2drtm_single_batch", 13)])
+def test_batch_shims_check_their_cell_arrays(shim, name, nrhs):
+    f = shim(name)
     with pytest.raises(mexsim.MexError, match="cell array"):
-        f(1, *([np.zeros(3, np.float32)] * 9))
+        f(1, *([np.zeros(3, np.float32)] * nrhs))
     with pytest.raises(mexsim.MexError, match="entries"):
-        f(1, *([[np.zeros(3, np.float32)]] * 8), [])
+        f(1, *([[np.zeros(3, np.float32)]] * (nrhs - 1)), [])
 
 
 @pytest.mark.gpu
-def test_batch_shim_matches_the_single_shim(O, shim):
+def test_batch_shims_match_the_single_shims(O, shim):
     """Two jobs on different grids in one eigen_staggerfd_single_batch call (cell arrays in and
-    out) give what two eigen_staggerfd_single calls give."""
+    out) give what two eigen_staggerfd_single calls give; likewise eigen_e2drtm_single_batch
+    against eigen_e2drtm_single on those jobs' wavefields."""
     import dataclasses
 
     from swd_b200 import configs
@@ -112,6 +114,22 @@ def test_batch_shim_matches_the_single_shim(O, shim):
         assert np.array_equal(su[j], ru) and np.array_equal(sw[j], rw), j
         for k in ("fux", "fuz", "bwx", "bwz"):
             assert np.array_equal(www[j][k], rwww[k]), (j, k)
+    rng = np.random.default_rng(2)
+    aargs, arefs = [[] for _ in range(13)], []
+    for s, (_, rw, rwww) in zip(cases, refs):
+        ainp = O.fd_inputs(s.nbc, s.nt, s.dtx, s.dx, s.dt, int(s.sx[1]), 1, s.gx, np.ones(s.ng), s.vp, s.vs,
+                           in_wf=s.nt_wf, adjoint=True)
+        res = (rng.standard_normal(rw.shape) * 1e-3).astype(np.float32)
+        one = (ainp.iv, ainp.temp, ainp.ca, ainp.cl, ainp.cm, ainp.cm1, ainp.b, ainp.b1, res, rwww["fux"],
+               rwww["fuz"], rwww["bwx"], rwww["bwz"])
+        for k in range(13):
+            aargs[k].append(one[k])
+        arefs.append(shim("eigen_e2drtm_single")(3, *one))
+    got = shim("eigen_e2drtm_single_batch")(3, *aargs)
+    for j, want in enumerate(arefs):
+        for k in range(3):
+            assert got[k][j].dtype == np.float32 and np.abs(want[k]).max() > 0, (j, k)
+            assert np.array_equal(got[k][j], want[k]), (j, k)
 
 
 @pytest.mark.gpu
