@@ -751,29 +751,36 @@ int swd_radon(const swd_radon_params* p, int side, int is, const double* seismo,
             "shot %d has an empty or out-of-range %s window", is, side ? "left" : "right");
   gg.valid = 1;
   const size_t nsz = (size_t)g.nt * g.ng, spec = (size_t)g.npair * g.np;
-  DevBuf b_seis, b_seis_t, b_W, b_K, b_D, b_MM, b_raw, b_ml, b_g;
-  SWD_TRY(b_seis.alloc(nsz * sizeof(double)));
-  SWD_TRY(b_seis_t.alloc(nsz * sizeof(double)));
-  SWD_TRY(b_W.alloc((size_t)g.npair * g.ntd * sizeof(double2)));
-  SWD_TRY(b_K.alloc((size_t)g.npair * g.offset * g.np * sizeof(double2)));
-  SWD_TRY(b_D.alloc((size_t)g.npair * g.offset * sizeof(double2)));
-  SWD_TRY(b_MM.alloc(spec * sizeof(double2)));
-  SWD_TRY(b_raw.alloc(spec * sizeof(double)));
-  SWD_TRY(b_ml.alloc(spec * sizeof(double)));
-  SWD_TRY(b_g.alloc(sizeof(Gather)));
+  SlabPlan sp;
+  const size_t o_seis = sp.add(nsz * sizeof(double)), o_seis_t = sp.add(nsz * sizeof(double));
+  const size_t o_W = sp.add((size_t)g.npair * g.ntd * sizeof(double2));
+  const size_t o_K = sp.add((size_t)g.npair * g.offset * g.np * sizeof(double2));
+  const size_t o_D = sp.add((size_t)g.npair * g.offset * sizeof(double2));
+  const size_t o_MM = sp.add(spec * sizeof(double2)), o_raw = sp.add(spec * sizeof(double));
+  const size_t o_ml = sp.add(spec * sizeof(double)), o_g = sp.add(sizeof(Gather));
+  DevBuf slab;
+  SWD_TRY(slab.alloc(sp.bytes));
+  double* d_seis = SlabPlan::at<double>(slab, o_seis);
+  double* d_seis_t = SlabPlan::at<double>(slab, o_seis_t);
+  double2* d_W = SlabPlan::at<double2>(slab, o_W);
+  double2* d_K = SlabPlan::at<double2>(slab, o_K);
+  double2* d_D = SlabPlan::at<double2>(slab, o_D);
+  double2* d_MM = SlabPlan::at<double2>(slab, o_MM);
+  double* d_raw = SlabPlan::at<double>(slab, o_raw);
+  double* d_ml = SlabPlan::at<double>(slab, o_ml);
+  Gather* d_g = SlabPlan::at<Gather>(slab, o_g);
   cudaStream_t st = 0;
-  SWD_CUDA(cudaMemcpyAsync(b_seis.p, seismo, nsz * sizeof(double), cudaMemcpyHostToDevice, st));
-  SWD_CUDA(cudaMemcpyAsync(b_g.p, &gg, sizeof(Gather), cudaMemcpyHostToDevice, st));
-  SWD_TRY(transpose<double, double>(b_seis.as<double>(), 0, b_seis_t.as<double>(), 0, 1, g.ng, g.nt, st));
-  SWD_TRY(radon_tables(g, b_W.as<double2>(), b_K.as<double2>(), st));
-  SWD_TRY(radon_dft<double>(g, b_g.as<Gather>(), 1, b_seis_t.as<double>(), 0, b_W.as<double2>(), b_D.as<double2>(), st));
-  SWD_TRY(radon_contract(g, b_g.as<Gather>(), 1, b_K.as<double2>(), b_D.as<double2>(), b_MM.as<double2>(),
-                         b_raw.as<double>(), b_ml.as<double>(), st));
-  SWD_CUDA(cudaMemcpyAsync(ml, b_ml.p, spec * sizeof(double), cudaMemcpyDeviceToHost, st));
-  if (ml_raw) SWD_CUDA(cudaMemcpyAsync(ml_raw, b_raw.p, spec * sizeof(double), cudaMemcpyDeviceToHost, st));
+  SWD_CUDA(cudaMemcpyAsync(d_seis, seismo, nsz * sizeof(double), cudaMemcpyHostToDevice, st));
+  SWD_CUDA(cudaMemcpyAsync(d_g, &gg, sizeof(Gather), cudaMemcpyHostToDevice, st));
+  SWD_TRY(transpose<double, double>(d_seis, 0, d_seis_t, 0, 1, g.ng, g.nt, st));
+  SWD_TRY(radon_tables(g, d_W, d_K, st));
+  SWD_TRY(radon_dft<double>(g, d_g, 1, d_seis_t, 0, d_W, d_D, st));
+  SWD_TRY(radon_contract(g, d_g, 1, d_K, d_D, d_MM, d_raw, d_ml, st));
+  SWD_CUDA(cudaMemcpyAsync(ml, d_ml, spec * sizeof(double), cudaMemcpyDeviceToHost, st));
+  if (ml_raw) SWD_CUDA(cudaMemcpyAsync(ml_raw, d_raw, spec * sizeof(double), cudaMemcpyDeviceToHost, st));
   if (mm) {  // np x nf interleaved complex, columns before lf are zero (RTrAD.m:22)
     std::memset(mm, 0, (size_t)(g.lf - 1) * g.np * 2 * sizeof(double));
-    SWD_CUDA(cudaMemcpyAsync(mm + (size_t)(g.lf - 1) * g.np * 2, b_MM.p, spec * sizeof(double2),
+    SWD_CUDA(cudaMemcpyAsync(mm + (size_t)(g.lf - 1) * g.np * 2, d_MM, spec * sizeof(double2),
                              cudaMemcpyDeviceToHost, st));
   }
   SWD_CUDA(cudaStreamSynchronize(st));
@@ -944,19 +951,33 @@ static int adwdgrad_impl(const swd_radon_params* p, int ns, int is, int w, doubl
     }
   }
   const size_t spec = (size_t)g.npair * g.np, nsz = (size_t)g.nt * g.ng;
-  DevBuf b_W, b_K, b_MM, b_raw, b_dc, b_sm, b_Gx, b_out, b_out_t, b_g, b_cr, b_tab, b_max;
-  if (maxnorm) SWD_TRY(b_max.alloc(sizeof(unsigned long long)));
-  if (gauss) SWD_TRY(b_cr.alloc(2 * (size_t)g.npair * sizeof(double)));
-  SWD_TRY(b_W.alloc((size_t)g.npair * g.ntd * sizeof(double2)));
-  SWD_TRY(b_K.alloc((size_t)g.npair * g.offset * g.np * sizeof(double2)));
-  SWD_TRY(b_MM.alloc(2 * spec * sizeof(double2)));
-  SWD_TRY(b_raw.alloc(2 * spec * sizeof(double)));
-  SWD_TRY(b_dc.alloc(2 * (size_t)g.npair * sizeof(double)));
-  SWD_TRY(b_Gx.alloc(2 * (size_t)g.npair * g.offset * sizeof(double2)));
-  SWD_TRY(b_out.alloc(nsz * sizeof(double)));
-  SWD_TRY(b_out_t.alloc(nsz * sizeof(double)));
-  SWD_TRY(b_g.alloc(2 * sizeof(Gather)));
-  if (space_m) SWD_TRY(b_sm.alloc(spec * sizeof(double)));
+  SlabPlan sp;
+  const size_t o_max = sp.add(maxnorm ? sizeof(unsigned long long) : 0);
+  const size_t o_cr = sp.add(gauss ? 2 * (size_t)g.npair * sizeof(double) : 0);
+  const size_t o_W = sp.add((size_t)g.npair * g.ntd * sizeof(double2));
+  const size_t o_K = sp.add((size_t)g.npair * g.offset * g.np * sizeof(double2));
+  const size_t o_MM = sp.add(2 * spec * sizeof(double2)), o_raw = sp.add(2 * spec * sizeof(double));
+  const size_t o_dc = sp.add(2 * (size_t)g.npair * sizeof(double));
+  const size_t o_Gx = sp.add(2 * (size_t)g.npair * g.offset * sizeof(double2));
+  const size_t o_out = sp.add(nsz * sizeof(double)), o_out_t = sp.add(nsz * sizeof(double));
+  const size_t o_g = sp.add(2 * sizeof(Gather));
+  const size_t o_sm = sp.add(space_m ? spec * sizeof(double) : 0);
+  const size_t o_tab = sp.add(mode == 2 ? 2 * (size_t)g.ntd * sizeof(double2) : 0);
+  DevBuf slab;
+  SWD_TRY(slab.alloc(sp.bytes));
+  unsigned long long* d_max = SlabPlan::at<unsigned long long>(slab, o_max);
+  double* d_cr = SlabPlan::at<double>(slab, o_cr);
+  double2* d_W = SlabPlan::at<double2>(slab, o_W);
+  double2* d_K = SlabPlan::at<double2>(slab, o_K);
+  double2* d_MM = SlabPlan::at<double2>(slab, o_MM);
+  double* d_raw = SlabPlan::at<double>(slab, o_raw);
+  double* d_dc = SlabPlan::at<double>(slab, o_dc);
+  double2* d_Gx = SlabPlan::at<double2>(slab, o_Gx);
+  double* d_out = SlabPlan::at<double>(slab, o_out);
+  double* d_out_t = SlabPlan::at<double>(slab, o_out_t);
+  Gather* d_g = SlabPlan::at<Gather>(slab, o_g);
+  double* d_sm = SlabPlan::at<double>(slab, o_sm);
+  double2* d_tab = SlabPlan::at<double2>(slab, o_tab);
   cudaStream_t st = 0;
   if (mode == 2) {
     // taper tables: bins i = lf-25 .. lf-1 carry bin lf times (i-lf+25)/25, bins nf+1 .. nf+25
@@ -980,36 +1001,31 @@ static int adwdgrad_impl(const swd_radon_params* p, int ns, int is, int w, doubl
       tab[t] = make_double2(ar, ai);
       tab[(size_t)g.ntd + t] = make_double2(br, bi);
     }
-    SWD_TRY(b_tab.alloc(tab.size() * sizeof(double2)));
-    SWD_CUDA(cudaMemcpy(b_tab.p, tab.data(), tab.size() * sizeof(double2), cudaMemcpyHostToDevice));
+    SWD_CUDA(cudaMemcpy(d_tab, tab.data(), tab.size() * sizeof(double2), cudaMemcpyHostToDevice));
   }
   for (int s = 0; s < 2; ++s) {
     if (gg[s].valid != 1) continue;
-    SWD_CUDA(cudaMemcpyAsync(b_MM.as<double2>() + s * spec, mm[s] + (size_t)(g.lf - 1) * g.np * 2,
-                             spec * sizeof(double2), cudaMemcpyHostToDevice, st));
-    SWD_CUDA(cudaMemcpyAsync(b_raw.as<double>() + s * spec, raw[s], spec * sizeof(double), cudaMemcpyHostToDevice, st));
-    SWD_CUDA(cudaMemcpyAsync(b_dc.as<double>() + s * g.npair, go[s], g.npair * sizeof(double),
+    SWD_CUDA(cudaMemcpyAsync(d_MM + s * spec, mm[s] + (size_t)(g.lf - 1) * g.np * 2, spec * sizeof(double2),
                              cudaMemcpyHostToDevice, st));
+    SWD_CUDA(cudaMemcpyAsync(d_raw + s * spec, raw[s], spec * sizeof(double), cudaMemcpyHostToDevice, st));
+    SWD_CUDA(cudaMemcpyAsync(d_dc + s * g.npair, go[s], g.npair * sizeof(double), cudaMemcpyHostToDevice, st));
     if (gauss)
-      SWD_CUDA(cudaMemcpyAsync(b_cr.as<double>() + s * g.npair, cr[s], g.npair * sizeof(double),
-                               cudaMemcpyHostToDevice, st));
+      SWD_CUDA(cudaMemcpyAsync(d_cr + s * g.npair, cr[s], g.npair * sizeof(double), cudaMemcpyHostToDevice, st));
   }
-  if (space_m) SWD_CUDA(cudaMemcpyAsync(b_sm.p, space_m, spec * sizeof(double), cudaMemcpyHostToDevice, st));
+  if (space_m) SWD_CUDA(cudaMemcpyAsync(d_sm, space_m, spec * sizeof(double), cudaMemcpyHostToDevice, st));
   gg[0].shot = 0;
   gg[1].shot = 0;
-  SWD_CUDA(cudaMemcpyAsync(b_g.p, gg, 2 * sizeof(Gather), cudaMemcpyHostToDevice, st));
-  SWD_CUDA(cudaMemsetAsync(b_out.p, 0, nsz * sizeof(double), st));
-  SWD_TRY(radon_tables(g, b_W.as<double2>(), b_K.as<double2>(), st));
-  SWD_TRY(softmax_adjoint(g, b_g.as<Gather>(), 2, b_raw.as<double>(), b_MM.as<double2>(), b_dc.as<double>(),
-                          space_m ? b_sm.as<double>() : nullptr, soft_arg_norm, b_K.as<double2>(),
-                          b_Gx.as<double2>(), st, gauss ? b_cr.as<double>() : nullptr, 0.0, mode == 2));
-  SWD_TRY(radon_idft_scatter<double>(g, b_g.as<Gather>(), 2, b_Gx.as<double2>(), b_W.as<double2>(),
-                                     b_out.as<double>(), 0, st, mode == 2 ? b_tab.as<double2>() : nullptr,
-                                     mode == 2 ? b_tab.as<double2>() + g.ntd : nullptr));
-  if (maxnorm) SWD_TRY(divide_by_maxabs(b_out.as<double>(), nsz, b_max.as<unsigned long long>(), st));
+  SWD_CUDA(cudaMemcpyAsync(d_g, gg, 2 * sizeof(Gather), cudaMemcpyHostToDevice, st));
+  SWD_CUDA(cudaMemsetAsync(d_out, 0, nsz * sizeof(double), st));
+  SWD_TRY(radon_tables(g, d_W, d_K, st));
+  SWD_TRY(softmax_adjoint(g, d_g, 2, d_raw, d_MM, d_dc, space_m ? d_sm : nullptr, soft_arg_norm, d_K, d_Gx, st,
+                          gauss ? d_cr : nullptr, 0.0, mode == 2));
+  SWD_TRY(radon_idft_scatter<double>(g, d_g, 2, d_Gx, d_W, d_out, 0, st, mode == 2 ? d_tab : nullptr,
+                                     mode == 2 ? d_tab + g.ntd : nullptr));
+  if (maxnorm) SWD_TRY(divide_by_maxabs(d_out, nsz, d_max, st));
   // [nt][ng] -> MATLAB nt x ng
-  SWD_TRY(transpose<double, double>(b_out.as<double>(), 0, b_out_t.as<double>(), 0, 1, g.nt, g.ng, st));
-  SWD_CUDA(cudaMemcpyAsync(a_data_res, b_out_t.p, nsz * sizeof(double), cudaMemcpyDeviceToHost, st));
+  SWD_TRY(transpose<double, double>(d_out, 0, d_out_t, 0, 1, g.nt, g.ng, st));
+  SWD_CUDA(cudaMemcpyAsync(a_data_res, d_out_t, nsz * sizeof(double), cudaMemcpyDeviceToHost, st));
   SWD_CUDA(cudaStreamSynchronize(st));
   return SWD_OK;
 }

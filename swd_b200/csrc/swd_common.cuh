@@ -72,4 +72,19 @@ struct DevBuf {
   template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Offsets of several scratch arrays inside one allocation, each on a 256-byte boundary, so that
+// a call needing many arrays makes one cudaMalloc and one cudaFree (each cudaFree synchronises
+// the device).  add(n) reserves n bytes and returns their offset; add(0) reserves nothing.
+struct SlabPlan {
+  size_t bytes = 0;
+  size_t add(size_t n) {
+    const size_t o = bytes;
+    bytes += (n + 255) / 256 * 256;
+    return o;
+  }
+  template <typename T> static T* at(const DevBuf& b, size_t off) {
+    return reinterpret_cast<T*>(static_cast<char*>(b.p) + off);
+  }
+};
+
 }  // namespace swd
