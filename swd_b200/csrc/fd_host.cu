@@ -510,7 +510,8 @@ template <typename T>
 struct FwdJob {
   FwdIv p{};
   FdGeom g{};
-  DevBuf d_in, d_m1, d_m2, d_state, d_seis, d_seis_t, d_snap, d_snap_t, d_src;
+  DevBuf slab;  // one allocation holding every buffer below
+  DevView d_in, d_m1, d_m2, d_state, d_seis, d_seis_t, d_snap, d_snap_t, d_src;
   FwdArgs<T> a{};
   T* bufs[2] = {nullptr, nullptr};
   T* out[6] = {};  // host: seis_u, seis_w, fux, fuz, bwx, bwz
@@ -536,17 +537,24 @@ int fwd_job_setup(FwdJob<T>& J, const T* iv, int n_iv, const T* temp, const T* c
   using V = typename Vec4<T>::type;
   using V2 = typename Vec2<T>::type;
   const size_t NN = (size_t)p.nzbc * p.nxbc, plane = (size_t)p.nz * p.nx;
-  SWD_TRY(J.d_in.alloc(6 * NN * sizeof(T) + p.nt * sizeof(T)));
-  SWD_TRY(J.d_m1.alloc(g.field * sizeof(V)));
-  SWD_TRY(J.d_m2.alloc(g.field * sizeof(V2)));
-  SWD_TRY(J.d_state.alloc(2 * 5 * g.field * sizeof(T)));
-  SWD_TRY(J.d_seis.alloc(2 * (size_t)p.nt * p.ng * sizeof(T)));
-  SWD_TRY(J.d_seis_t.alloc(2 * (size_t)p.nt * p.ng * sizeof(T)));
-  SWD_TRY(J.d_src.alloc(sizeof(int2)));
-  if (want_wf) {
-    SWD_TRY(J.d_snap.alloc((size_t)g.nrec * 4 * plane * sizeof(T)));
-    SWD_TRY(J.d_snap_t.alloc((size_t)g.nrec * plane * sizeof(T)));
-  }
+  const size_t n_in = 6 * NN * sizeof(T) + p.nt * sizeof(T), n_m1 = g.field * sizeof(V), n_m2 = g.field * sizeof(V2);
+  const size_t n_state = 2 * 5 * g.field * sizeof(T), n_seis = 2 * (size_t)p.nt * p.ng * sizeof(T);
+  const size_t n_snap = want_wf ? (size_t)g.nrec * 4 * plane * sizeof(T) : 0;
+  const size_t n_snap_t = want_wf ? (size_t)g.nrec * plane * sizeof(T) : 0;
+  SlabPlan sl;
+  const size_t o_in = sl.add(n_in), o_m1 = sl.add(n_m1), o_m2 = sl.add(n_m2), o_state = sl.add(n_state);
+  const size_t o_seis = sl.add(n_seis), o_seis_t = sl.add(n_seis), o_src = sl.add(sizeof(int2));
+  const size_t o_snap = sl.add(n_snap), o_snap_t = sl.add(n_snap_t);
+  SWD_TRY(J.slab.alloc(sl.bytes));
+  J.d_in = DevView(J.slab, o_in, n_in);
+  J.d_m1 = DevView(J.slab, o_m1, n_m1);
+  J.d_m2 = DevView(J.slab, o_m2, n_m2);
+  J.d_state = DevView(J.slab, o_state, n_state);
+  J.d_seis = DevView(J.slab, o_seis, n_seis);
+  J.d_seis_t = DevView(J.slab, o_seis_t, n_seis);
+  J.d_src = DevView(J.slab, o_src, sizeof(int2));
+  J.d_snap = DevView(J.slab, o_snap, n_snap);
+  J.d_snap_t = DevView(J.slab, o_snap_t, n_snap_t);
   T* din = J.d_in.template as<T>();
   const T* hsrc[6] = {temp, b, b1, ca, cl, cm1};
   for (int i = 0; i < 6; ++i) SWD_CUDA(cudaMemcpyAsync(din + i * NN, hsrc[i], NN * sizeof(T), cudaMemcpyHostToDevice, st));
@@ -616,7 +624,8 @@ struct AdjJob {
   int nt = 0;
   size_t plane = 0;
   FdGeom g{};
-  DevBuf d_in, d_m1, d_m2, d_state, d_res, d_snap, d_img, d_out;
+  DevBuf slab;  // one allocation holding every buffer below
+  DevView d_in, d_m1, d_m2, d_state, d_res, d_snap, d_img, d_out;
   AdjArgs<T> a{};
   T* bufs[2] = {nullptr, nullptr};
   TO* out[3] = {};  // host: cl_img, cm_img, illum
@@ -649,14 +658,22 @@ int adj_job_setup(AdjJob<T, TO>& J, const T* iv, int n_iv, const T* temp, const 
   const size_t NN = (size_t)NZ * NX, plane = (size_t)nz * nx, nsnap = (size_t)g.nrec * plane;
   J.nt = nt;
   J.plane = plane;
-  SWD_TRY(J.d_in.alloc(std::max(6 * NN, nsnap) * sizeof(T) + (size_t)nt * ng * sizeof(T)));
-  SWD_TRY(J.d_m1.alloc(g.field * sizeof(V)));
-  SWD_TRY(J.d_m2.alloc(g.field * sizeof(V2)));
-  SWD_TRY(J.d_state.alloc(2 * 5 * g.field * sizeof(T)));
-  SWD_TRY(J.d_res.alloc((size_t)nt * ng * sizeof(T)));
-  SWD_TRY(J.d_snap.alloc(4 * nsnap * sizeof(T)));
-  SWD_TRY(J.d_img.alloc(3 * plane * sizeof(double)));
-  SWD_TRY(J.d_out.alloc(3 * plane * sizeof(TO)));
+  const size_t n_in = std::max(6 * NN, nsnap) * sizeof(T) + (size_t)nt * ng * sizeof(T);
+  const size_t n_m1 = g.field * sizeof(V), n_m2 = g.field * sizeof(V2), n_state = 2 * 5 * g.field * sizeof(T);
+  const size_t n_res = (size_t)nt * ng * sizeof(T), n_snap = 4 * nsnap * sizeof(T);
+  const size_t n_img = 3 * plane * sizeof(double), n_out = 3 * plane * sizeof(TO);
+  SlabPlan sl;
+  const size_t o_in = sl.add(n_in), o_m1 = sl.add(n_m1), o_m2 = sl.add(n_m2), o_state = sl.add(n_state);
+  const size_t o_res = sl.add(n_res), o_snap = sl.add(n_snap), o_img = sl.add(n_img), o_out = sl.add(n_out);
+  SWD_TRY(J.slab.alloc(sl.bytes));
+  J.d_in = DevView(J.slab, o_in, n_in);
+  J.d_m1 = DevView(J.slab, o_m1, n_m1);
+  J.d_m2 = DevView(J.slab, o_m2, n_m2);
+  J.d_state = DevView(J.slab, o_state, n_state);
+  J.d_res = DevView(J.slab, o_res, n_res);
+  J.d_snap = DevView(J.slab, o_snap, n_snap);
+  J.d_img = DevView(J.slab, o_img, n_img);
+  J.d_out = DevView(J.slab, o_out, n_out);
   T* din = J.d_in.template as<T>();
   T* dstage = din + std::max(6 * NN, nsnap);
   const T* hsrc[6] = {temp, b, b1, ca, cl, cm1};

@@ -87,4 +87,13 @@ struct SlabPlan {
   }
 };
 
+// n bytes at offset off of a slab, with DevBuf's accessors; it owns nothing (NULL when n is 0).
+struct DevView {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevView() = default;
+  DevView(const DevBuf& b, size_t off, size_t n) : p(n ? static_cast<char*>(b.p) + off : nullptr), bytes(n) {}
+  template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
 }  // namespace swd
