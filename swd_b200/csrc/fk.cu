@@ -131,12 +131,14 @@ extern "C" int swd_fk_filter(const double* d, int ns, int ntr, double dt, double
   }
   const std::vector<double2> w1 = roots(L1), w2 = roots(L2), wn = roots(nf);
   const size_t nd = (size_t)ns * ntr, nc = (size_t)ntr * nf;
-  DevBuf bd, bx, by, br, bt;
-  SWD_TRY(bd.alloc(nd * sizeof(double)));
-  SWD_TRY(bx.alloc(nc * sizeof(double2)));
-  SWD_TRY(by.alloc(nc * sizeof(double2)));
-  SWD_TRY(br.alloc(nc * sizeof(double2)));
-  SWD_TRY(bt.alloc((size_t)(L1 + L2 + nf + 2 * nk) * sizeof(double2)));
+  const size_t n_tab = (size_t)(L1 + L2 + nf + 2 * nk) * sizeof(double2);
+  SlabPlan sl;
+  const size_t o_d = sl.add(nd * sizeof(double)), o_x = sl.add(nc * sizeof(double2));
+  const size_t o_y = sl.add(nc * sizeof(double2)), o_r = sl.add(nc * sizeof(double2)), o_t = sl.add(n_tab);
+  DevBuf slab;
+  SWD_TRY(slab.alloc(sl.bytes));
+  const DevView bd(slab, o_d, nd * sizeof(double)), bx(slab, o_x, nc * sizeof(double2));
+  const DevView by(slab, o_y, nc * sizeof(double2)), br(slab, o_r, nc * sizeof(double2)), bt(slab, o_t, n_tab);
   double2* W1 = bt.as<double2>();
   double2* W2 = W1 + L1;
   double2* Wn = W2 + L2;

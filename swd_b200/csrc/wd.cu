@@ -220,15 +220,17 @@ extern "C" int swd_wd_residual(int nt, int ng, const double* seismo_v_d, const d
     SWD_CHECK(!gg[s].valid || (c0[s] && cp[s]), "missing %s-side picks", s ? "left" : "right");
   }
   const size_t nsz = (size_t)nt * ng, np2 = (size_t)g.npair;
-  DevBuf b_in, b_t, b_out, b_W, b_X, b_fre, b_cr, b_g;
-  SWD_TRY(b_in.alloc(nsz * sizeof(double)));
-  SWD_TRY(b_t.alloc(nsz * sizeof(double)));
-  SWD_TRY(b_out.alloc(nsz * sizeof(double)));
-  SWD_TRY(b_W.alloc((size_t)g.win * nt * sizeof(double2)));
-  SWD_TRY(b_X.alloc(2 * (size_t)g.win * offset * sizeof(double2)));
-  SWD_TRY(b_fre.alloc(np2 * sizeof(double)));
-  SWD_TRY(b_cr.alloc(4 * np2 * sizeof(double)));
-  SWD_TRY(b_g.alloc(2 * sizeof(Gather)));
+  const size_t n_seis = nsz * sizeof(double), n_W = (size_t)g.win * nt * sizeof(double2);
+  const size_t n_X = 2 * (size_t)g.win * offset * sizeof(double2);
+  SlabPlan sl;
+  const size_t o_in = sl.add(n_seis), o_t = sl.add(n_seis), o_out = sl.add(n_seis), o_W = sl.add(n_W);
+  const size_t o_X = sl.add(n_X), o_fre = sl.add(np2 * sizeof(double)), o_cr = sl.add(4 * np2 * sizeof(double));
+  const size_t o_g = sl.add(2 * sizeof(Gather));
+  DevBuf slab;
+  SWD_TRY(slab.alloc(sl.bytes));
+  const DevView b_in(slab, o_in, n_seis), b_t(slab, o_t, n_seis), b_out(slab, o_out, n_seis), b_W(slab, o_W, n_W);
+  const DevView b_X(slab, o_X, n_X), b_fre(slab, o_fre, np2 * sizeof(double));
+  const DevView b_cr(slab, o_cr, 4 * np2 * sizeof(double)), b_g(slab, o_g, 2 * sizeof(Gather));
   std::vector<double> fre(np2);
   wd_fre(fmin, fmax, g.nfre, fre.data());
   cudaStream_t st = 0;
