@@ -92,6 +92,21 @@ typedef struct {
 } swd_e2drtm_job;
 int swd_e2drtm_single_batch(int n_jobs, const swd_e2drtm_job* jobs);
 
+/* A forward batch whose strain snapshots stay on the device for an adjoint batch of the same
+ * jobs, so that they need not go to the host and back (no counterpart in the reference, where
+ * the snapshots are MEX outputs and inputs).  swd_staggerfd_single_batch_keep runs the forward
+ * as swd_staggerfd_single_batch, recording every job's snapshots on the device even where fux..bwz
+ * are NULL (where they are given they are also returned), and fills *kept.
+ * swd_e2drtm_single_batch_kept runs the adjoint as swd_e2drtm_single_batch with job j reading
+ * forward job j's snapshots in place of its fux..bwz (ignored; job j must have forward job j's
+ * nz, nx and nt / nt_wf).  Its images equal those of the adjoint batch given the forward's
+ * returned snapshots, bit for bit.  kept may serve several adjoint batches; swd_fd_batch_free
+ * releases it. */
+typedef struct swd_fd_batch swd_fd_batch;
+int swd_staggerfd_single_batch_keep(int n_jobs, const swd_staggerfd_job* jobs, swd_fd_batch** kept);
+int swd_e2drtm_single_batch_kept(int n_jobs, const swd_e2drtm_job* jobs, const swd_fd_batch* kept);
+void swd_fd_batch_free(swd_fd_batch* kept);
+
 /* Replaces eigen_staggerfd_double (binary-only in the reference; interface at
  * core/staggerfd_eigend.m:139).  Same arguments in double precision. */
 int swd_staggerfd_double(const double* iv, int n_iv, const double* temp, const double* ca,

@@ -39,6 +39,9 @@ _SIGS = {
     "swd_staggerfd_single": [_f32p, _c_int] + [_f32p] * 14,
     "swd_staggerfd_single_batch": [_c_int, ctypes.c_void_p],
     "swd_e2drtm_single_batch": [_c_int, ctypes.c_void_p],
+    "swd_staggerfd_single_batch_keep": [_c_int, ctypes.c_void_p, ctypes.c_void_p],
+    "swd_e2drtm_single_batch_kept": [_c_int, ctypes.c_void_p, ctypes.c_void_p],
+    "swd_fd_batch_free": [ctypes.c_void_p],
     "swd_staggerfd_double": [_f64p, _c_int] + [_f64p] * 14,
     "swd_e2drtm_single": [_f32p, _c_int] + [_f32p] * 15,
     "swd_e2drtm_single_f64out": [_f32p, _c_int] + [_f32p] * 12 + [_f64p] * 3,
@@ -60,7 +63,7 @@ _SIGS = {
     "swd_wd_residual": [_c_int, _c_int, _f64p, _f64p, _c_int, _c_dbl, _c_dbl, _c_int, _c_dbl, _c_int, _c_int,
                         _c_dbl, _c_int, _c_int, _f64p, _c_int, _c_dbl, _c_dbl] + [_f64p] * 4 + [_c_int, _f64p],
 }
-_RESTYPE = {"swd_last_error": ctypes.c_char_p, "swd_kernel_launches": ctypes.c_uint64}
+_RESTYPE = {"swd_last_error": ctypes.c_char_p, "swd_kernel_launches": ctypes.c_uint64, "swd_fd_batch_free": None}
 
 SWD_OK = 0
 _STATUS = {1: "SWD_ERR_INVALID", 2: "SWD_ERR_UNSUPPORTED", 3: "SWD_ERR_CUDA", 4: "SWD_ERR_OOM",

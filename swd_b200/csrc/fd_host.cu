@@ -519,18 +519,20 @@ struct FwdJob {
 
 // Validates the call, allocates and fills the job's device buffers on st (materials packed,
 // state and seismograms cleared); the time loop then sets a.in / a.out from bufs.
+// keep_wf records the strain snapshots on the device even when fux..bwz are NULL.
 template <typename T>
 int fwd_job_setup(FwdJob<T>& J, const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, const T* cm1,
                   const T* b, const T* b1, const T* s, T* seis_u, T* seis_w, T* fux, T* fuz, T* bwx, T* bwz,
-                  cudaStream_t st) {
+                  cudaStream_t st, bool keep_wf = false) {
   FwdIv& p = J.p;
   SWD_TRY(parse_fwd_iv(iv, n_iv, p));
   const int nbc = (p.nxbc - p.nx) / 2;  // core/eigen_staggerfd_single.cpp:116
   SWD_TRY(validate_geom(p.nt, p.nzbc, p.nxbc, p.nz, p.nx, nbc, p.nt_wf, p.fd_order, p.ng, p.gz, p.gx, p.dg));
   SWD_TRY(validate_source(p.src_type, p.sz, p.sx, p.nzbc, p.nxbc));
   SWD_CHECK(temp && ca && cl && cm1 && b && b1 && s && seis_w, "null input/output pointer");
-  const bool want_wf = fux || fuz || bwx || bwz;
-  SWD_CHECK(!want_wf || (fux && fuz && bwx && bwz), "fux/fuz/bwx/bwz must all be given or all be NULL");
+  const bool host_wf = fux || fuz || bwx || bwz;
+  SWD_CHECK(!host_wf || (fux && fuz && bwx && bwz), "fux/fuz/bwx/bwz must all be given or all be NULL");
+  const bool want_wf = host_wf || keep_wf;
   FdGeom& g = J.g;
   fill_geom<T>(g, p.nzbc, p.nxbc, p.nz, p.nx, nbc, p.nt, p.nt_wf, p.ng, p.gz, p.gx, p.dg);
   plan_decomposition(g, 1, 0);
@@ -540,7 +542,7 @@ int fwd_job_setup(FwdJob<T>& J, const T* iv, int n_iv, const T* temp, const T* c
   const size_t n_in = 6 * NN * sizeof(T) + p.nt * sizeof(T), n_m1 = g.field * sizeof(V), n_m2 = g.field * sizeof(V2);
   const size_t n_state = 2 * 5 * g.field * sizeof(T), n_seis = 2 * (size_t)p.nt * p.ng * sizeof(T);
   const size_t n_snap = want_wf ? (size_t)g.nrec * 4 * plane * sizeof(T) : 0;
-  const size_t n_snap_t = want_wf ? (size_t)g.nrec * plane * sizeof(T) : 0;
+  const size_t n_snap_t = host_wf ? (size_t)g.nrec * plane * sizeof(T) : 0;
   SlabPlan sl;
   const size_t o_in = sl.add(n_in), o_m1 = sl.add(n_m1), o_m2 = sl.add(n_m2), o_state = sl.add(n_state);
   const size_t o_seis = sl.add(n_seis), o_seis_t = sl.add(n_seis), o_src = sl.add(sizeof(int2));
@@ -588,7 +590,7 @@ int fwd_job_finish(FwdJob<T>& J, cudaStream_t st) {
   SWD_TRY(transpose<T, T>(J.d_seis.template as<T>(), nn, J.d_seis_t.template as<T>(), nn, 2, p.nt, p.ng, st));
   SWD_CUDA(cudaMemcpyAsync(J.out[1], J.d_seis_t.template as<T>(), nn * sizeof(T), cudaMemcpyDeviceToHost, st));
   if (J.out[0]) SWD_CUDA(cudaMemcpyAsync(J.out[0], J.d_seis_t.template as<T>() + nn, nn * sizeof(T), cudaMemcpyDeviceToHost, st));
-  if (J.a.snap) {
+  if (J.a.snap && J.out[2]) {
     for (int f = 0; f < 4; ++f) {
       SWD_TRY(transpose<T, T>(J.d_snap.template as<T>() + f * plane, 4 * plane, J.d_snap_t.template as<T>(), plane, J.g.nrec, p.nz,
                               p.nx, st));
@@ -637,10 +639,12 @@ struct AdjJob {
 // Validates the call, allocates and fills the job's device buffers on st: materials packed, the
 // residual [nt][ng] and the snapshots [nrec][f][nz][nx] transposed from MATLAB's layout, state
 // and images cleared; the time loop then sets a.in / a.out from bufs.
+// d_snap, when given, is a forward job's device snapshots in this layout, read in place of
+// fux..bwz (which are then ignored).
 template <typename T, typename TO>
 int adj_job_setup(AdjJob<T, TO>& J, const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, const T* cm1,
                   const T* b, const T* b1, const T* res, const T* fux, const T* fuz, const T* bwx, const T* bwz,
-                  TO* cl_img, TO* cm_img, TO* illum, cudaStream_t st) {
+                  TO* cl_img, TO* cm_img, TO* illum, cudaStream_t st, const T* d_snap = nullptr) {
   SWD_CHECK(iv != nullptr && n_iv >= 14, "input_vector needs 14 entries (got %d)", n_iv);
   // core/eigen_e2drtm_single.cpp:69-84
   const int nt = (int)iv[0], NZ = (int)iv[1], NX = (int)iv[2], ng = (int)iv[4], nbc = (int)iv[5];
@@ -648,7 +652,8 @@ int adj_job_setup(AdjJob<T, TO>& J, const T* iv, int n_iv, const T* temp, const 
   const int nt_wf = (int)iv[10], nz = (int)iv[11], nx = (int)iv[12];
   const T dtx = iv[3], dt = iv[13];
   SWD_TRY(validate_geom(nt, NZ, NX, nz, nx, nbc, nt_wf, fd_order, ng, gz, gx, dg));
-  SWD_CHECK(temp && ca && cl && cm1 && b && b1 && res && fux && fuz && bwx && bwz && cl_img && cm_img && illum,
+  SWD_CHECK(temp && ca && cl && cm1 && b && b1 && res && (d_snap || (fux && fuz && bwx && bwz)) && cl_img &&
+                cm_img && illum,
             "null input/output pointer");
   FdGeom& g = J.g;
   fill_geom<T>(g, NZ, NX, nz, nx, nbc, nt, nt_wf, ng, gz, gx, dg);
@@ -658,9 +663,10 @@ int adj_job_setup(AdjJob<T, TO>& J, const T* iv, int n_iv, const T* temp, const 
   const size_t NN = (size_t)NZ * NX, plane = (size_t)nz * nx, nsnap = (size_t)g.nrec * plane;
   J.nt = nt;
   J.plane = plane;
-  const size_t n_in = std::max(6 * NN, nsnap) * sizeof(T) + (size_t)nt * ng * sizeof(T);
+  const size_t n_stage = d_snap ? 6 * NN : std::max(6 * NN, nsnap);
+  const size_t n_in = n_stage * sizeof(T) + (size_t)nt * ng * sizeof(T);
   const size_t n_m1 = g.field * sizeof(V), n_m2 = g.field * sizeof(V2), n_state = 2 * 5 * g.field * sizeof(T);
-  const size_t n_res = (size_t)nt * ng * sizeof(T), n_snap = 4 * nsnap * sizeof(T);
+  const size_t n_res = (size_t)nt * ng * sizeof(T), n_snap = d_snap ? 0 : 4 * nsnap * sizeof(T);
   const size_t n_img = 3 * plane * sizeof(double), n_out = 3 * plane * sizeof(TO);
   SlabPlan sl;
   const size_t o_in = sl.add(n_in), o_m1 = sl.add(n_m1), o_m2 = sl.add(n_m2), o_state = sl.add(n_state);
@@ -675,7 +681,7 @@ int adj_job_setup(AdjJob<T, TO>& J, const T* iv, int n_iv, const T* temp, const 
   J.d_img = DevView(J.slab, o_img, n_img);
   J.d_out = DevView(J.slab, o_out, n_out);
   T* din = J.d_in.template as<T>();
-  T* dstage = din + std::max(6 * NN, nsnap);
+  T* dstage = din + n_stage;
   const T* hsrc[6] = {temp, b, b1, ca, cl, cm1};
   for (int i = 0; i < 6; ++i) SWD_CUDA(cudaMemcpyAsync(din + i * NN, hsrc[i], NN * sizeof(T), cudaMemcpyHostToDevice, st));
   SWD_TRY(pack_materials<T>(din, din + NN, din + 2 * NN, din + 3 * NN, din + 4 * NN, din + 5 * NN,
@@ -685,7 +691,7 @@ int adj_job_setup(AdjJob<T, TO>& J, const T* iv, int n_iv, const T* temp, const 
   SWD_TRY(transpose<T, T>(dstage, 0, J.d_res.template as<T>(), 0, 1, ng, nt, st));
   // snapshots: MATLAB nz x nx x nrec per field -> [nrec][f][nz][nx]
   const T* wf[4] = {fux, fuz, bwx, bwz};
-  for (int f = 0; f < 4; ++f) {
+  for (int f = 0; f < 4 && !d_snap; ++f) {
     SWD_CUDA(cudaMemcpyAsync(din, wf[f], nsnap * sizeof(T), cudaMemcpyHostToDevice, st));
     SWD_TRY(transpose<T, T>(din, plane, J.d_snap.template as<T>() + f * plane, 4 * plane, g.nrec, nx, nz, st));
   }
@@ -693,7 +699,8 @@ int adj_job_setup(AdjJob<T, TO>& J, const T* iv, int n_iv, const T* temp, const 
   SWD_CUDA(cudaMemsetAsync(J.d_img.p, 0, J.d_img.bytes, st));
   AdjArgs<T>& a = J.a;
   a.g = g; a.mat = J.d_m1.template as<V>(); a.mb = J.d_m2.template as<V2>();
-  a.res = J.d_res.template as<T>(); a.snap = J.d_snap.template as<T>(); a.img = J.d_img.template as<double>();
+  a.res = J.d_res.template as<T>(); a.snap = d_snap ? d_snap : J.d_snap.template as<T>();
+  a.img = J.d_img.template as<double>();
   if (AdjJob<T, TO>::f32img) a.img32 = J.d_img.template as<float>();
   a.dtx = dtx; a.dt = dt; a.n_shots = 1;
   J.bufs[0] = J.d_state.template as<T>();
@@ -745,22 +752,22 @@ int e2drtm_mex(const T* iv, int n_iv, const T* temp, const T* ca, const T* cl, c
 
 using namespace swd;
 
-extern "C" {
+// The forward jobs of a batch whose strain snapshots stay on the device for an adjoint batch.
+struct swd_fd_batch {
+  std::vector<std::unique_ptr<swd::FwdJob<float>>> jobs;
+};
 
-const char* swd_last_error(void) { return g_err; }
-int swd_version(void) { return 100; }
-uint64_t swd_kernel_launches(void) { return g_launches.load(); }
+namespace swd {
+namespace {
 
-int swd_staggerfd_single(const float* iv, int n_iv, const float* temp, const float* ca, const float* cl,
-                         const float* cm, const float* cm1, const float* b, const float* b1, const float* s,
-                         float* seismo_u, float* seismo_w, float* fux, float* fuz, float* bwx, float* bwz) {
-  return staggerfd_mex<float>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, s, seismo_u, seismo_w, fux, fuz, bwx, bwz);
-}
-int swd_staggerfd_single_batch(int n_jobs, const swd_staggerfd_job* jobs) {
-  clear_error();
+const float* kept_snap(const swd_fd_batch* kept, int j) { return kept->jobs[j]->a.snap; }
+
+// The forward batch; keep_wf records every job's snapshots on the device for a later adjoint batch.
+int fwd_batch(int n_jobs, const swd_staggerfd_job* jobs, std::vector<std::unique_ptr<FwdJob<float>>>& J,
+              bool keep_wf) {
   SWD_CHECK(jobs && n_jobs >= 1, "a batch needs at least one job (got %d)", n_jobs);
   cudaStream_t st = 0;
-  std::vector<std::unique_ptr<FwdJob<float>>> J;
+  J.clear();
   std::vector<int> cta0(n_jobs + 1, 0);
   int nt_max = 0;
   for (int j = 0; j < n_jobs; ++j) {
@@ -768,7 +775,7 @@ int swd_staggerfd_single_batch(int n_jobs, const swd_staggerfd_job* jobs) {
     J.push_back(std::make_unique<FwdJob<float>>());
     FwdJob<float>& w = *J.back();
     const int rc = fwd_job_setup(w, q.iv, q.n_iv, q.temp, q.ca, q.cl, q.cm1, q.b, q.b1, q.s, q.seismo_u, q.seismo_w,
-                                 q.fux, q.fuz, q.bwx, q.bwz, st);
+                                 q.fux, q.fuz, q.bwx, q.bwz, st, keep_wf);
     if (rc != SWD_OK) {
       set_error("job %d: %s", j, std::string(swd_last_error()).c_str());
       return rc;
@@ -810,14 +817,8 @@ int swd_staggerfd_single_batch(int n_jobs, const swd_staggerfd_job* jobs) {
   SWD_CUDA(cudaStreamSynchronize(st));
   return SWD_OK;
 }
-int swd_staggerfd_double(const double* iv, int n_iv, const double* temp, const double* ca, const double* cl,
-                         const double* cm, const double* cm1, const double* b, const double* b1, const double* s,
-                         double* seismo_u, double* seismo_w, double* fux, double* fuz, double* bwx,
-                         double* bwz) {
-  return staggerfd_mex<double>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, s, seismo_u, seismo_w, fux, fuz, bwx, bwz);
-}
-int swd_e2drtm_single_batch(int n_jobs, const swd_e2drtm_job* jobs) {
-  clear_error();
+// The adjoint batch; with kept, job j reads forward job j's device snapshots in place of fux..bwz.
+int adj_batch(int n_jobs, const swd_e2drtm_job* jobs, const swd_fd_batch* kept) {
   SWD_CHECK(jobs && n_jobs >= 1, "a batch needs at least one job (got %d)", n_jobs);
   cudaStream_t st = 0;
   std::vector<std::unique_ptr<AdjJob<float, float>>> J;
@@ -828,10 +829,16 @@ int swd_e2drtm_single_batch(int n_jobs, const swd_e2drtm_job* jobs) {
     J.push_back(std::make_unique<AdjJob<float, float>>());
     AdjJob<float, float>& w = *J.back();
     const int rc = adj_job_setup(w, q.iv, q.n_iv, q.temp, q.ca, q.cl, q.cm1, q.b, q.b1, q.seismo_w, q.fux, q.fuz, q.bwx,
-                                 q.bwz, q.cl_img, q.cm_img, q.illum_div, st);
+                                 q.bwz, q.cl_img, q.cm_img, q.illum_div, st, kept ? kept_snap(kept, j) : nullptr);
     if (rc != SWD_OK) {
       set_error("job %d: %s", j, std::string(swd_last_error()).c_str());
       return rc;
+    }
+    if (kept) {  // the forward job's snapshots must have this job's shape
+      const FdGeom& fg = kept->jobs[j]->g;
+      SWD_CHECK(fg.nrec == w.g.nrec && fg.nz == w.g.nz && fg.nx == w.g.nx,
+                "job %d: the kept forward job has %d snapshots of %d x %d, this job needs %d of %d x %d", j, fg.nrec,
+                fg.nz, fg.nx, w.g.nrec, w.g.nz, w.g.nx);
     }
     // the one kernel shape of the MEX-convention adjoint (launch_adj_step with b, b1 arrays)
     SWD_CHECK(w.g.sched == 0 && w.g.warps == 4 && w.g.cells == 1 && w.g.ring_adj == 4,
@@ -869,6 +876,51 @@ int swd_e2drtm_single_batch(int n_jobs, const swd_e2drtm_job* jobs) {
   for (int j = 0; j < n_jobs; ++j) SWD_TRY(adj_job_finish(*J[j], st));
   SWD_CUDA(cudaStreamSynchronize(st));
   return SWD_OK;
+}
+}  // namespace
+}  // namespace swd
+
+extern "C" {
+
+const char* swd_last_error(void) { return g_err; }
+int swd_version(void) { return 100; }
+uint64_t swd_kernel_launches(void) { return g_launches.load(); }
+
+int swd_staggerfd_single(const float* iv, int n_iv, const float* temp, const float* ca, const float* cl,
+                         const float* cm, const float* cm1, const float* b, const float* b1, const float* s,
+                         float* seismo_u, float* seismo_w, float* fux, float* fuz, float* bwx, float* bwz) {
+  return staggerfd_mex<float>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, s, seismo_u, seismo_w, fux, fuz, bwx, bwz);
+}
+int swd_staggerfd_single_batch(int n_jobs, const swd_staggerfd_job* jobs) {
+  clear_error();
+  std::vector<std::unique_ptr<FwdJob<float>>> J;
+  return fwd_batch(n_jobs, jobs, J, false);
+}
+int swd_staggerfd_single_batch_keep(int n_jobs, const swd_staggerfd_job* jobs, swd_fd_batch** kept) {
+  clear_error();
+  SWD_CHECK(kept != nullptr, "kept must point to a swd_fd_batch* to fill");
+  *kept = nullptr;
+  std::unique_ptr<swd_fd_batch> b(new swd_fd_batch);
+  SWD_TRY(fwd_batch(n_jobs, jobs, b->jobs, true));
+  *kept = b.release();
+  return SWD_OK;
+}
+int swd_e2drtm_single_batch(int n_jobs, const swd_e2drtm_job* jobs) {
+  clear_error();
+  return adj_batch(n_jobs, jobs, nullptr);
+}
+int swd_e2drtm_single_batch_kept(int n_jobs, const swd_e2drtm_job* jobs, const swd_fd_batch* kept) {
+  clear_error();
+  SWD_CHECK(kept != nullptr && (int)kept->jobs.size() == n_jobs,
+            "the kept forward batch has %d jobs, this adjoint batch %d", kept ? (int)kept->jobs.size() : 0, n_jobs);
+  return adj_batch(n_jobs, jobs, kept);
+}
+void swd_fd_batch_free(swd_fd_batch* kept) { delete kept; }
+int swd_staggerfd_double(const double* iv, int n_iv, const double* temp, const double* ca, const double* cl,
+                         const double* cm, const double* cm1, const double* b, const double* b1, const double* s,
+                         double* seismo_u, double* seismo_w, double* fux, double* fuz, double* bwx,
+                         double* bwz) {
+  return staggerfd_mex<double>(iv, n_iv, temp, ca, cl, cm, cm1, b, b1, s, seismo_u, seismo_w, fux, fuz, bwx, bwz);
 }
 int swd_e2drtm_single(const float* iv, int n_iv, const float* temp, const float* ca, const float* cl,
                       const float* cm, const float* cm1, const float* b, const float* b1, const float* seismo_w,

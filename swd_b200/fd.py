@@ -19,7 +19,7 @@ import ctypes
 
 import numpy as np
 
-from ._lib import call, ptr
+from ._lib import call, lib, ptr
 
 _SRC = {"p": 1, "s": 2, "s1": 3, "z": 4, "w": 5}  # core/staggerfd_eigen.m:126-136
 
@@ -35,12 +35,26 @@ class _FdJob(ctypes.Structure):
                                                 "seismo_w", "fux", "fuz", "bwx", "bwz")]
 
 
-def eigen_staggerfd_single_batch(jobs, want_wf=False):
+class KeptWavefields:
+    """The strain snapshots of a forward batch, kept on the device for eigen_e2drtm_single_batch
+    (swd_staggerfd_single_batch_keep); released when this object goes."""
+
+    def __init__(self, handle, n_jobs):
+        self.handle, self.n_jobs = handle, n_jobs
+
+    def __del__(self):
+        if self.handle:
+            lib().swd_fd_batch_free(self.handle)
+            self.handle = None
+
+
+def eigen_staggerfd_single_batch(jobs, want_wf=False, keep=False):
     """Several eigen_staggerfd_single calls, on grids of any sizes, advanced together by one launch per
     time step; it has no counterpart in the reference (one MEX call per shot and model).  jobs: a
     list of (iv, temp, ca, cl, cm, cm1, b, b1, s) as for eigen_staggerfd_single.  Returns
-    [(seismo_u, seismo_w, www or None)], bit for bit those of the separate calls."""
-    keep, outs = [], []
+    [(seismo_u, seismo_w, www or None)], bit for bit those of the separate calls; with keep, also
+    a KeptWavefields holding every job's snapshots on the device for eigen_e2drtm_single_batch."""
+    alive, outs = [], []
     arr = (_FdJob * len(jobs))()
     for k, (iv, temp, ca, cl, cm, cm1, b, b1, s) in enumerate(jobs):
         iv = np.ascontiguousarray(np.asarray(iv, np.float32).reshape(-1))
@@ -53,13 +67,17 @@ def eigen_staggerfd_single_batch(jobs, want_wf=False):
         sw = np.zeros((nt, ng), np.float32, order="F")
         wf = ({f: np.zeros((nz, nx, nt // max(ntwf, 1)), np.float32, order="F") for f in ("fux", "fuz", "bwx", "bwz")}
               if want_wf else None)
-        keep += [iv, s, *mats]
+        alive += [iv, s, *mats]
         outs.append((su, sw, wf))
         w = [wf[f].ctypes.data if wf else None for f in ("fux", "fuz", "bwx", "bwz")]
         arr[k] = _FdJob(iv.ctypes.data, iv.size, *[m.ctypes.data for m in mats], s.ctypes.data, su.ctypes.data,
                         sw.ctypes.data, *w)
-    call("swd_staggerfd_single_batch", len(jobs), ctypes.cast(arr, ctypes.c_void_p))
-    return outs
+    if not keep:
+        call("swd_staggerfd_single_batch", len(jobs), ctypes.cast(arr, ctypes.c_void_p))
+        return outs
+    h = ctypes.c_void_p()
+    call("swd_staggerfd_single_batch_keep", len(jobs), ctypes.cast(arr, ctypes.c_void_p), ctypes.byref(h))
+    return outs, KeptWavefields(h.value, len(jobs))
 
 
 class _AdjJob(ctypes.Structure):
@@ -69,22 +87,32 @@ class _AdjJob(ctypes.Structure):
                                                 "bwx", "bwz", "cl_img", "cm_img", "illum_div")]
 
 
-def eigen_e2drtm_single_batch(jobs):
+def eigen_e2drtm_single_batch(jobs, kept=None):
     """Several eigen_e2drtm_single calls, on grids of any sizes, advanced together by one launch per
     time step (no counterpart in the reference).  jobs: a list of (iv, temp, ca, cl, cm, cm1, b, b1,
     seismo_w, fux, fuz, bwx, bwz) as for eigen_e2drtm_single.  Returns [(cl_img, cm_img, illum_div)],
-    FP32 as the single MEX, bit for bit those of the separate calls."""
+    FP32 as the single MEX, bit for bit those of the separate calls.  kept: the KeptWavefields of
+    the forward batch of the same jobs, whose device snapshots job k then reads in place of its
+    fux..bwz (which may be None)."""
+    if kept is not None and kept.n_jobs != len(jobs):
+        raise ValueError(f"the kept forward batch has {kept.n_jobs} jobs, this batch {len(jobs)}")
     keep, outs = [], []
     arr = (_AdjJob * len(jobs))()
     for k, job in enumerate(jobs):
         iv = np.ascontiguousarray(np.asarray(job[0], np.float32).reshape(-1))
         nz, nx = int(iv[11]), int(iv[12])
-        ins = [_f(a, np.float32) for a in job[1:]]
+        ins = [None if (a is None and kept is not None and i >= 10) else _f(a, np.float32)
+               for i, a in enumerate(job[1:], 1)]
         img = [np.zeros((nz, nx), np.float32, order="F") for _ in range(3)]
         keep += [iv, *ins]
         outs.append(tuple(img))
-        arr[k] = _AdjJob(iv.ctypes.data, iv.size, *[a.ctypes.data for a in ins], *[o.ctypes.data for o in img])
-    call("swd_e2drtm_single_batch", len(jobs), ctypes.cast(arr, ctypes.c_void_p))
+        arr[k] = _AdjJob(iv.ctypes.data, iv.size, *[None if a is None else a.ctypes.data for a in ins],
+                         *[o.ctypes.data for o in img])
+    if kept is None:
+        call("swd_e2drtm_single_batch", len(jobs), ctypes.cast(arr, ctypes.c_void_p))
+    else:
+        call("swd_e2drtm_single_batch_kept", len(jobs), ctypes.cast(arr, ctypes.c_void_p),
+             ctypes.c_void_p(kept.handle))
     return outs
 
 

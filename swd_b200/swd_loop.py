@@ -158,8 +158,9 @@ def gradient_many(cases, field=0, FK=0):
     """SWD_single.m:171-201 for several surveys at once, on grids of any sizes: the forward of every
     shot of every survey runs as one batch (swd_staggerfd_single_batch: one launch per time step
     for all of them), the spectra, picks and adjoint sources per shot, then the adjoint of every
-    shot as one batch (swd_e2drtm_single_batch).  cases: [(s, vs, cr0_r, cr0_l)].  Returns one
-    dict per survey, equal to gradient(s, vs, cr0_r, cr0_l) of each (single path)."""
+    shot as one batch (swd_e2drtm_single_batch), reading the forward's strain snapshots where the
+    forward batch left them on the device.  cases: [(s, vs, cr0_r, cr0_l)].  Returns one dict per
+    survey, equal to gradient(s, vs, cr0_r, cr0_l) of each (single path)."""
     from .fd import (e2drtm_mex_args, eigen_e2drtm_single_batch, eigen_staggerfd_single_batch, prep_model,
                      staggerfd_mex_args)
     fwd, keys, mats = [], [], []
@@ -171,16 +172,19 @@ def gradient_many(cases, field=0, FK=0):
                                       s.vp_ratio * vs, vs, s.isfs, s.fd_order, s.source_type, 0, s.nt_wf, True, m)
             fwd.append((*args, s.source()))
             keys.append((c, is_))
-    seis = eigen_staggerfd_single_batch(fwd, want_wf=True)
+    seis, kept = eigen_staggerfd_single_batch(fwd, keep=True)
     per = [[] for _ in cases]
     adj = []
-    for (c, is_), (_, sw, www) in zip(keys, seis):
+    on_device = dict.fromkeys(("fux", "fuz", "bwx", "bwz"))  # read from kept
+    for (c, is_), (_, sw, _) in zip(keys, seis):
         s, vs, cr0_r, cr0_l = cases[c]
         out, a = _shot_adjoint_source(s, is_, sw, cr0_r, cr0_l, True, field, FK)
         per[c].append(out)
-        adj.append(e2drtm_mex_args(www, a, s.nbc, s.nt, s.dtx, s.dx, s.dt, s.gx, np.ones(s.ng), s.vp_ratio * vs, vs,
-                                   s.isfs, s.fd_order, 0, s.nt_wf, True, mats[c]))
-    for (c, _), (cl, cm, il), out in zip(keys, eigen_e2drtm_single_batch(adj), [o for p in per for o in p]):
+        adj.append(e2drtm_mex_args(on_device, a, s.nbc, s.nt, s.dtx, s.dx, s.dt, s.gx, np.ones(s.ng), s.vp_ratio * vs,
+                                   vs, s.isfs, s.fd_order, 0, s.nt_wf, True, mats[c]))
+    imgs = eigen_e2drtm_single_batch(adj, kept)
+    del kept
+    for (c, _), (cl, cm, il), out in zip(keys, imgs, [o for p in per for o in p]):
         out.update(cl=np.asarray(cl, np.float64), cm=np.asarray(cm, np.float64), il=np.asarray(il, np.float64))
     return [_assemble(cases[c][0], cases[c][1], per[c], False) for c in range(len(cases))]
 

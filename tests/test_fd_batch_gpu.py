@@ -8,6 +8,7 @@ import pytest
 
 import swd_b200 as S
 from swd_b200 import configs
+from swd_b200._lib import SwdError
 from swd_b200.fd import eigen_e2drtm_single_batch, eigen_staggerfd_single_batch
 
 pytestmark = pytest.mark.gpu
@@ -104,3 +105,36 @@ def test_gradient_of_several_surveys_in_one_batch(O):
             assert np.array_equal(got[k], ref[k]), (s.name, k)
         for k in ("dk_vs", "res_r", "res_l"):
             assert np.array_equal(got[k], ref[k], equal_nan=True), (s.name, k)
+
+
+def test_adjoint_batch_reads_the_kept_forward_snapshots(O):
+    """swd_staggerfd_single_batch_keep / swd_e2drtm_single_batch_kept: the adjoint batch reads the
+    forward batch's snapshots on the device and gives the images of the adjoint batch fed the
+    forward's returned snapshots, bit for bit; the handle serves a second batch, and a job whose
+    shape differs from its forward job's is refused before any launch."""
+    tiny = configs.tiny(nt=400)
+    c1 = dataclasses.replace(configs.plain_c1(), nt=800, nt_wf=10)
+    fwd, adj_in = [], []
+    for s, is_ in ((tiny, 2), (c1, 4)):
+        inp, w = _job(O, s, is_)
+        fwd.append((inp.iv, inp.temp, inp.ca, inp.cl, inp.cm, inp.cm1, inp.b, inp.b1, w))
+        adj_in.append(O.fd_inputs(s.nbc, s.nt, s.dtx, s.dx, s.dt, int(s.sx[is_ - 1]), 1, s.gx, np.ones(s.ng), s.vp,
+                                  s.vs, in_wf=s.nt_wf, adjoint=True))
+    host = eigen_staggerfd_single_batch(fwd, want_wf=True)
+    seis, kept = eigen_staggerfd_single_batch(fwd, keep=True)
+    with_wf, on_device = [], []
+    for (_, sw, wf), (_, sw2, wf2), ai in zip(host, seis, adj_in):
+        assert np.array_equal(sw, sw2) and wf2 is None
+        res = np.asfortranarray(sw * 0.5)
+        head = (ai.iv, ai.temp, ai.ca, ai.cl, ai.cm, ai.cm1, ai.b, ai.b1, res)
+        with_wf.append(head + (wf["fux"], wf["fuz"], wf["bwx"], wf["bwz"]))
+        on_device.append(head + (None, None, None, None))
+    want = eigen_e2drtm_single_batch(with_wf)
+    for _ in range(2):
+        for got, ref in zip(eigen_e2drtm_single_batch(on_device, kept), want):
+            for g, r in zip(got, ref):
+                assert np.abs(r).max() > 0 and np.array_equal(g, r)
+    with pytest.raises(SwdError, match="job 0: the kept forward job"):
+        eigen_e2drtm_single_batch(on_device[::-1], kept)
+    with pytest.raises(ValueError, match="kept forward batch has 2 jobs"):
+        eigen_e2drtm_single_batch(on_device[:1], kept)
